@@ -1,0 +1,95 @@
+"""Compile the CUDA sources of the package into ``critmc_b200/libcritmc_b200.so``.
+
+Every ``csrc/*.cu`` file is compiled for sm_100a only (``-gencode
+arch=compute_100a,code=sm_100a``) and linked into one shared library that
+exports the C ABI declared in ``include/critmc_b200.h``.  Objects go to
+``critmc_b200/_build/``; a file is recompiled when it or any header is newer
+than its object.  nvcc cross-compiles, so this works on a machine without a GPU.
+"""
+
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = PKG / "_build"
+LIB = PKG / "libcritmc_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-O3",
+    "-lineinfo",
+    "-std=c++17",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler",
+    "-fPIC,-O2",
+    f"-I{INCLUDE}",
+    f"-I{CSRC}",
+]
+
+
+def nvcc() -> str:
+    exe = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(exe).exists():
+        raise RuntimeError("nvcc not found: the CUDA toolkit is needed to build critmc_b200")
+    return exe
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _compile(src: Path, obj: Path, extra: list[str]) -> None:
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stdout}\n{res.stderr}")
+
+
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
+    """Build the shared library (incrementally) and return its path."""
+    extra = list(extra or [])
+    BUILD.mkdir(exist_ok=True)
+    sources = sorted(CSRC.glob("*.cu"))
+    newest_header = max((p.stat().st_mtime for p in _headers()), default=0.0)
+    jobs = []
+    objects = []
+    for src in sources:
+        obj = BUILD / (src.stem + ".o")
+        objects.append(obj)
+        stale = (
+            force
+            or not obj.exists()
+            or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
+        )
+        if stale:
+            jobs.append((src, obj))
+    if jobs:
+        workers = max(1, min(len(jobs), os.cpu_count() or 1))
+        with cf.ThreadPoolExecutor(workers) as ex:
+            futs = [ex.submit(_compile, s, o, extra) for s, o in jobs]
+            for f in futs:
+                f.result()
+        if verbose:
+            print(f"compiled {[s.name for s, _ in jobs]}")
+    if jobs or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objects):
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objects), "-lcudart"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    import sys
+
+    print(build(force="--force" in sys.argv, verbose=True))

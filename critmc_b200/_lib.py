@@ -1,0 +1,81 @@
+"""ctypes binding of ``libcritmc_b200.so`` (the C ABI in ``include/critmc_b200.h``).
+
+The library is built in-tree by :mod:`critmc_b200._build`.  Loading fails
+loudly when it is missing: there is no CPU fallback for any sampler.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libcritmc_b200.so"
+
+_lib: ctypes.CDLL | None = None
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_U32 = ctypes.c_uint32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+# name -> (restype, argtypes); kept in the order of include/critmc_b200.h
+SIGNATURES: dict[str, tuple] = {
+    "critmc_version": (_I32, []),
+    "critmc_last_error": (_I32, [_P, _I32]),
+    "critmc_ising_class_table": (_I32, [_I32, _I32, _D, _D, _P, _P, _P]),
+    "critmc_ising_msc_scratch_bytes": (_I64, [_I32, _I32]),
+    "critmc_ising_msc_run": (
+        _I32,
+        [_P, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P, _P, _P,
+         _I32, _I32, _P],
+    ),
+    "critmc_ising_msc_measure": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+}
+
+
+class CritmcError(RuntimeError):
+    """Error status returned by the C ABI."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"critmc_b200 error {status}: {message}")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    """Load the shared library (once)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            if os.environ.get("CRITMC_B200_NO_BUILD"):
+                raise RuntimeError(f"{LIB_PATH} is missing; build it with python -m critmc_b200._build")
+            from . import _build
+
+            _build.build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(512)
+    lib().critmc_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise CritmcError(status, last_error())
+
+
+def call(name: str, *args) -> int:
+    """Call ``name`` and raise :class:`CritmcError` on a non-zero status."""
+    status = getattr(lib(), name)(*args)
+    check(status)
+    return status

@@ -1,0 +1,126 @@
+// C ABI plumbing shared by all kernels: version, error text, class tables.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "host_common.h"
+
+namespace critmc {
+
+static thread_local char g_error[512] = {0};
+
+void set_error(const char* msg) {
+  std::snprintf(g_error, sizeof(g_error), "%s", msg ? msg : "");
+}
+
+void clear_error() { g_error[0] = 0; }
+
+int cuda_fail(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  std::snprintf(g_error, sizeof(g_error), "%s: %s", what, cudaGetErrorString(e));
+  return CRITMC_ERR_CUDA;
+}
+
+int CaptureStream::begin(void* stream) {
+  user = (cudaStream_t)stream;
+  if (user != nullptr && user != cudaStreamLegacy && user != cudaStreamPerThread) {
+    work = user;
+    private_stream = false;
+    return CRITMC_OK;
+  }
+  static thread_local cudaStream_t priv = nullptr;
+  if (!priv && cudaStreamCreateWithFlags(&priv, cudaStreamNonBlocking) != cudaSuccess)
+    return cuda_fail("stream create");
+  work = priv;
+  private_stream = true;
+  cudaEvent_t ev;
+  if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
+  cudaEventRecord(ev, user);
+  cudaStreamWaitEvent(work, ev, 0);
+  cudaEventDestroy(ev);
+  return CRITMC_OK;
+}
+
+int CaptureStream::finish() {
+  if (!private_stream) return CRITMC_OK;
+  cudaEvent_t ev;
+  if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
+  cudaEventRecord(ev, work);
+  cudaStreamWaitEvent(user, ev, 0);
+  cudaEventDestroy(ev);
+  return CRITMC_OK;
+}
+
+}  // namespace critmc
+
+using namespace critmc;
+
+extern "C" int32_t critmc_version(void) { return 100; }
+
+extern "C" int32_t critmc_last_error(char* buf, int32_t size) {
+  if (!buf || size <= 0) return CRITMC_ERR_INVALID;
+  std::snprintf(buf, (size_t)size, "%s", g_error);
+  return CRITMC_OK;
+}
+
+// p -> (kind, thr) with thr = round(p 2^32)
+static void classify_p(double p, uint32_t& kind, uint32_t& thr) {
+  if (!(p > 0.0)) {  // also NaN
+    kind = CRITMC_KIND_NEVER;
+    thr = 0;
+    return;
+  }
+  if (p >= 1.0) {
+    kind = CRITMC_KIND_ALWAYS;
+    thr = 0;
+    return;
+  }
+  const double t = std::nearbyint(std::ldexp(p, 32));
+  if (t >= 4294967296.0) {
+    kind = CRITMC_KIND_ALWAYS;
+    thr = 0;
+  } else if (t <= 0.0) {
+    kind = CRITMC_KIND_NEVER;
+    thr = 0;
+  } else {
+    kind = CRITMC_KIND_RANDOM;
+    thr = (uint32_t)t;
+  }
+}
+
+extern "C" int32_t critmc_ising_class_table(int32_t algo, int32_t z, double beta, double h,
+                                            uint32_t* kind, uint32_t* thr,
+                                            int32_t* spin_dependent) {
+  clear_error();
+  if (!kind || !thr) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (z < 1 || z > 7) return fail(CRITMC_ERR_INVALID, "coordination number must be in [1, 7]");
+  if (!std::isfinite(beta) || !std::isfinite(h)) return fail(CRITMC_ERR_INVALID, "beta and h must be finite");
+  for (int c = 0; c < CRITMC_NCLS; ++c) {
+    kind[c] = CRITMC_KIND_NEVER;
+    thr[c] = 0;
+  }
+  int dep = 0;
+  for (int v = 0; v <= z; ++v) {
+    for (int sb = 0; sb < 2; ++sb) {
+      const double spin = sb ? 1.0 : -1.0;
+      double p;
+      if (algo == CRITMC_METROPOLIS) {
+        // v anti-aligned neighbours: a = s * sum_j s_j = z - 2v; dE = 2a + 2 h s
+        // (critmc kernels/ising.py:48-57)
+        const double a = (double)(z - 2 * v);
+        const double d_e = 2.0 * a + 2.0 * h * spin;
+        p = d_e <= 0.0 ? 1.0 : std::exp(-beta * d_e);
+      } else if (algo == CRITMC_HEATBATH) {
+        // v neighbours up: sum_j s_j = 2v - z (critmc kernels/ising.py:60-65)
+        const double field = (double)(2 * v - z);
+        p = 1.0 / (1.0 + std::exp(-2.0 * beta * (field + h)));
+      } else {
+        return fail(CRITMC_ERR_UNSUPPORTED, "class tables exist for metropolis and heatbath");
+      }
+      classify_p(p, kind[2 * v + sb], thr[2 * v + sb]);
+    }
+    if (kind[2 * v] != kind[2 * v + 1] || thr[2 * v] != thr[2 * v + 1]) dep = 1;
+  }
+  if (spin_dependent) *spin_dependent = dep;
+  return CRITMC_OK;
+}

@@ -1,0 +1,91 @@
+// Device helpers shared by every sampler kernel of the library.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "philox.h"
+#include "critmc_b200.h"
+
+namespace critmc {
+
+// ---------------------------------------------------------------------------
+// Bit-sliced arithmetic on 32 independent lanes (one lane per bit).
+// ---------------------------------------------------------------------------
+
+// three-input boolean function with a compile-time truth table
+template <unsigned LUT>
+__device__ __forceinline__ uint32_t lop3(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("lop3.b32 %0, %1, %2, %3, %4;" : "=r"(d) : "r"(a), "r"(b), "r"(c), "n"(LUT));
+  return d;
+}
+// truth-table constants for lop3: a = 0xF0, b = 0xCC, c = 0xAA
+constexpr unsigned LA = 0xF0, LB = 0xCC, LC = 0xAA;
+constexpr unsigned lut_xor3 = LA ^ LB ^ LC;
+constexpr unsigned lut_maj = (LA & LB) | (LA & LC) | (LB & LC);
+
+// Per-lane count (0..Z) of the set bits of Z masks, as three bit planes.
+struct Count3 {
+  uint32_t b0, b1, b2;
+};
+
+template <int Z>
+__device__ __forceinline__ Count3 count_bits(const uint32_t* x);
+
+template <>
+__device__ __forceinline__ Count3 count_bits<2>(const uint32_t* x) {
+  return Count3{x[0] ^ x[1], x[0] & x[1], 0u};
+}
+
+template <>
+__device__ __forceinline__ Count3 count_bits<4>(const uint32_t* x) {
+  const uint32_t s1 = x[0] ^ x[1], c1 = x[0] & x[1];
+  const uint32_t s2 = x[2] ^ x[3], c2 = x[2] & x[3];
+  const uint32_t c3 = s1 & s2;
+  return Count3{s1 ^ s2, lop3<lut_xor3>(c1, c2, c3), lop3<lut_maj>(c1, c2, c3)};
+}
+
+template <>
+__device__ __forceinline__ Count3 count_bits<6>(const uint32_t* x) {
+  const uint32_t sa = lop3<lut_xor3>(x[0], x[1], x[2]), ca = lop3<lut_maj>(x[0], x[1], x[2]);
+  const uint32_t sb = lop3<lut_xor3>(x[3], x[4], x[5]), cb = lop3<lut_maj>(x[3], x[4], x[5]);
+  const uint32_t cab = sa & sb;
+  return Count3{sa ^ sb, lop3<lut_xor3>(ca, cb, cab), lop3<lut_maj>(ca, cb, cab)};
+}
+
+// mask of the lanes whose count equals V (compile-time V)
+template <int V>
+__device__ __forceinline__ uint32_t count_eq(const Count3& c) {
+  constexpr unsigned m0 = (V & 1) ? LC : (0xFFu & ~LC);
+  constexpr unsigned m1 = (V & 2) ? LB : (0xFFu & ~LB);
+  constexpr unsigned m2 = (V & 4) ? LA : (0xFFu & ~LA);
+  return lop3<(m0 & m1 & m2)>(c.b2, c.b1, c.b0);
+}
+
+// broadcast bit `bit` of a uniform word to a full lane mask
+__device__ __forceinline__ uint32_t bcast_bit(uint32_t t, int bit) {
+  return 0u - ((t >> bit) & 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long as_ull(long long v) {
+  return static_cast<unsigned long long>(v);
+}
+
+// ---------------------------------------------------------------------------
+// Error reporting from kernels: the first failing kernel writes its code.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void report_error(int* err, int code) {
+  if (err) atomicCAS(err, 0, code);
+}
+
+}  // namespace critmc

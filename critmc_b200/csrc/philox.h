@@ -1,0 +1,100 @@
+/*
+ * Philox4x32-10 counter-based random number generator, host and device.
+ *
+ * Written from the published description: J. K. Salmon, M. A. Moraes,
+ * R. O. Dror and D. E. Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+ * SC'11.  One call maps a 128-bit counter and a 64-bit key to 128 random
+ * bits; ten rounds of the multiply/xor bijection are applied, with the key
+ * bumped by the Weyl constants between rounds.
+ *
+ * The sampler kernels never carry generator state: every random word is a
+ * pure function of (key, counter), so any sub-range of a chain can be
+ * recomputed bit for bit (halo rows of a tile, a CPU replay, a request that
+ * is served alone or batched with others).
+ *
+ * Counter layout used by every kernel in this library:
+ *   c0  unit index (MSC word, site or work item inside the colour class)
+ *   c1  sweep index of the chain (low 32 bits)
+ *   c2  stream tag: purpose | colour | plane group (see CRITMC_TAG_*)
+ *   c3  chain-local extra index (lane quad, PT temperature pair, ...)
+ */
+#ifndef CRITMC_PHILOX_H
+#define CRITMC_PHILOX_H
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define CRITMC_HD __host__ __device__ __forceinline__
+#else
+#define CRITMC_HD static inline
+#endif
+
+#define CRITMC_PHILOX_M0 0xD2511F53u
+#define CRITMC_PHILOX_M1 0xCD9E8D57u
+#define CRITMC_PHILOX_W0 0x9E3779B9u
+#define CRITMC_PHILOX_W1 0xBB67AE85u
+
+#ifndef CRITMC_PHILOX_ROUNDS
+#define CRITMC_PHILOX_ROUNDS 10
+#endif
+
+/* stream tags (counter word c2); bits 0..7 purpose, 8..15 sub-index */
+#define CRITMC_TAG_PLANES 0x01u   /* MSC acceptance planes, sub-index = plane group */
+#define CRITMC_TAG_SITE 0x02u     /* per-site draws (byte/float layouts) */
+#define CRITMC_TAG_SITE2 0x03u    /* per-site extra draws (rejection loops) */
+#define CRITMC_TAG_SWAP 0x04u     /* replica-exchange acceptance */
+#define CRITMC_TAG_INIT 0x05u     /* initial configurations */
+#define CRITMC_TAG_COUPLING 0x06u /* quenched couplings */
+
+typedef struct {
+  uint32_t v[4];
+} critmc_u32x4;
+
+CRITMC_HD uint32_t critmc_mulhi32(uint32_t a, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
+#endif
+}
+
+CRITMC_HD critmc_u32x4 critmc_philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                         uint32_t k0, uint32_t k1) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int r = 0; r < CRITMC_PHILOX_ROUNDS; ++r) {
+    const uint32_t hi0 = critmc_mulhi32(CRITMC_PHILOX_M0, c0);
+    const uint32_t lo0 = CRITMC_PHILOX_M0 * c0;
+    const uint32_t hi1 = critmc_mulhi32(CRITMC_PHILOX_M1, c2);
+    const uint32_t lo1 = CRITMC_PHILOX_M1 * c2;
+    c0 = hi1 ^ c1 ^ k0;
+    c1 = lo1;
+    c2 = hi0 ^ c3 ^ k1;
+    c3 = lo0;
+    k0 += CRITMC_PHILOX_W0;
+    k1 += CRITMC_PHILOX_W1;
+  }
+  critmc_u32x4 out;
+  out.v[0] = c0;
+  out.v[1] = c1;
+  out.v[2] = c2;
+  out.v[3] = c3;
+  return out;
+}
+
+/* uniform double in [0, 1) with 53 random bits from two words */
+CRITMC_HD double critmc_u01_53(uint32_t a, uint32_t b) {
+  const uint64_t m = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
+  return (double)m * (1.0 / 9007199254740992.0);
+}
+
+/* uniform float in (0, 1] with 24 random bits (never 0, safe for logf) */
+CRITMC_HD float critmc_u01f_open0(uint32_t a) {
+  return (float)((a >> 8) + 1u) * (1.0f / 16777216.0f);
+}
+
+/* uniform float in [0, 1) with 24 random bits */
+CRITMC_HD float critmc_u01f(uint32_t a) { return (float)(a >> 8) * (1.0f / 16777216.0f); }
+
+#endif /* CRITMC_PHILOX_H */

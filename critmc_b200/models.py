@@ -1,0 +1,358 @@
+"""Spin models whose chains advance on the GPU.
+
+Mirrors critmc ``src/critmc/models.py``: a model is a stateless description
+(Hamiltonian on a lattice) that knows how to create states, which update
+moves it supports, how to advance a chain, and how to derive per-site
+observables (``derive``, critmc models.py:325-351).  The difference is where
+the chain lives: ``to_device`` moves a configuration into the device layout
+and ``advance`` runs the schedule there through the C ABI, returning the same
+raw streams, keys and dtypes as critmc's numba ``run`` kernels.
+
+Conventions (J = k_B = 1): Ising ``H = -sum s_i s_j - h sum s_i``,
+Potts ``H = -sum delta(s_i, s_j)``, O(n) ``H = -sum S_i . S_j``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from abc import ABC, abstractmethod
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import empty_bytes, ptr, require_cuda, stream_handle, to_dev, to_host
+from .layout import msc_pack, msc_unpack
+from .lattice import Lattice, make_lattice
+from .rng import philox_key
+
+__all__ = ["Model", "Ising", "Potts", "ON", "XY", "Heisenberg", "build_model", "derive",
+           "UPDATE_CODES", "N_AUX"]
+
+# critmc kernels/common.py:16-31
+METROPOLIS, METROPOLIS_RANDOM, HEATBATH, WOLFF, SWENDSEN_WANG, OVERRELAX = 0, 1, 2, 3, 4, 5
+UPDATE_CODES = {
+    "metropolis": METROPOLIS,
+    "metropolis-random": METROPOLIS_RANDOM,
+    "heatbath": HEATBATH,
+    "wolff": WOLFF,
+    "sw": SWENDSEN_WANG,
+    "swendsen-wang": SWENDSEN_WANG,
+    "overrelax": OVERRELAX,
+}
+AUX_ACCEPTED, AUX_WOLFF_SIZE, AUX_SW_C2, AUX_SW_NCLUSTERS = 0, 1, 2, 3
+N_AUX = 4
+
+# moves of critmc that are not data-parallel sweeps and stay on its CPU path
+_NOT_ON_GPU = {
+    "metropolis-random": "random-site Metropolis is a sequential walk, not a checkerboard sweep",
+    "wolff": "cluster updates are not part of the checkerboard sampling path",
+    "sw": "cluster updates are not part of the checkerboard sampling path",
+    "swendsen-wang": "cluster updates are not part of the checkerboard sampling path",
+}
+
+
+def _checkerboard_shape(lattice: Lattice) -> tuple[int, ...]:
+    if not lattice.hypercubic:
+        raise ValueError(
+            f"{lattice!r}: the GPU sweeps are checkerboard sweeps and need a bipartite "
+            "hypercubic lattice (chain, square, cubic)"
+        )
+    if not lattice.bipartite:
+        raise ValueError(f"{lattice!r}: checkerboard sweeps need every extent to be even")
+    if lattice.dim > 3:
+        raise ValueError("lattices of dimension > 3 are not supported on the GPU")
+    return lattice.shape
+
+
+class Model(ABC):
+    """Base class of the GPU spin models (critmc models.py:32-92)."""
+
+    kind: str = ""
+    updates: tuple[str, ...] = ()
+
+    def __init__(self, lattice: Lattice):
+        self.lattice = lattice
+
+    @property
+    def n_sites(self) -> int:
+        return self.lattice.n_sites
+
+    @abstractmethod
+    def initial_state(self, start: str, rng: np.random.Generator) -> np.ndarray: ...
+
+    @abstractmethod
+    def energy(self, state: np.ndarray) -> float: ...
+
+    @abstractmethod
+    def begin(self, state: np.ndarray) -> dict[str, Any]: ...
+
+    @abstractmethod
+    def to_device(self, state: np.ndarray, rng: np.random.Generator, device=None): ...
+
+    @abstractmethod
+    def advance(self, chain, running: dict[str, Any], beta: float, schedule: np.ndarray,
+                n_meas: int) -> dict[str, np.ndarray]: ...
+
+    def check_updates(self, names: list[str]) -> None:
+        bad = [n for n in names if n not in self.updates]
+        if bad:
+            why = "; ".join(f"{n}: {_NOT_ON_GPU[n]}" for n in bad if n in _NOT_ON_GPU)
+            raise ValueError(
+                f"{type(self).__name__} does not support updates {bad} on the GPU; "
+                f"available: {list(self.updates)}" + (f" ({why})" if why else "")
+            )
+
+    def spec(self) -> dict[str, Any]:
+        return {"model": self.kind, "lattice": self.lattice.name, "L": self.lattice.L}
+
+    def meta(self) -> dict[str, Any]:
+        return {**self.spec(), "N": self.n_sites, "dim": self.lattice.dim,
+                "n_bonds": self.lattice.n_bonds}
+
+    def __repr__(self) -> str:
+        return f"{type(self).__name__}({self.lattice!r})"
+
+
+def _msc_ok(shape: tuple[int, ...]) -> bool:
+    lx = shape[0]
+    wc = lx // 64
+    return len(shape) in (2, 3) and lx % 64 == 0 and wc & (wc - 1) == 0
+
+
+class _IsingMscChain:
+    """One Ising chain in the multi-spin-coded layout."""
+
+    def __init__(self, model: "Ising", state: np.ndarray, key: np.ndarray, device):
+        self.device = require_cuda(device)
+        self.shape = model.lattice.shape
+        self.dims = tuple(self.shape) + (1,) * (3 - len(self.shape))
+        self.words = to_dev(msc_pack(state, self.shape), self.device)
+        self.key = np.asarray(key, dtype=np.uint32)
+        self.keys = to_dev(self.key.reshape(1, 2), self.device)
+        self.sweep = 0
+        self.mode = 0
+        self.k_inline = 8
+
+    def fetch(self) -> np.ndarray:
+        return msc_unpack(to_host(self.words, np.uint32), self.shape)
+
+
+class Ising(Model):
+    """Ising model with uniform field ``h`` (critmc models.py:95-162)."""
+
+    kind = "ising"
+    updates = ("metropolis", "heatbath")
+
+    def __init__(self, lattice: Lattice, h: float = 0.0):
+        super().__init__(lattice)
+        self.h = float(h)
+        if not math.isfinite(self.h):
+            raise ValueError(f"field h must be finite, got {h}")
+
+    def initial_state(self, start, rng):
+        n = self.n_sites
+        if start == "random":
+            return (2 * rng.integers(0, 2, size=n) - 1).astype(np.int8)
+        if start in ("ordered", "up"):
+            return np.ones(n, dtype=np.int8)
+        if start == "down":
+            return -np.ones(n, dtype=np.int8)
+        raise ValueError(f"unknown start {start!r}")
+
+    def bond_energy(self, state) -> int:
+        s = np.asarray(state, dtype=np.int64)
+        b = self.lattice.bonds
+        return int(-np.sum(s[b[:, 0]] * s[b[:, 1]]))
+
+    def energy(self, state):
+        return float(self.bond_energy(state)) - self.h * float(np.asarray(state, dtype=np.int64).sum())
+
+    def begin(self, state):
+        return {"e_b": self.bond_energy(state), "m": int(np.asarray(state, dtype=np.int64).sum())}
+
+    def tables(self, beta: float) -> tuple[np.ndarray, int]:
+        """``(2, 2, 16)`` uint32 class tables (metropolis, heat bath) and the spin flag."""
+        z = self.lattice.z
+        out = np.zeros((2, 2, 16), dtype=np.uint32)
+        dep = 0
+        for slot, algo in enumerate((METROPOLIS, HEATBATH)):
+            flag = ctypes.c_int32(0)
+            _lib.call("critmc_ising_class_table", algo, z, float(beta), self.h,
+                      out[slot, 0].ctypes.data, out[slot, 1].ctypes.data, ctypes.byref(flag))
+            if algo == METROPOLIS:
+                dep = flag.value
+        return out, dep
+
+    def to_device(self, state, rng, device=None):
+        shape = _checkerboard_shape(self.lattice)
+        key = philox_key(rng)
+        if _msc_ok(shape):
+            return _IsingMscChain(self, np.asarray(state, dtype=np.int8), key, device)
+        from .byte_models import IsingByteChain
+
+        return IsingByteChain(self, np.asarray(state, dtype=np.int8), key, device)
+
+    def advance(self, chain, running, beta, schedule, n_meas):
+        if not isinstance(chain, _IsingMscChain):
+            return chain.advance(running, beta, schedule, n_meas)
+        dev = chain.device
+        tables, _ = self.tables(beta)
+        sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+        run = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
+        e = torch.empty((1, n_meas), dtype=torch.int64, device=dev)
+        m = torch.empty((1, n_meas), dtype=torch.int64, device=dev)
+        aux = torch.empty((1, n_meas, N_AUX), dtype=torch.int64, device=dev)
+        scratch = empty_bytes(_lib.lib().critmc_ising_msc_scratch_bytes(1, n_meas), dev)
+        lx, ly, lz = chain.dims
+        _lib.call("critmc_ising_msc_run", ptr(chain.words), len(chain.shape), lx, ly, lz, 1,
+                  ptr(chain.keys), tables.ctypes.data, 1, chain.sweep, sched.ctypes.data, len(sched),
+                  n_meas, ptr(run), ptr(e), ptr(m), ptr(aux), ptr(scratch), chain.mode,
+                  chain.k_inline, stream_handle(dev))
+        chain.sweep += int(sched[:, 1].sum()) * n_meas
+        r = to_host(run)[0]
+        running["e_b"], running["m"] = int(r[0]), int(r[1])
+        e_b = to_host(e)[0]
+        mm = to_host(m)[0]
+        energy = e_b - self.h * mm if self.h != 0.0 else e_b
+        return {"E": energy, "Eb": e_b, "M": mm, "aux": to_host(aux)[0]}
+
+    def spec(self):
+        return {**super().spec(), "h": self.h}
+
+
+class Potts(Model):
+    """q-state Potts model (critmc models.py:165-222)."""
+
+    kind = "potts"
+    updates = ("metropolis", "heatbath")
+
+    def __init__(self, lattice: Lattice, q: int):
+        super().__init__(lattice)
+        if q < 2 or q > 127:
+            raise ValueError(f"q must be in [2, 127], got {q}")
+        self.q = int(q)
+
+    def initial_state(self, start, rng):
+        n = self.n_sites
+        if start == "random":
+            return rng.integers(0, self.q, size=n).astype(np.int8)
+        if start in ("ordered", "up"):
+            return np.zeros(n, dtype=np.int8)
+        raise ValueError(f"unknown start {start!r}")
+
+    def bond_energy(self, state) -> int:
+        s = np.asarray(state)
+        b = self.lattice.bonds
+        return int(-np.sum(s[b[:, 0]] == s[b[:, 1]]))
+
+    def energy(self, state):
+        return float(self.bond_energy(state))
+
+    def begin(self, state):
+        counts = np.bincount(np.asarray(state, dtype=np.int64), minlength=self.q).astype(np.int64)
+        return {"energy": self.bond_energy(state), "counts": counts}
+
+    def to_device(self, state, rng, device=None):
+        _checkerboard_shape(self.lattice)
+        from .byte_models import PottsChain
+
+        return PottsChain(self, np.asarray(state, dtype=np.int8), philox_key(rng), device)
+
+    def advance(self, chain, running, beta, schedule, n_meas):
+        return chain.advance(running, beta, schedule, n_meas)
+
+    def spec(self):
+        return {**super().spec(), "q": self.q}
+
+
+class ON(Model):
+    """Classical O(n) vector model with unit spins (critmc models.py:225-299)."""
+
+    kind = "on"
+    updates = ("metropolis", "heatbath", "overrelax")
+
+    def __init__(self, lattice: Lattice, n: int):
+        super().__init__(lattice)
+        if n < 2:
+            raise ValueError(f"n must be at least 2, got {n} (n = 1 is the Ising model)")
+        if n > 3:
+            raise ValueError("the GPU O(n) kernels handle n = 2 (XY) and n = 3 (Heisenberg)")
+        self.n = int(n)
+
+    def initial_state(self, start, rng):
+        if start == "random":
+            s = rng.standard_normal((self.n_sites, self.n))
+            s /= np.linalg.norm(s, axis=1, keepdims=True)
+            return s
+        if start in ("ordered", "up"):
+            s = np.zeros((self.n_sites, self.n))
+            s[:, 0] = 1.0
+            return s
+        raise ValueError(f"unknown start {start!r}")
+
+    def energy(self, state):
+        s = np.asarray(state, dtype=np.float64)
+        b = self.lattice.bonds
+        return float(-np.sum(s[b[:, 0]] * s[b[:, 1]]))
+
+    def begin(self, state):
+        return {"step": 1.0}
+
+    def to_device(self, state, rng, device=None):
+        _checkerboard_shape(self.lattice)
+        from .on_models import ONChain
+
+        return ONChain(self, np.asarray(state, dtype=np.float64), philox_key(rng), device)
+
+    def advance(self, chain, running, beta, schedule, n_meas):
+        return chain.advance(running, beta, schedule, n_meas)
+
+    def spec(self):
+        return {**super().spec(), "n": self.n}
+
+
+def XY(lattice: Lattice) -> ON:
+    return ON(lattice, 2)
+
+
+def Heisenberg(lattice: Lattice) -> ON:
+    return ON(lattice, 3)
+
+
+def build_model(spec: dict[str, Any]) -> Model:
+    lattice = make_lattice(spec["lattice"], int(spec["L"]))
+    kind = spec["model"]
+    if kind == "ising":
+        return Ising(lattice, h=float(spec.get("h", 0.0)))
+    if kind == "potts":
+        return Potts(lattice, int(spec["q"]))
+    if kind == "on":
+        return ON(lattice, int(spec["n"]))
+    raise ValueError(f"unknown model kind {kind!r}")
+
+
+def derive(raw: dict[str, np.ndarray], meta: dict[str, Any]) -> dict[str, np.ndarray]:
+    """Per-site observables from raw streams (critmc models.py:325-351)."""
+    n = float(meta["N"])
+    kind = meta["model"]
+    out: dict[str, np.ndarray] = {"e": np.asarray(raw["E"], dtype=np.float64) / n}
+    if kind == "ising":
+        m = raw["M"] / n
+        out["m"] = m
+        out["m2"] = m * m
+    elif kind == "potts":
+        q = int(meta["q"])
+        rho = raw["counts"] / n
+        out["m2"] = np.clip((q * np.sum(rho * rho, axis=1) - 1.0) / (q - 1.0), 0.0, None)
+        out["mmax"] = (q * rho.max(axis=1) - 1.0) / (q - 1.0)
+    elif kind == "on":
+        mv = raw["M"] / n
+        out["m2"] = np.sum(mv * mv, axis=1)
+    else:
+        raise ValueError(f"unknown model kind {kind!r}")
+    out["absm"] = np.sqrt(out["m2"])
+    out["m4"] = out["m2"] ** 2
+    return out

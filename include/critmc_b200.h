@@ -1,0 +1,108 @@
+/*
+ * critmc_b200: C ABI of the B200 sampling kernels.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int32 status
+ * (0 = ok, < 0 = error; text via critmc_last_error) and runs asynchronously
+ * on the caller's CUDA stream (passed as void*, NULL = legacy default stream).
+ * Device buffers are allocated by the caller (the Python layer uses torch
+ * tensors); the library allocates nothing except CUDA graph objects.
+ *
+ * The entry points replace the numba `run` kernels of critmc, which execute an
+ * update schedule n_meas times and record the observables after each
+ * application.  Update codes are critmc's (src/critmc/kernels/common.py:16-21).
+ */
+#ifndef CRITMC_B200_H
+#define CRITMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define CRITMC_OK 0
+#define CRITMC_ERR_INVALID (-1)     /* bad argument (checked before any launch) */
+#define CRITMC_ERR_CUDA (-2)        /* CUDA runtime error */
+#define CRITMC_ERR_UNSUPPORTED (-3) /* geometry/update not handled by this kernel */
+#define CRITMC_ERR_TIMEOUT (-4)     /* a bounded device wait ran out */
+#define CRITMC_ERR_CANCELLED (-5)   /* host cancel word was set */
+#define CRITMC_ERR_DEVICE (-6)      /* a kernel flagged an internal inconsistency */
+
+/* ---- update codes (critmc kernels/common.py:16-21) --------------------- */
+#define CRITMC_METROPOLIS 0
+#define CRITMC_METROPOLIS_RANDOM 1
+#define CRITMC_HEATBATH 2
+#define CRITMC_WOLFF 3
+#define CRITMC_SWENDSEN_WANG 4
+#define CRITMC_OVERRELAX 5
+
+/* ---- aux columns (critmc kernels/common.py:36-40) ---------------------- */
+#define CRITMC_N_AUX 4
+
+/* ---- acceptance classes ---------------------------------------------------
+ * Binary-spin kernels classify each site by a neighbour count v (0..z) and
+ * its own spin bit sb (1 = spin +1).  Class index c = 2*v + sb.  A class is
+ * NEVER (decision 0), ALWAYS (decision 1) or RANDOM: decision = (u < thr)
+ * with u a uniform 32-bit integer.  For Metropolis v counts anti-aligned
+ * neighbours and the decision flips the spin; for heat bath v counts
+ * neighbours equal to +1 and the decision is the new spin (1 = +1).        */
+#define CRITMC_NCLS 16
+#define CRITMC_KIND_NEVER 0u
+#define CRITMC_KIND_ALWAYS 1u
+#define CRITMC_KIND_RANDOM 2u
+
+/* library version (major*10000 + minor*100 + patch) */
+int32_t critmc_version(void);
+
+/* copy the last error message of the calling thread (always NUL-terminated) */
+int32_t critmc_last_error(char* buf, int32_t size);
+
+/* Acceptance table of a binary-spin kernel: kind[16], thr[16].
+ * Metropolis: p = min(1, exp(-beta*(2a + 2h s))), a = s*sum_j s_j
+ *   (critmc kernels/ising.py:48-57 metropolis_table).
+ * Heat bath: p_up = 1/(1 + exp(-2 beta (sum_j s_j + h)))
+ *   (critmc kernels/ising.py:60-65 heatbath_table).
+ * thr = round(p * 2^32); p >= 1 or thr == 2^32 gives ALWAYS, thr == 0 NEVER.
+ * Returns 1 in *spin_dependent when the classes depend on the own spin.   */
+int32_t critmc_ising_class_table(int32_t algo, int32_t z, double beta, double h, uint32_t* kind,
+                                 uint32_t* thr, int32_t* spin_dependent);
+
+/* ---- multi-spin-coded Ising (2D square / 3D cubic, periodic) -------------
+ * Layout of one chain: spins[colour][row][word], colour = (x+y+z)&1,
+ * row = y + ly*z, word k bit j holds the colour's site x = 2*(32k+j) + p with
+ * p = (colour + y + z) & 1; bit value 1 = spin +1.  lx must be a multiple of
+ * 64 with lx/64 a power of two; ly, lz even.  Chains are contiguous:
+ * chain c starts at spins + c * 2 * rows * (lx/64).
+ *
+ * Replaces critmc kernels/ising.py:174-237 `run` (Metropolis and heat-bath
+ * rows of the schedule) with checkerboard sweeps.  Chains come in n_groups
+ * equal groups of consecutive chains (n_groups <= 16) sharing one acceptance
+ * table (one beta, h): tables is a HOST array [n_groups][2][2][16]
+ * (metropolis kind, thr, then heat-bath kind, thr; see
+ * critmc_ising_class_table).  Device inputs: keys[n_chains][2] (Philox key),
+ * running[n_chains][2] (E_b, M, updated in place).  Device outputs:
+ * e_out/m_out[n_chains][n_meas], aux_out[n_chains][n_meas][4].  scratch must
+ * hold critmc_ising_msc_scratch_bytes(n_chains, n_meas) bytes of device
+ * memory.  schedule is a HOST array of n_rows (code, reps) pairs; sweep k of
+ * the call uses sweep index sweep0 + k of every chain.
+ * mode: 0 auto, 1 one launch per half-sweep, 3 = 1 replayed as CUDA graphs.
+ * k_inline: 4 or 8 acceptance planes resolved inline (tuning only; the
+ * results do not depend on it).                                            */
+int64_t critmc_ising_msc_scratch_bytes(int32_t n_chains, int32_t n_meas);
+int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                             int32_t n_chains, const uint32_t* keys, const uint32_t* tables,
+                             int32_t n_groups, uint32_t sweep0, const int64_t* schedule,
+                             int32_t n_rows, int32_t n_meas, int64_t* running, int64_t* e_out,
+                             int64_t* m_out, int64_t* aux_out, void* scratch, int32_t mode,
+                             int32_t k_inline, void* stream);
+
+/* Energy E_b = -sum_<ij> s_i s_j and magnetisation M of MSC chains, written
+ * to out[n_chains][2] (device).  critmc kernels/ising.py:32-45.           */
+int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,
+                                 int32_t lz, int32_t n_chains, int64_t* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRITMC_B200_H */

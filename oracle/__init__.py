@@ -1,0 +1,115 @@
+"""CPU oracle of the critmc_b200 kernels.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, by ``__graft_entry__.smoke()``
+and by the CPU-baseline leg of ``bench.py``.  The library itself never calls
+it.  ``liboracle.so`` is a plain-C restatement of critmc's numba kernels
+(file:line citations in each ``oracle_*.c``) driven by the same Philox
+streams as the GPU kernels, so it reproduces their results bit for bit
+(integer models) or to rounding (O(n) models).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile ``liboracle.so`` with the Makefile next to this file."""
+    res = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        srcs = list(HERE.glob("oracle_*.c")) + [HERE / "oracle.h"]
+        if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(p.stat().st_mtime for p in srcs):
+            build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_U32 = ctypes.c_uint32
+
+
+def _declare(L: ctypes.CDLL) -> None:
+    L.oracle_philox.argtypes = [_P, _P, _P]
+    L.oracle_philox.restype = None
+    L.oracle_ising_table.argtypes = [_I, _I, _D, _D, _P, _P]
+    L.oracle_ising_table.restype = _I
+    L.oracle_ising_bond_energy.argtypes = [_P, _I, _I, _I, _I]
+    L.oracle_ising_bond_energy.restype = ctypes.c_int64
+    L.oracle_ising_msc_run.argtypes = [_P, _I, _I, _I, _I, _P, _P, _U32, _P, _I, _I, _P, _P, _P, _P]
+    L.oracle_ising_msc_run.restype = _I
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def philox(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().oracle_philox(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+def ising_table(algo: int, z: int, beta: float, h: float) -> np.ndarray:
+    """``(2, 16)`` uint32: kind row then thr row."""
+    kind = np.zeros(16, dtype=np.uint32)
+    thr = np.zeros(16, dtype=np.uint32)
+    if lib().oracle_ising_table(algo, z, beta, h, _ptr(kind), _ptr(thr)) != 0:
+        raise ValueError("unsupported algorithm")
+    return np.stack([kind, thr])
+
+
+def ising_bond_energy(s: np.ndarray, shape: tuple[int, ...]) -> int:
+    dims = tuple(shape) + (1,) * (3 - len(shape))
+    s8 = np.ascontiguousarray(s, dtype=np.int8)
+    return int(lib().oracle_ising_bond_energy(_ptr(s8), len(shape), *dims))
+
+
+def ising_msc_run(s, shape, key, beta, h, schedule, n_meas, sweep0=0, running=None):
+    """Replay the MSC checkerboard sweeps on ``s`` (int8, reference site order, modified).
+
+    Returns ``(e_b, m, aux, running)``.
+    """
+    s8 = s if (isinstance(s, np.ndarray) and s.dtype == np.int8 and s.flags["C_CONTIGUOUS"]) else None
+    if s8 is None:
+        raise TypeError("s must be a C-contiguous int8 array (it is updated in place)")
+    dims = tuple(shape) + (1,) * (3 - len(shape))
+    z = 2 * len(shape)
+    tables = np.concatenate([ising_table(0, z, beta, h).ravel(), ising_table(2, z, beta, h).ravel()])
+    tables = np.ascontiguousarray(tables, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+    if running is None:
+        running = np.array([ising_bond_energy(s8, shape), int(s8.astype(np.int64).sum())], dtype=np.int64)
+    running = np.ascontiguousarray(running, dtype=np.int64).copy()
+    e = np.zeros(n_meas, dtype=np.int64)
+    m = np.zeros(n_meas, dtype=np.int64)
+    aux = np.zeros((n_meas, 4), dtype=np.int64)
+    rc = lib().oracle_ising_msc_run(
+        _ptr(s8), len(shape), *dims, _ptr(k), _ptr(tables), sweep0, _ptr(sched), len(sched), n_meas,
+        _ptr(running), _ptr(e), _ptr(m), _ptr(aux),
+    )
+    if rc != 0:
+        raise ValueError(f"oracle_ising_msc_run failed ({rc})")
+    return e, m, aux, running

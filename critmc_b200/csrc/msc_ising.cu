@@ -16,24 +16,30 @@
 namespace critmc {
 
 constexpr int MSC_THREADS = 256;
-constexpr int MSC_WPT = 4;  // words per thread per block
-constexpr int MSC_WPB = MSC_THREADS * MSC_WPT;
+constexpr int MSC_WARPS = MSC_THREADS / 32;
+constexpr int MSC_FIXCAP = 64;     // deferred words per warp before a flush
+constexpr int MSC_PCHAINS = 256;   // chains per launch (their keys travel as kernel parameters)
 
-struct MscFix {
-  uint32_t w, U, s, D;
-};
-
-struct MscHalfArgs {
+// Kernel parameters: keys and tables live in the constant bank, so the Philox
+// key schedule and the threshold broadcasts run on the uniform datapath.
+struct MscParams {
   uint32_t* spins;
-  const uint32_t* keys;
-  unsigned long long* acc;  // [meas][chain][3]
+  unsigned long long* acc;  // [meas][n_chains][3]
   const uint32_t* cursor;   // optional device (sweep base, meas base)
   MscGeom g;
-  int n_chains;
+  int n_chains;             // chains of the call (stride of acc)
+  int chain0;               // first chain of this launch
   int chains_per_group;
   int col;
-  uint32_t sweep;  // absolute sweep (or offset when cursor != null)
-  uint32_t meas;   // measurement slot (or offset when cursor != null)
+  int run;                  // rows walked by one thread
+  uint32_t sweep;           // absolute sweep (or offset when cursor != null)
+  uint32_t meas;            // measurement slot (or offset when cursor != null)
+  uint32_t keys[MSC_PCHAINS][2];
+  MscTables tabs;
+};
+
+struct MscFix {
+  uint32_t w, U, D;
 };
 
 template <int Z>
@@ -49,85 +55,123 @@ __device__ __forceinline__ void msc_row_coords(const MscGeom& g, uint32_t w, int
   }
 }
 
-// grid: x = word blocks of one colour plane, y = chain within group, z = group
+// Finish one deferred word: continue the MSB-first comparison plane group by
+// plane group until every lane is decided, then store it.
+template <int Z, int RULE, int KG>
+__device__ __forceinline__ void msc_fixup(const MscRule<Z, RULE>& rule, const MscGeom& g,
+                                          const MscFix f, uint32_t* own, const uint32_t* other,
+                                          uint32_t col, uint32_t k0, uint32_t k1, uint32_t sweep,
+                                          int& dE, int& dM, int& nacc) {
+  int y, z, k;
+  msc_row_coords<Z>(g, f.w, y, z, k);
+  uint32_t n[Z];
+  msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
+  MscWord w;
+  rule.classify(own[f.w], n, w);
+  w.D = f.D;
+  w.U = f.U;
+  for (int grp = KG; grp < 8 && w.U != 0; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, f.w, sweep, col, grp);
+  const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
+  msc_obs<Z>((w.s ^ s_new) & f.U, w.s, w.anti, dE, dM, nacc);
+  own[f.w] = s_new;
+}
+
+// One colour of one sweep.  grid: x = column/run tiles, y = chain of the launch.
+// Thread t walks `run` consecutive rows of column k = t mod wc.
 template <int Z, int RULE, int KG>
 __global__ void __launch_bounds__(MSC_THREADS)
-    msc_halfsweep_kernel(const MscHalfArgs a, const __grid_constant__ MscTables tabs) {
-  __shared__ MscFix fix[MSC_WPB];
-  __shared__ int nfix;
-  __shared__ int red[3][MSC_THREADS / 32];
+    msc_halfsweep_kernel(const __grid_constant__ MscParams P) {
+  __shared__ MscFix fix[MSC_WARPS][MSC_FIXCAP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lchain = blockIdx.y;
+  const int chain = P.chain0 + lchain;
+  const int group = chain / P.chains_per_group;
+  const MscGeom& g = P.g;
+  const MscRule<Z, RULE> rule{P.tabs.kind[group], P.tabs.thr[group]};
+  const uint32_t k0 = P.keys[lchain][0], k1 = P.keys[lchain][1];
+  const uint32_t sweep = P.cursor ? P.cursor[0] + P.sweep : P.sweep;
+  const uint32_t meas = P.cursor ? P.cursor[1] + P.meas : P.meas;
+  const uint32_t col = (uint32_t)P.col;
+  uint32_t* own = P.spins + (size_t)chain * 2 * g.words + (size_t)col * g.words;
+  const uint32_t* other = P.spins + (size_t)chain * 2 * g.words + (size_t)(col ^ 1) * g.words;
 
-  const int group = blockIdx.z;
-  const int chain = group * a.chains_per_group + blockIdx.y;
-  const int tid = threadIdx.x;
-  const MscGeom& g = a.g;
-  if (tid == 0) nfix = 0;
-  __syncthreads();
-
-  MscRule<Z, RULE> rule{tabs.kind[group], tabs.thr[group]};
-  const uint32_t k0 = a.keys[2 * chain], k1 = a.keys[2 * chain + 1];
-  const uint32_t sweep = a.cursor ? a.cursor[0] + a.sweep : a.sweep;
-  const uint32_t meas = a.cursor ? a.cursor[1] + a.meas : a.meas;
-  const uint32_t col = (uint32_t)a.col;
-
-  uint32_t* own = a.spins + (size_t)chain * 2 * g.words + (size_t)col * g.words;
-  const uint32_t* other = a.spins + (size_t)chain * 2 * g.words + (size_t)(col ^ 1) * g.words;
-
+  const uint32_t t = blockIdx.x * MSC_THREADS + threadIdx.x;
+  const int k = (int)(t & (g.wc - 1));
+  const int r0 = (int)(t >> g.wc_log2) * P.run;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  int nf = 0;  // entries in this warp's list (warp-uniform)
   int dE = 0, dM = 0, nacc = 0;
-  const uint32_t wbase = blockIdx.x * (uint32_t)MSC_WPB;
-#pragma unroll 1
-  for (int j = 0; j < MSC_WPT; ++j) {
-    const uint32_t widx = wbase + j * MSC_THREADS + tid;
-    if (widx >= g.words) break;
-    int y, z, k;
-    msc_row_coords<Z>(g, widx, y, z, k);
-    uint32_t n[Z];
-    msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
-    MscWord w;
-    rule.classify(own[widx], n, w);
-#pragma unroll
-    for (int grp = 0; grp < KG; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, widx, sweep, col, grp);
-    const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
-    msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, dE, dM, nacc);
-    if (w.U == 0) {
-      own[widx] = s_new;
-    } else {
-      const int slot = atomicAdd(&nfix, 1);
-      fix[slot] = MscFix{widx, w.U, w.s, w.D};
+
+  auto flush = [&]() {
+    __syncwarp();
+    for (int e = lane; e < nf; e += 32)
+      msc_fixup<Z, RULE, KG>(rule, g, fix[warp][e], own, other, col, k0, k1, sweep, dE, dM, nacc);
+    __syncwarp();
+    nf = 0;
+  };
+
+  // 2D: sliding window down the column over the other colour
+  uint32_t o_m = 0, o_c = 0;
+  if constexpr (Z == 4) {
+    if (r0 < g.rows) {
+      const int ym = (r0 == 0) ? g.ly - 1 : r0 - 1;
+      o_m = other[(size_t)ym * g.wc + k];
+      o_c = other[(size_t)r0 * g.wc + k];
     }
   }
-  __syncthreads();
-  // deferred lanes: continue the comparison with the next plane groups
-  const int nf = nfix;
-  for (int e = tid; e < nf; e += MSC_THREADS) {
-    const MscFix f = fix[e];
-    int y, z, k;
-    msc_row_coords<Z>(g, f.w, y, z, k);
-    uint32_t n[Z];
-    msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
+#pragma unroll 1
+  for (int i = 0; i < P.run; ++i) {
+    const int r = r0 + i;
+    const bool valid = r < g.rows;
+    const uint32_t widx = (uint32_t)r * g.wc + k;
     MscWord w;
-    rule.classify(f.s, n, w);
-    w.D = f.D;
-    w.U = f.U;
-    for (int grp = KG; grp < 8 && w.U != 0; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, f.w, sweep, col, grp);
-    const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (f.s ^ w.D);
-    msc_obs<Z>((f.s ^ s_new) & f.U, f.s, w.anti, dE, dM, nacc);
-    own[f.w] = s_new;
+    w.U = 0;
+    uint32_t s_new = 0;
+    if (valid) {
+      uint32_t n[Z];
+      if constexpr (Z == 4) {
+        const int y = r;
+        const int yp = (y == g.ly - 1) ? 0 : y + 1;
+        const uint32_t o_p = other[(size_t)yp * g.wc + k];
+        const int p = (P.col + y) & 1;
+        const int ka = p ? ((k == g.wc - 1) ? 0 : k + 1) : ((k == 0) ? g.wc - 1 : k - 1);
+        const uint32_t adj = other[(size_t)y * g.wc + ka];
+        n[0] = o_c;
+        n[1] = p ? __funnelshift_r(o_c, adj, 1) : __funnelshift_l(adj, o_c, 1);
+        n[2] = o_m;
+        n[3] = o_p;
+        o_m = o_c;
+        o_c = o_p;
+      } else {
+        int y, z, kk;
+        msc_row_coords<Z>(g, widx, y, z, kk);
+        msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
+      }
+      rule.classify(own[widx], n, w);
+#pragma unroll
+      for (int grp = 0; grp < KG; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, widx, sweep, col, grp);
+      s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
+      msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, dE, dM, nacc);
+      if (w.U == 0) own[widx] = s_new;
+    }
+    const uint32_t need = __ballot_sync(0xffffffffu, w.U != 0);
+    if (need) {
+      const int cnt = __popc(need);
+      if (nf + cnt > MSC_FIXCAP) flush();
+      if (w.U != 0) fix[warp][nf + __popc(need & lt_mask)] = MscFix{widx, w.U, w.D};
+      nf += cnt;
+    }
   }
-  // block reduction of the observable increments
+  if (nf) flush();
+  // observable increments: warp reduction, one atomic per quantity and warp
   dE = warp_sum(dE);
   dM = warp_sum(dM);
   nacc = warp_sum(nacc);
-  if ((tid & 31) == 0) {
-    red[0][tid >> 5] = dE;
-    red[1][tid >> 5] = dM;
-    red[2][tid >> 5] = nacc;
-  }
-  __syncthreads();
-  if (tid < 3 && a.acc) {
-    long long v = 0;
-    for (int q = 0; q < MSC_THREADS / 32; ++q) v += red[tid][q];
-    atomicAdd(a.acc + ((size_t)meas * a.n_chains + chain) * 3 + tid, as_ull(v));
+  if (lane == 0 && P.acc) {
+    unsigned long long* dst = P.acc + ((size_t)meas * P.n_chains + chain) * 3;
+    if (dE) atomicAdd(dst + 0, as_ull(dE));
+    if (dM) atomicAdd(dst + 1, as_ull(dM));
+    if (nacc) atomicAdd(dst + 2, as_ull(nacc));
   }
 }
 
@@ -272,28 +316,32 @@ int msc_pick_rule(const uint32_t* kind, const uint32_t* thr, int z, int algo, in
 }
 
 template <int Z, int RULE>
-static void launch_half_kg(const MscHalfArgs& a, const MscTables& t, int n_groups, int kg,
-                           cudaStream_t st) {
-  const dim3 grid((a.g.words + MSC_WPB - 1) / MSC_WPB, a.chains_per_group, n_groups);
-  if (kg == 1) msc_halfsweep_kernel<Z, RULE, 1><<<grid, MSC_THREADS, 0, st>>>(a, t);
-  else msc_halfsweep_kernel<Z, RULE, 2><<<grid, MSC_THREADS, 0, st>>>(a, t);
+static void launch_half_kg(const MscParams& P, int kg, cudaStream_t st) {
+  const long long threads = (long long)P.g.wc * ((P.g.rows + P.run - 1) / P.run);
+  const dim3 grid((unsigned)((threads + MSC_THREADS - 1) / MSC_THREADS), P.n_chains - P.chain0 < MSC_PCHAINS ? P.n_chains - P.chain0 : MSC_PCHAINS);
+  if (kg == 1) msc_halfsweep_kernel<Z, RULE, 1><<<grid, MSC_THREADS, 0, st>>>(P);
+  else msc_halfsweep_kernel<Z, RULE, 2><<<grid, MSC_THREADS, 0, st>>>(P);
 }
 
 template <int Z>
-static void launch_half_z(const MscHalfArgs& a, const MscTables& t, int n_groups, int rule, int kg,
-                          cudaStream_t st) {
+static void launch_half_z(const MscParams& P, int rule, int kg, cudaStream_t st) {
   switch (rule) {
-    case RULE_METRO0: launch_half_kg<Z, RULE_METRO0>(a, t, n_groups, kg, st); break;
-    case RULE_HB0: launch_half_kg<Z, RULE_HB0>(a, t, n_groups, kg, st); break;
-    case RULE_GEN: launch_half_kg<Z, RULE_GEN>(a, t, n_groups, kg, st); break;
-    default: launch_half_kg<Z, RULE_GENSPIN>(a, t, n_groups, kg, st); break;
+    case RULE_METRO0: launch_half_kg<Z, RULE_METRO0>(P, kg, st); break;
+    case RULE_HB0: launch_half_kg<Z, RULE_HB0>(P, kg, st); break;
+    case RULE_GEN: launch_half_kg<Z, RULE_GEN>(P, kg, st); break;
+    default: launch_half_kg<Z, RULE_GENSPIN>(P, kg, st); break;
   }
 }
 
-void msc_launch_half(const MscHalfArgs& a, const MscTables& t, int n_groups, int rule, int kg,
-                     cudaStream_t st) {
-  if (a.g.dim == 2) launch_half_z<4>(a, t, n_groups, rule, kg, st);
-  else launch_half_z<6>(a, t, n_groups, rule, kg, st);
+// One half-sweep of every chain, in launches of at most MSC_PCHAINS chains.
+void msc_launch_half(MscParams& P, const uint32_t* keys, int rule, int kg, cudaStream_t st) {
+  for (int c0 = 0; c0 < P.n_chains; c0 += MSC_PCHAINS) {
+    P.chain0 = c0;
+    const int nc = std::min(MSC_PCHAINS, P.n_chains - c0);
+    std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
+    if (P.g.dim == 2) launch_half_z<4>(P, rule, kg, st);
+    else launch_half_z<6>(P, rule, kg, st);
+  }
 }
 
 }  // namespace critmc
@@ -360,27 +408,38 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
   if (cudaMemsetAsync(acc, 0, (size_t)n_chains * n_meas * 3 * 8, s) != cudaSuccess)
     return cuda_fail("memset");
 
-  MscHalfArgs a;
-  a.spins = spins;
-  a.keys = keys;
-  a.acc = acc;
-  a.g = g;
-  a.n_chains = n_chains;
-  a.chains_per_group = n_chains / n_groups;
+  // rows walked per thread: long runs reuse the sliding window, short runs
+  // keep enough threads in flight when few chains are batched
+  const long long col_threads = (long long)n_chains * g.wc * g.rows;
+  int run = 8;
+  while (run > 1 && col_threads / run < 148LL * 1536) run /= 2;
+
+  static thread_local MscParams P[2];
+  for (int slot = 0; slot < 2; ++slot) {
+    MscParams& q = P[slot];
+    q.spins = spins;
+    q.acc = acc;
+    q.g = g;
+    q.n_chains = n_chains;
+    q.chains_per_group = n_chains / n_groups;
+    q.run = run;
+    q.tabs = tabs[slot];
+  }
   const int kg = k_inline / 4;
 
   auto launch_meas = [&](uint32_t sweep_rel, uint32_t meas_rel, const uint32_t* cur) {
-    a.cursor = cur;
     uint32_t sw = sweep_rel;
     for (int r = 0; r < n_rows; ++r) {
       const int slot = schedule[2 * r] == CRITMC_HEATBATH ? 1 : 0;
+      MscParams& q = P[slot];
+      q.cursor = cur;
       for (int64_t rep = 0; rep < schedule[2 * r + 1]; ++rep) {
-        a.sweep = sw;
-        a.meas = meas_rel;
-        a.col = 0;
-        msc_launch_half(a, tabs[slot], n_groups, rule[slot], kg, s);
-        a.col = 1;
-        msc_launch_half(a, tabs[slot], n_groups, rule[slot], kg, s);
+        q.sweep = sw;
+        q.meas = meas_rel;
+        q.col = 0;
+        msc_launch_half(q, keys, rule[slot], kg, s);
+        q.col = 1;
+        msc_launch_half(q, keys, rule[slot], kg, s);
         ++sw;
       }
     }

@@ -138,6 +138,37 @@ struct MscRule {
     }
   }
 
+  // number of threshold classes the specialised rules read per plane
+  static constexpr int NR = (RULE == RULE_METRO0) ? (Z / 2) : (RULE == RULE_HB0) ? (Z + 1) : 0;
+
+  // broadcast threshold bits of the first 4*KG planes, computed once per thread
+  template <int KG>
+  __device__ __forceinline__ void prepare(uint32_t (&pre)[4 * KG][NR > 0 ? NR : 1]) const {
+#pragma unroll
+    for (int q = 0; q < 4 * KG; ++q)
+#pragma unroll
+      for (int v = 0; v < NR; ++v) pre[q][v] = bcast_bit(thr[2 * v], 31 - q);
+  }
+
+  // threshold bit plane from precomputed broadcasts (specialised rules)
+  __device__ __forceinline__ uint32_t tbits_pre(const MscWord& w, const uint32_t* B) const {
+    const Count3& c = w.cnt;
+    if constexpr (RULE == RULE_METRO0) {
+      const uint32_t lo = mux(c.b0, B[1], B[0]);
+      if constexpr (Z == 6) return mux(c.b1, B[2], lo);
+      return lo;
+    } else {
+      const uint32_t m10 = mux(c.b0, B[1], B[0]);
+      if constexpr (Z == 2) return mux(c.b1, B[2], m10);
+      const uint32_t m32 = mux(c.b0, B[3], B[2]);
+      const uint32_t lo = mux(c.b1, m32, m10);
+      if constexpr (Z == 4) return mux(c.b2, B[4], lo);
+      const uint32_t m54 = mux(c.b0, B[5], B[4]);
+      const uint32_t hi = mux(c.b1, B[6], m54);
+      return mux(c.b2, hi, lo);
+    }
+  }
+
   // threshold bit plane of bit `bit` (31 = most significant) for the lanes of w
   __device__ __forceinline__ uint32_t tbits(const MscWord& w, int bit) const {
     const Count3& c = w.cnt;
@@ -175,15 +206,21 @@ struct MscRule {
 };
 
 // Resolve plane group `grp` (planes 4 grp .. 4 grp + 3) for the undecided lanes.
+// pre: broadcast threshold bits of these four planes (pre[q * NR + v]) or null.
 template <int Z, int RULE>
 __device__ __forceinline__ void msc_group(const MscRule<Z, RULE>& rule, MscWord& w, uint32_t k0,
                                           uint32_t k1, uint32_t widx, uint32_t sweep, uint32_t col,
-                                          int grp) {
+                                          int grp, const uint32_t* pre = nullptr) {
   const critmc_u32x4 r = critmc_philox4x32(
       widx, sweep, CRITMC_TAG_PLANES | ((uint32_t)grp << 8) | (col << 16), 0u, k0, k1);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const uint32_t t = rule.tbits(w, 31 - (4 * grp + q));
+    uint32_t t;
+    if constexpr (MscRule<Z, RULE>::NR > 0) {
+      t = pre ? rule.tbits_pre(w, pre + q * MscRule<Z, RULE>::NR) : rule.tbits(w, 31 - (4 * grp + q));
+    } else {
+      t = rule.tbits(w, 31 - (4 * grp + q));
+    }
     w.D |= w.U & t & ~r.v[q];
     w.U &= ~(r.v[q] ^ t);
   }

@@ -50,28 +50,19 @@ typedef struct {
   uint32_t v[4];
 } critmc_u32x4;
 
-CRITMC_HD uint32_t critmc_mulhi32(uint32_t a, uint32_t b) {
-#if defined(__CUDA_ARCH__)
-  return __umulhi(a, b);
-#else
-  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
-#endif
-}
-
 CRITMC_HD critmc_u32x4 critmc_philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
                                          uint32_t k0, uint32_t k1) {
 #if defined(__CUDA_ARCH__)
 #pragma unroll
 #endif
   for (int r = 0; r < CRITMC_PHILOX_ROUNDS; ++r) {
-    const uint32_t hi0 = critmc_mulhi32(CRITMC_PHILOX_M0, c0);
-    const uint32_t lo0 = CRITMC_PHILOX_M0 * c0;
-    const uint32_t hi1 = critmc_mulhi32(CRITMC_PHILOX_M1, c2);
-    const uint32_t lo1 = CRITMC_PHILOX_M1 * c2;
-    c0 = hi1 ^ c1 ^ k0;
-    c1 = lo1;
-    c2 = hi0 ^ c3 ^ k1;
-    c3 = lo0;
+    /* one 32x32->64 product per lane word: a single wide multiply-add on the GPU */
+    const uint64_t p0 = (uint64_t)CRITMC_PHILOX_M0 * c0;
+    const uint64_t p1 = (uint64_t)CRITMC_PHILOX_M1 * c2;
+    c0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    c1 = (uint32_t)p1;
+    c2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    c3 = (uint32_t)p0;
     k0 += CRITMC_PHILOX_W0;
     k1 += CRITMC_PHILOX_W1;
   }

@@ -130,8 +130,7 @@ class _IsingMscChain:
         self.shape = model.lattice.shape
         self.dims = tuple(self.shape) + (1,) * (3 - len(self.shape))
         self.words = to_dev(msc_pack(state, self.shape), self.device)
-        self.key = np.asarray(key, dtype=np.uint32)
-        self.keys = to_dev(self.key.reshape(1, 2), self.device)
+        self.key = np.ascontiguousarray(key, dtype=np.uint32).reshape(1, 2)
         self.sweep = 0
         self.mode = 0
         self.k_inline = 8
@@ -208,7 +207,7 @@ class Ising(Model):
         scratch = empty_bytes(_lib.lib().critmc_ising_msc_scratch_bytes(1, n_meas), dev)
         lx, ly, lz = chain.dims
         _lib.call("critmc_ising_msc_run", ptr(chain.words), len(chain.shape), lx, ly, lz, 1,
-                  ptr(chain.keys), tables.ctypes.data, 1, chain.sweep, sched.ctypes.data, len(sched),
+                  chain.key.ctypes.data, tables.ctypes.data, 1, chain.sweep, sched.ctypes.data, len(sched),
                   n_meas, ptr(run), ptr(e), ptr(m), ptr(aux), ptr(scratch), chain.mode,
                   chain.k_inline, stream_handle(dev))
         chain.sweep += int(sched[:, 1].sum()) * n_meas

@@ -80,8 +80,8 @@ int32_t critmc_ising_class_table(int32_t algo, int32_t z, double beta, double h,
  * equal groups of consecutive chains (n_groups <= 16) sharing one acceptance
  * table (one beta, h): tables is a HOST array [n_groups][2][2][16]
  * (metropolis kind, thr, then heat-bath kind, thr; see
- * critmc_ising_class_table).  Device inputs: keys[n_chains][2] (Philox key),
- * running[n_chains][2] (E_b, M, updated in place).  Device outputs:
+ * critmc_ising_class_table).  keys is a HOST array [n_chains][2] of Philox
+ * keys.  Device inputs: running[n_chains][2] (E_b, M, updated in place).  Device outputs:
  * e_out/m_out[n_chains][n_meas], aux_out[n_chains][n_meas][4].  scratch must
  * hold critmc_ising_msc_scratch_bytes(n_chains, n_meas) bytes of device
  * memory.  schedule is a HOST array of n_rows (code, reps) pairs; sweep k of

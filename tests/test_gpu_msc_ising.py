@@ -77,7 +77,7 @@ def test_msc_batched_chains_match_single_chain_replays(cuda):
     aux = torch.empty((n_chains, n_meas, 4), dtype=torch.int64, device=cuda)
     scratch = empty_bytes(_lib.lib().critmc_ising_msc_scratch_bytes(n_chains, n_meas), cuda)
     sched = np.array([[0, 1]], dtype=np.int64)
-    _lib.call("critmc_ising_msc_run", ptr(words), 2, lx, ly, 1, n_chains, ptr(to_dev(keys, cuda)),
+    _lib.call("critmc_ising_msc_run", ptr(words), 2, lx, ly, 1, n_chains, keys.ctypes.data,
               tables.ctypes.data, 1, 17, sched.ctypes.data, 1, n_meas, ptr(running), ptr(e), ptr(m),
               ptr(aux), ptr(scratch), 3, 8, stream_handle(cuda))
     torch.cuda.synchronize()

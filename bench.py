@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Throughput of the batched checkerboard Ising sampler on B200.
+
+Workload (one "step" = one checkerboard Metropolis sweep of every chain):
+2D Ising, multi-spin-coded uint32, L = 4096, beta in {0.40, 0.4406868, 0.48},
+64 independent chains per beta (192 chains, 3.2e9 sites, 384 MiB of spins:
+far larger than the 126 MB L2, so no L2 flush is needed), hot
+random start, seeds (seed, "ising", L, beta index, chain).
+
+Metric: attempted spin updates per ns (N site visits per sweep).  Extras in
+the same JSON line: heat bath, the plain one-chain-per-launch path, L = 1024,
+the HBM roofline of the half-sweep kernel, clocks, and a CPU baseline (the C
+oracle on host threads).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: one process per GPU under torch.distributed.run; every rank runs
+its own 192 chains (weak scaling, no collective on the data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L_HEAD = 4096
+BETAS = (0.40, 0.4406868, 0.48)
+CHAINS_PER_BETA = 64
+BYTES_PER_UPDATE = 0.25  # 1 bit read + 1 bit written per site and sweep
+METRIC = "attempted spin updates/ns"
+
+
+def peaks() -> tuple[float, str]:
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic() -> dict | None:
+    """DRAM bytes per chain and half-sweep launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "msc_halfsweep_L4096.json"
+    try:
+        return json.loads(p.read_text())
+    except Exception:
+        return None
+
+
+class Clocks:
+    """Samples nvidia-smi clocks every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(threads: int, sweeps: int = 1, L: int = L_HEAD) -> dict:
+    """The C oracle (a plain-C port of critmc's Ising sweep with the same Philox
+    stream) on `threads` host threads, one L x L chain per thread."""
+    import oracle
+
+    oracle.lib()
+
+    def one(t: int) -> float:
+        s = (2 * np.random.default_rng(100 + t).integers(0, 2, L * L) - 1).astype(np.int8)
+        t0 = time.perf_counter()
+        oracle.ising_msc_run(s, (L, L), (t, 7), BETAS[t % 3], 0.0, [[0, 1]], sweeps)
+        return time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(one, range(threads)))
+    wall = time.perf_counter() - t0
+    upd = threads * sweeps * L * L
+    return {"value": upd / wall / 1e9, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{threads} chains of {L}x{L}, {sweeps} checkerboard Metropolis sweep(s) each, "
+                      f"one host thread per chain, hot start ({wall:.1f} s wall)"}
+
+
+def run_reference(args) -> None:
+    """CPU arm: the C oracle (port of critmc's sweep) on every host thread.
+
+    One step advances, on each host thread, its own 4096 x 64 torus (a strip of
+    the L = 4096 workload, 262,144 sites) by one checkerboard Metropolis sweep,
+    so that `--steps K` stays within minutes; the rate is updates per ns of
+    wall time over the K steps."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+
+    oracle.lib()
+    threads = os.cpu_count() or 1
+    shape = (L_HEAD, 64)
+    n = shape[0] * shape[1]
+    states = [(2 * np.random.default_rng(200 + t).integers(0, 2, n) - 1).astype(np.int8)
+              for t in range(threads)]
+    runs = [None] * threads
+
+    def step(t: int, sweep: int) -> None:
+        _, _, _, runs[t] = oracle.ising_msc_run(states[t], shape, (t, 11), BETAS[t % 3], 0.0,
+                                                [[0, 1]], 1, sweep0=sweep, running=runs[t])
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        for w in range(args.warmup):
+            list(ex.map(lambda t: step(t, w), range(threads)))
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            list(ex.map(lambda t: step(t, args.warmup + k), range(threads)))
+        wall = time.perf_counter() - t0
+    value = threads * n * args.steps / wall / 1e9
+    sample = (f"{threads} host threads, each advancing its own {shape[0]}x{shape[1]} torus by one "
+              f"checkerboard Metropolis sweep per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"2D Ising L={L_HEAD} checkerboard Metropolis (4096x64 strips per thread)",
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extras", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from critmc_b200.ensemble import IsingEnsemble
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps) -> float:
+        s = torch.cuda.current_stream(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(s)
+        for _ in range(steps):
+            fn()
+        e1.record(s)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    ens = IsingEnsemble(L_HEAD, BETAS, CHAINS_PER_BETA, seed=1000 + rank, device=dev)
+    n_upd = ens.n_chains * ens.n_sites  # per step and rank
+    for _ in range(args.warmup):
+        ens.run(1, "metropolis", host=False)
+    with Clocks(local) as clk:
+        ms = timed(lambda: ens.run(1, "metropolis", host=False), args.steps)
+    value = world * n_upd * args.steps / (ms * 1e6)
+
+    # end to end through the public API: host outputs (pinned) every step
+    out = None
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = ens.run(1, "metropolis", host=True, out=out)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    d2h = sum(t.numel() * t.element_size() for t in (out.Eb, out.M, out.aux))
+    h2d = ens.keys.nbytes + ens.tables.nbytes + 16  # host inputs of a call: keys, tables, schedule
+    e2e = {"value": world * n_upd * args.steps / (e2e_s * 1e9), "unit": METRIC,
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+           "note": "ensemble.run(1) with host (pinned) outputs, host wall clock; the spin "
+                   "configurations stay resident on the GPU between steps"}
+
+    peak, peak_kind = peaks()
+    launches_per_step = 2  # half-sweep kernels (one launch covers <= 256 chains)
+    avg_launch_ms = ms / (args.steps * launches_per_step)
+    algo_bytes = ens.n_chains * (ens.n_sites / 2) * BYTES_PER_UPDATE
+    achieved = algo_bytes / (avg_launch_ms * 1e-3) / 1e9
+    prof = profile_traffic()
+    traffic = prof["dram_bytes_per_chain_launch"] * ens.n_chains if prof else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": algo_bytes,
+                "kernel": "msc_halfsweep_kernel (Metropolis, zero field)"}
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        hb_steps = max(2, args.steps // 2)  # one heat-bath sweep per step
+        ms_hb = timed(lambda: ens.run(1, "heatbath", host=False), hb_steps)
+        extras["heatbath_L4096"] = n_upd * hb_steps / (ms_hb * 1e6)
+        del ens
+        torch.cuda.empty_cache()
+        plain = IsingEnsemble(L_HEAD, BETAS[1:2], 1, seed=7, device=dev, mode=1)
+        for _ in range(2):
+            plain.run(1, host=False)
+        ms_p = timed(lambda: plain.run(4, host=False), 3)
+        extras["plain_one_chain_L4096"] = plain.n_sites * 12 / (ms_p * 1e6)
+        del plain
+        small = IsingEnsemble(1024, BETAS, CHAINS_PER_BETA, seed=8, device=dev)
+        for _ in range(2):
+            small.run(8, host=False)
+        ms_s = timed(lambda: small.run(8, host=False), 3)
+        extras["batched_L1024"] = small.n_chains * small.n_sites * 24 / (ms_s * 1e6)
+        del small
+        plain1k = IsingEnsemble(1024, BETAS[1:2], 1, seed=9, device=dev, mode=1)
+        plain1k.run(4, host=False)
+        ms_p1 = timed(lambda: plain1k.run(50, host=False), 1)
+        extras["plain_one_chain_L1024"] = plain1k.n_sites * 50 / (ms_p1 * 1e6)
+        extras["batched_over_plain"] = {
+            "L4096": value / world / extras["plain_one_chain_L4096"],
+            "L1024": extras["batched_L1024"] / extras["plain_one_chain_L1024"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(min(32, os.cpu_count() or 1))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": f"2D Ising MSC L={L_HEAD}, betas {list(BETAS)} x "
+                                   f"{CHAINS_PER_BETA} chains, checkerboard Metropolis, 1 sweep/step",
+                       "chains_per_gpu": len(BETAS) * CHAINS_PER_BETA, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (384 MiB of spins per GPU)"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "gpu_launches": args.steps * (1 + launches_per_step + 1),
+            "clocks": clk.summary(), "extras": extras,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

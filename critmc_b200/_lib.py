@@ -33,6 +33,17 @@ SIGNATURES: dict[str, tuple] = {
          _I32, _I32, _P],
     ),
     "critmc_ising_msc_measure": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+    "critmc_ising_msc_init": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P]),
+    "critmc_ising_byte_run": (
+        _I32,
+        [_P, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P, _P, _P],
+    ),
+    "critmc_potts_run": (
+        _I32,
+        [_P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P, _P,
+         _P, _P],
+    ),
+    "critmc_potts_tables": (_I32, [_I32, _D, _P, _P]),
 }
 
 

@@ -1,0 +1,425 @@
+// Byte lattices: int8 Ising and q-state Potts chains, one thread block per
+// chain running the whole schedule (lattice staged in shared memory when it
+// fits).  This is also the batched form for many small chains: a launch
+// carries up to BYTE_PCHAINS chains, one block each.
+//
+// Replaces critmc src/critmc/kernels/ising.py:174-237 / potts.py:171-235
+// (`run`), ising.py:69-107 and potts.py:45-103 (the sweeps) for checkerboard
+// visiting order.
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "host_common.h"
+
+namespace critmc {
+
+constexpr int BYTE_PCHAINS = 1024;      // chains per launch (keys in kernel parameters)
+constexpr int BYTE_MAX_GROUPS = 16;
+constexpr int BYTE_MAX_ROWS = 8;        // schedule rows
+constexpr int BYTE_SMEM_MAX = 160 * 1024;
+constexpr int MODEL_ISING = 0, MODEL_POTTS = 1;
+
+struct ByteGeom {
+  int dim, lx, ly, lz, hx, rows;
+  uint32_t slots;  // sites per colour
+};
+
+struct ByteParams {
+  int8_t* spins;
+  long long* running;   // Ising: [n][2] (E_b, M); Potts: energy [n]
+  long long* counts;    // Potts: [n][q]
+  long long* e_out;
+  long long* m_out;     // Ising only
+  long long* counts_out;  // Potts only
+  long long* aux_out;
+  ByteGeom g;
+  int q;
+  int n_chains, chain0, chains_per_group, n_meas;
+  int n_rows;
+  int codes[BYTE_MAX_ROWS];
+  int reps[BYTE_MAX_ROWS];
+  int resident;
+  uint32_t sweep0;
+  // Ising: kind/thr per group and algorithm slot; Potts: 64-bit thresholds and weights
+  uint32_t kind[BYTE_MAX_GROUPS][2][CRITMC_NCLS];
+  uint32_t thr[BYTE_MAX_GROUPS][2][CRITMC_NCLS];
+  unsigned long long boltz[BYTE_MAX_GROUPS][8];
+  unsigned long long weight[BYTE_MAX_GROUPS][8];
+  uint32_t keys[BYTE_PCHAINS][2];
+};
+
+__device__ __forceinline__ void byte_row_index(const ByteGeom& g, uint32_t slot, int& r, int& i) {
+  r = (int)(slot / (uint32_t)g.hx);
+  i = (int)slot - r * g.hx;
+}
+
+// slots (in the other colour's plane) of the Z neighbours of slot (r, i) of colour c
+template <int Z>
+__device__ __forceinline__ void byte_neighbours(const ByteGeom& g, int c, int r, int i, uint32_t* nb) {
+  int y = r, z = 0;
+  if constexpr (Z == 6) {
+    y = r % g.ly;
+    z = r / g.ly;
+  }
+  const int p = (c + y + z) & 1;
+  const int ia = p ? ((i == g.hx - 1) ? 0 : i + 1) : ((i == 0) ? g.hx - 1 : i - 1);
+  nb[0] = (uint32_t)(r * g.hx + i);
+  nb[1] = (uint32_t)(r * g.hx + ia);
+  if constexpr (Z >= 4) {
+    const int ym = (y == 0) ? g.ly - 1 : y - 1, yp = (y == g.ly - 1) ? 0 : y + 1;
+    nb[2] = (uint32_t)((ym + g.ly * z) * g.hx + i);
+    nb[3] = (uint32_t)((yp + g.ly * z) * g.hx + i);
+  }
+  if constexpr (Z == 6) {
+    const int zm = (z == 0) ? g.lz - 1 : z - 1, zp = (z == g.lz - 1) ? 0 : z + 1;
+    nb[4] = (uint32_t)((y + g.ly * zm) * g.hx + i);
+    nb[5] = (uint32_t)((y + g.ly * zp) * g.hx + i);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  T out = 0;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int q = 0; q < nw; ++q) out += red[q];
+  return out;
+}
+
+template <int MODEL, int Z>
+__global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ ByteParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ long long red[16];
+  __shared__ int cnt[128];
+  const int lchain = blockIdx.x;
+  const int chain = P.chain0 + lchain;
+  const int group = chain / P.chains_per_group;
+  const ByteGeom& g = P.g;
+  const uint32_t k0 = P.keys[lchain][0], k1 = P.keys[lchain][1];
+  const size_t n_sites = 2 * (size_t)g.slots;
+  int8_t* gl = P.spins + (size_t)chain * n_sites;
+  int8_t* lat = P.resident ? reinterpret_cast<int8_t*>(smem_raw) : gl;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (P.resident)
+    for (size_t j = tid; j < n_sites; j += nt) lat[j] = gl[j];
+  const int q = P.q;
+  if (MODEL == MODEL_POTTS)
+    for (int k = tid; k < q; k += nt) cnt[k] = (int)P.counts[(size_t)chain * q + k];
+  __syncthreads();
+
+  long long e_run = (MODEL == MODEL_ISING) ? P.running[2 * chain] : P.running[chain];
+  long long m_run = (MODEL == MODEL_ISING) ? P.running[2 * chain + 1] : 0;
+  uint32_t sweep = P.sweep0;
+  for (int meas = 0; meas < P.n_meas; ++meas) {
+    long long dE = 0, dM = 0, nacc = 0;
+    for (int row = 0; row < P.n_rows; ++row) {
+      const int code = P.codes[row];
+      const int slot_alg = (code == CRITMC_HEATBATH) ? 1 : 0;
+      for (int rep = 0; rep < P.reps[row]; ++rep) {
+        for (int c = 0; c < 2; ++c) {
+          int8_t* own = lat + (size_t)c * g.slots;
+          const int8_t* other = lat + (size_t)(c ^ 1) * g.slots;
+          for (uint32_t s = tid; s < g.slots; s += nt) {
+            int r, i;
+            byte_row_index(g, s, r, i);
+            uint32_t nb[Z];
+            byte_neighbours<Z>(g, c, r, i, nb);
+            const critmc_u32x4 rnd =
+                critmc_philox4x32(s, sweep, CRITMC_TAG_SITE | ((uint32_t)c << 16), 0u, k0, k1);
+            const int old = own[s];
+            if constexpr (MODEL == MODEL_ISING) {
+              int field = 0;
+#pragma unroll
+              for (int k = 0; k < Z; ++k) field += other[nb[k]];
+              const int sb = old > 0;
+              int v;
+              if (slot_alg == 0) v = (Z - old * field) / 2;  // anti-aligned neighbours
+              else v = (field + Z) / 2;                       // up neighbours
+              const int cls = 2 * v + sb;
+              const uint32_t kd = P.kind[group][slot_alg][cls];
+              const bool dec = kd == CRITMC_KIND_ALWAYS ||
+                               (kd == CRITMC_KIND_RANDOM && rnd.v[0] < P.thr[group][slot_alg][cls]);
+              const int nw = slot_alg == 0 ? (dec ? -old : old) : (dec ? 1 : -1);
+              if (nw != old) {
+                own[s] = (int8_t)nw;
+                dE += 2 * old * field;
+                dM += nw - old;
+                ++nacc;
+              }
+            } else {
+              int nbs[Z];
+#pragma unroll
+              for (int k = 0; k < Z; ++k) nbs[k] = other[nb[k]];
+              int nw;
+              if (slot_alg == 0) {
+                // propose a uniformly chosen different state (potts.py:53-56)
+                nw = (int)(((unsigned long long)rnd.v[0] * (unsigned)(q - 1)) >> 32);
+                if (nw >= old) ++nw;
+                int n_old = 0, n_new = 0;
+#pragma unroll
+                for (int k = 0; k < Z; ++k) {
+                  n_old += nbs[k] == old;
+                  n_new += nbs[k] == nw;
+                }
+                const int delta = n_old - n_new;
+                const bool acc = delta <= 0 || (unsigned long long)rnd.v[1] < P.boltz[group][delta];
+                if (acc) {
+                  own[s] = (int8_t)nw;
+                  atomicSub(&cnt[old], 1);
+                  atomicAdd(&cnt[nw], 1);
+                  dE += delta;
+                  ++nacc;
+                }
+              } else {
+                // heat bath: state k with weight W[#neighbours in k] (potts.py:75-103)
+                const unsigned long long u = ((unsigned long long)rnd.v[0] << 32) | rnd.v[1];
+                unsigned long long total = 0;
+                for (int k = 0; k < q; ++k) {
+                  int nk = 0;
+#pragma unroll
+                  for (int j = 0; j < Z; ++j) nk += nbs[j] == k;
+                  total += P.weight[group][nk];
+                }
+                const unsigned long long x = __umul64hi(u, total);
+                unsigned long long cum = 0;
+                nw = q - 1;
+                for (int k = 0; k < q; ++k) {
+                  int nk = 0;
+#pragma unroll
+                  for (int j = 0; j < Z; ++j) nk += nbs[j] == k;
+                  cum += P.weight[group][nk];
+                  if (x < cum) {
+                    nw = k;
+                    break;
+                  }
+                }
+                if (nw != old) {
+                  int n_old = 0, n_new = 0;
+#pragma unroll
+                  for (int k = 0; k < Z; ++k) {
+                    n_old += nbs[k] == old;
+                    n_new += nbs[k] == nw;
+                  }
+                  own[s] = (int8_t)nw;
+                  atomicSub(&cnt[old], 1);
+                  atomicAdd(&cnt[nw], 1);
+                  dE += n_old - n_new;
+                  ++nacc;
+                }
+              }
+            }
+          }
+          __syncthreads();
+        }
+        ++sweep;
+      }
+    }
+    dE = block_sum(dE, red);
+    dM = block_sum(dM, red);
+    nacc = block_sum(nacc, red);
+    e_run += dE;
+    m_run += dM;
+    const size_t o = (size_t)chain * P.n_meas + meas;
+    if (tid == 0) {
+      P.e_out[o] = e_run;
+      if (MODEL == MODEL_ISING) P.m_out[o] = m_run;
+      P.aux_out[4 * o + 0] = nacc;
+      P.aux_out[4 * o + 1] = 0;
+      P.aux_out[4 * o + 2] = 0;
+      P.aux_out[4 * o + 3] = 0;
+    }
+    if (MODEL == MODEL_POTTS)
+      for (int k = tid; k < q; k += nt) P.counts_out[o * q + k] = cnt[k];
+  }
+  __syncthreads();
+  if (P.resident)
+    for (size_t j = tid; j < n_sites; j += nt) gl[j] = lat[j];
+  if (tid == 0) {
+    if (MODEL == MODEL_ISING) {
+      P.running[2 * chain] = e_run;
+      P.running[2 * chain + 1] = m_run;
+    } else {
+      P.running[chain] = e_run;
+    }
+  }
+  if (MODEL == MODEL_POTTS)
+    for (int k = tid; k < q; k += nt) P.counts[(size_t)chain * q + k] = cnt[k];
+}
+
+static int byte_geom(int dim, int lx, int ly, int lz, ByteGeom& g) {
+  if (dim < 1 || dim > 3) return fail(CRITMC_ERR_UNSUPPORTED, "dimension must be 1, 2 or 3");
+  if (dim < 2) ly = 1;
+  if (dim < 3) lz = 1;
+  if (lx < 2 || lx % 2 || (dim >= 2 && (ly < 2 || ly % 2)) || (dim == 3 && (lz < 2 || lz % 2)))
+    return fail(CRITMC_ERR_UNSUPPORTED, "checkerboard sweeps need every extent even and >= 2");
+  const long long n = (long long)lx * ly * lz;
+  if (n >= (1LL << 30)) return fail(CRITMC_ERR_UNSUPPORTED, "lattice too large");
+  g.dim = dim;
+  g.lx = lx;
+  g.ly = ly;
+  g.lz = lz;
+  g.hx = lx / 2;
+  g.rows = ly * lz;
+  g.slots = (uint32_t)(n / 2);
+  return CRITMC_OK;
+}
+
+static int byte_schedule(ByteParams& P, const int64_t* schedule, int n_rows, long long& per_meas) {
+  if (!schedule || n_rows < 1 || n_rows > BYTE_MAX_ROWS)
+    return fail(CRITMC_ERR_INVALID, "schedule must have 1..8 rows");
+  per_meas = 0;
+  for (int r = 0; r < n_rows; ++r) {
+    const int64_t code = schedule[2 * r], reps = schedule[2 * r + 1];
+    if (code != CRITMC_METROPOLIS && code != CRITMC_HEATBATH)
+      return fail(CRITMC_ERR_UNSUPPORTED, "byte lattices run checkerboard metropolis and heatbath rows only");
+    if (reps < 1 || reps > (1 << 20)) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be in [1, 2^20]");
+    P.codes[r] = (int)code;
+    P.reps[r] = (int)reps;
+    per_meas += reps;
+  }
+  P.n_rows = n_rows;
+  return CRITMC_OK;
+}
+
+template <int MODEL>
+static int byte_launch(ByteParams& P, const uint32_t* keys, cudaStream_t s) {
+  const size_t lat_bytes = 2 * (size_t)P.g.slots;
+  P.resident = lat_bytes <= (size_t)BYTE_SMEM_MAX;
+  const size_t smem = P.resident ? lat_bytes : 0;
+  int threads = (int)std::min<uint32_t>(512, ((P.g.slots + 31) / 32) * 32);
+  threads = std::max(threads, 32);
+  for (int c0 = 0; c0 < P.n_chains; c0 += BYTE_PCHAINS) {
+    const int nc = std::min(BYTE_PCHAINS, P.n_chains - c0);
+    P.chain0 = c0;
+    std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
+    auto launch = [&](auto kern) {
+      if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<nc, threads, smem, s>>>(P);
+    };
+    switch (P.g.dim) {
+      case 1: launch(byte_run_kernel<MODEL, 2>); break;
+      case 2: launch(byte_run_kernel<MODEL, 4>); break;
+      default: launch(byte_run_kernel<MODEL, 6>); break;
+    }
+    if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  }
+  return CRITMC_OK;
+}
+
+static thread_local ByteParams g_params;  // large: kept off the stack, one per calling thread
+
+}  // namespace critmc
+
+using namespace critmc;
+
+extern "C" int32_t critmc_potts_tables(int32_t z, double beta, uint64_t* boltz_thr, uint64_t* hb_weight) {
+  clear_error();
+  if (!boltz_thr || !hb_weight) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (z < 1 || z > 7 || !std::isfinite(beta)) return fail(CRITMC_ERR_INVALID, "need 1 <= z <= 7 and finite beta");
+  for (int d = 0; d < 8; ++d) {
+    const double p = std::exp(-beta * d);  // potts.py:192-194 boltz[d]
+    if (d == 0 || p >= 1.0) {
+      boltz_thr[d] = 1ULL << 32;
+    } else {
+      const double t = std::nearbyint(std::ldexp(p, 32));
+      boltz_thr[d] = t >= 4294967296.0 ? (1ULL << 32) : (uint64_t)t;
+    }
+  }
+  // weight[n] = exp(beta n) (potts.py:192-194), scaled so that the largest is 2^52
+  double mx = -INFINITY;
+  for (int n = 0; n <= z; ++n) mx = std::max(mx, beta * n);
+  for (int n = 0; n < 8; ++n) {
+    const double w = n <= z ? std::exp(beta * n - mx) : 0.0;
+    hb_weight[n] = (uint64_t)std::nearbyint(std::ldexp(w, 52));
+  }
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_ising_byte_run(int8_t* spins, int32_t dim, int32_t lx, int32_t ly,
+                                         int32_t lz, int32_t n_chains, const uint32_t* keys,
+                                         const uint32_t* tables, int32_t n_groups, uint32_t sweep0,
+                                         const int64_t* schedule, int32_t n_rows, int32_t n_meas,
+                                         int64_t* running, int64_t* e_out, int64_t* m_out,
+                                         int64_t* aux_out, void* stream) {
+  clear_error();
+  ByteParams& P = g_params;
+  int st = byte_geom(dim, lx, ly, lz, P.g);
+  if (st) return st;
+  if (!spins || !keys || !tables || !running || !e_out || !m_out || !aux_out)
+    return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (n_chains < 1 || n_groups < 1 || n_groups > BYTE_MAX_GROUPS || n_chains % n_groups)
+    return fail(CRITMC_ERR_INVALID, "need n_chains >= 1 and 1 <= n_groups <= 16 dividing n_chains");
+  if (n_meas < 0) return fail(CRITMC_ERR_INVALID, "n_meas must not be negative");
+  long long per_meas = 0;
+  if ((st = byte_schedule(P, schedule, n_rows, per_meas))) return st;
+  if ((long long)sweep0 + per_meas * n_meas > 0xFFFFFFFFLL)
+    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+  if (n_meas == 0) return CRITMC_OK;
+  for (int gi = 0; gi < n_groups; ++gi)
+    for (int a = 0; a < 2; ++a) {
+      std::memcpy(P.kind[gi][a], tables + ((size_t)gi * 4 + 2 * a) * CRITMC_NCLS, CRITMC_NCLS * 4);
+      std::memcpy(P.thr[gi][a], tables + ((size_t)gi * 4 + 2 * a + 1) * CRITMC_NCLS, CRITMC_NCLS * 4);
+    }
+  P.spins = spins;
+  P.running = (long long*)running;
+  P.e_out = (long long*)e_out;
+  P.m_out = (long long*)m_out;
+  P.aux_out = (long long*)aux_out;
+  P.counts = nullptr;
+  P.counts_out = nullptr;
+  P.q = 2;
+  P.n_chains = n_chains;
+  P.chains_per_group = n_chains / n_groups;
+  P.n_meas = n_meas;
+  P.sweep0 = sweep0;
+  return byte_launch<MODEL_ISING>(P, keys, (cudaStream_t)stream);
+}
+
+extern "C" int32_t critmc_potts_run(int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                                    int32_t q, int32_t n_chains, const uint32_t* keys,
+                                    const double* betas, int32_t n_groups, uint32_t sweep0,
+                                    const int64_t* schedule, int32_t n_rows, int32_t n_meas,
+                                    int64_t* energy, int64_t* counts, int64_t* e_out,
+                                    int64_t* counts_out, int64_t* aux_out, void* stream) {
+  clear_error();
+  ByteParams& P = g_params;
+  int st = byte_geom(dim, lx, ly, lz, P.g);
+  if (st) return st;
+  if (!spins || !keys || !betas || !energy || !counts || !e_out || !counts_out || !aux_out)
+    return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (q < 2 || q > 127) return fail(CRITMC_ERR_INVALID, "q must be in [2, 127]");
+  if (n_chains < 1 || n_groups < 1 || n_groups > BYTE_MAX_GROUPS || n_chains % n_groups)
+    return fail(CRITMC_ERR_INVALID, "need n_chains >= 1 and 1 <= n_groups <= 16 dividing n_chains");
+  if (n_meas < 0) return fail(CRITMC_ERR_INVALID, "n_meas must not be negative");
+  long long per_meas = 0;
+  if ((st = byte_schedule(P, schedule, n_rows, per_meas))) return st;
+  if ((long long)sweep0 + per_meas * n_meas > 0xFFFFFFFFLL)
+    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+  if (n_meas == 0) return CRITMC_OK;
+  for (int gi = 0; gi < n_groups; ++gi) {
+    uint64_t b[8], w[8];
+    if ((st = critmc_potts_tables(2 * dim, betas[gi], b, w))) return st;
+    for (int d = 0; d < 8; ++d) {
+      P.boltz[gi][d] = b[d];
+      P.weight[gi][d] = w[d];
+    }
+  }
+  P.spins = spins;
+  P.running = (long long*)energy;
+  P.counts = (long long*)counts;
+  P.e_out = (long long*)e_out;
+  P.m_out = nullptr;
+  P.counts_out = (long long*)counts_out;
+  P.aux_out = (long long*)aux_out;
+  P.q = q;
+  P.n_chains = n_chains;
+  P.chains_per_group = n_chains / n_groups;
+  P.n_meas = n_meas;
+  P.sweep0 = sweep0;
+  return byte_launch<MODEL_POTTS>(P, keys, (cudaStream_t)stream);
+}

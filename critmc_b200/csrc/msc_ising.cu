@@ -265,6 +265,22 @@ __global__ void msc_measure_final(unsigned long long* io, int n_chains, long lon
   io[2 * c + 1] = (unsigned long long)(2 * up - n_sites);
 }
 
+// Hot (random) or cold start of MSC chains from the Philox init stream:
+// word w of colour c = word 0 of Philox(w, 0, TAG_INIT | c << 16, 0).
+__global__ void msc_init_kernel(uint32_t* spins, MscGeom g, const uint32_t* __restrict__ keys,
+                                int start) {
+  const int chain = blockIdx.y;
+  const uint32_t k0 = keys[2 * chain], k1 = keys[2 * chain + 1];
+  uint32_t* base = spins + (size_t)chain * 2 * g.words;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * g.words; i += gridDim.x * blockDim.x) {
+    const uint32_t col = i >= g.words, w = i - col * g.words;
+    uint32_t v;
+    if (start == 0) v = critmc_philox4x32(w, 0u, CRITMC_TAG_INIT | (col << 16), 0u, k0, k1).v[0];
+    else v = start > 0 ? ~0u : 0u;
+    base[i] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -500,6 +516,23 @@ extern "C" int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, 
   else msc_measure_kernel<6><<<grid, 256, 0, s>>>(spins, g, (unsigned long long*)out);
   const long long n_sites = (long long)lx * ly * (dim == 3 ? lz : 1);
   msc_measure_final<<<(n_chains + 127) / 128, 128, 0, s>>>((unsigned long long*)out, n_chains, n_sites, 2 * dim);
+  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_ising_msc_init(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,
+                                         int32_t lz, int32_t n_chains, const uint32_t* keys,
+                                         int32_t start, void* stream) {
+  clear_error();
+  MscGeom g;
+  int st = msc_geom(dim, lx, ly, lz, g);
+  if (st) return st;
+  if (!spins || !keys) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (n_chains < 1 || n_chains > 65535) return fail(CRITMC_ERR_INVALID, "n_chains must be in [1, 65535]");
+  if (start < -1 || start > 1) return fail(CRITMC_ERR_INVALID, "start must be 0 (random), 1 (up) or -1 (down)");
+  cudaStream_t s = (cudaStream_t)stream;
+  const dim3 grid(std::min<uint32_t>(2048, (2 * g.words + 255) / 256), n_chains);
+  msc_init_kernel<<<grid, 256, 0, s>>>(spins, g, keys, start);
   if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
   return CRITMC_OK;
 }

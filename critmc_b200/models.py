@@ -104,6 +104,18 @@ class Model(ABC):
                 f"{type(self).__name__} does not support updates {bad} on the GPU; "
                 f"available: {list(self.updates)}" + (f" ({why})" if why else "")
             )
+        if self._binary and self.lattice.dim == 1 and "metropolis" in names:
+            # On a ring a zero-energy flip is accepted with certainty; updating a whole
+            # sublattice at once then moves every domain wall one site per half-sweep in
+            # lockstep, walls never meet, and the chain is not ergodic.
+            raise ValueError(
+                "checkerboard metropolis is not ergodic for two-state spins on a ring; "
+                "use heatbath"
+            )
+
+    @property
+    def _binary(self) -> bool:
+        return False
 
     def spec(self) -> dict[str, Any]:
         return {"model": self.kind, "lattice": self.lattice.name, "L": self.lattice.L}
@@ -150,6 +162,10 @@ class Ising(Model):
         self.h = float(h)
         if not math.isfinite(self.h):
             raise ValueError(f"field h must be finite, got {h}")
+
+    @property
+    def _binary(self) -> bool:
+        return True
 
     def initial_state(self, start, rng):
         n = self.n_sites
@@ -233,6 +249,10 @@ class Potts(Model):
         if q < 2 or q > 127:
             raise ValueError(f"q must be in [2, 127], got {q}")
         self.q = int(q)
+
+    @property
+    def _binary(self) -> bool:
+        return self.q == 2
 
     def initial_state(self, start, rng):
         n = self.n_sites

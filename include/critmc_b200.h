@@ -97,6 +97,52 @@ int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx, int32_t l
                              int64_t* m_out, int64_t* aux_out, void* scratch, int32_t mode,
                              int32_t k_inline, void* stream);
 
+/* Initial configurations of MSC chains, drawn on the device: start 0 = random
+ * (word w of colour c is word 0 of Philox(w, 0, 0x05 | c << 16, 0) with the
+ * chain's key), 1 = all up, -1 = all down.  keys: DEVICE [n_chains][2].
+ * critmc models.py:113-121 draws the same hot/cold starts on the host.    */
+int32_t critmc_ising_msc_init(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                              int32_t n_chains, const uint32_t* keys, int32_t start, void* stream);
+
+/* ---- byte lattices (int8 Ising, q-state Potts) -----------------------------
+ * Layout of one chain: elem[colour][row][i] (int8), row = y + ly*z, slot i
+ * of the colour's row holds site x = 2i + p, p = (colour + y + z) & 1.  All
+ * extents must be even (dim 1..3).  One thread block advances one chain
+ * through the whole schedule; the lattice is staged in shared memory when it
+ * fits (lx*ly*lz bytes <= 160 KiB) and updated in HBM otherwise.
+ * keys: HOST [n_chains][2].  Chains form n_groups equal groups of
+ * consecutive chains sharing one acceptance table / beta.
+ * Each site draws Philox4x32-10(c0 = slot (row*lx/2 + i), c1 = sweep,
+ * c2 = 0x02 | colour << 16, c3 = 0) once per sweep.                        */
+
+/* Ising with int8 spins (+1/-1), same class tables and outputs as
+ * critmc_ising_msc_run; replaces critmc kernels/ising.py:174-237.         */
+int32_t critmc_ising_byte_run(int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                              int32_t n_chains, const uint32_t* keys, const uint32_t* tables,
+                              int32_t n_groups, uint32_t sweep0, const int64_t* schedule,
+                              int32_t n_rows, int32_t n_meas, int64_t* running, int64_t* e_out,
+                              int64_t* m_out, int64_t* aux_out, void* stream);
+
+/* q-state Potts (2 <= q <= 127), states 0..q-1 in int8.  betas: HOST
+ * [n_groups].  Device in/out: energy[n_chains] (E = -#satisfied bonds),
+ * counts[n_chains][q].  Device outputs: e_out[n_chains][n_meas],
+ * counts_out[n_chains][n_meas][q], aux_out[n_chains][n_meas][4].
+ * Replaces critmc kernels/potts.py:171-235 (`run`), :45-71 (Metropolis with
+ * a uniformly proposed different state, boltz[d] = exp(-beta d)) and :75-103
+ * (heat bath, weight[n] = exp(beta n)).                                    */
+int32_t critmc_potts_run(int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t q,
+                         int32_t n_chains, const uint32_t* keys, const double* betas,
+                         int32_t n_groups, uint32_t sweep0, const int64_t* schedule,
+                         int32_t n_rows, int32_t n_meas, int64_t* energy, int64_t* counts,
+                         int64_t* e_out, int64_t* counts_out, int64_t* aux_out, void* stream);
+
+/* Potts acceptance tables for one beta: boltz_thr[8] (accept iff u < thr for
+ * a uniform 32-bit u; thr = round(2^32 exp(-beta d)), 2^32 = always, for
+ * d = 0..7) and hb_weight[8] (uint64 weights round(2^52 exp(beta n - max)),
+ * n = 0..7; the heat bath picks state k with probability proportional to
+ * hb_weight[#neighbours in state k]).                                       */
+int32_t critmc_potts_tables(int32_t z, double beta, uint64_t* boltz_thr, uint64_t* hb_weight);
+
 /* Energy E_b = -sum_<ij> s_i s_j and magnetisation M of MSC chains, written
  * to out[n_chains][2] (device).  critmc kernels/ising.py:32-45.           */
 int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,

@@ -56,6 +56,12 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_ising_bond_energy.restype = ctypes.c_int64
     L.oracle_ising_msc_run.argtypes = [_P, _I, _I, _I, _I, _P, _P, _U32, _P, _I, _I, _P, _P, _P, _P]
     L.oracle_ising_msc_run.restype = _I
+    L.oracle_ising_byte_run.argtypes = [_P, _I, _I, _I, _I, _P, _P, _U32, _P, _I, _I, _P, _P, _P, _P]
+    L.oracle_ising_byte_run.restype = _I
+    L.oracle_potts_tables.argtypes = [_I, _D, _P, _P]
+    L.oracle_potts_tables.restype = _I
+    L.oracle_potts_run.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _U32, _P, _I, _I, _P, _P, _P, _P, _P]
+    L.oracle_potts_run.restype = _I
 
 
 def _ptr(a: np.ndarray) -> int:
@@ -113,3 +119,66 @@ def ising_msc_run(s, shape, key, beta, h, schedule, n_meas, sweep0=0, running=No
     if rc != 0:
         raise ValueError(f"oracle_ising_msc_run failed ({rc})")
     return e, m, aux, running
+
+
+def _dims(shape):
+    return tuple(shape) + (1,) * (3 - len(shape))
+
+
+def ising_byte_run(s, shape, key, beta, h, schedule, n_meas, sweep0=0, running=None):
+    """Replay the int8 checkerboard sweeps on ``s`` (int8, critmc order, modified in place)."""
+    if not (isinstance(s, np.ndarray) and s.dtype == np.int8 and s.flags["C_CONTIGUOUS"]):
+        raise TypeError("s must be a C-contiguous int8 array (it is updated in place)")
+    z = 2 * len(shape)
+    tables = np.ascontiguousarray(
+        np.concatenate([ising_table(0, z, beta, h).ravel(), ising_table(2, z, beta, h).ravel()]),
+        dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+    if running is None:
+        running = np.array([ising_bond_energy(s, shape), int(s.astype(np.int64).sum())], dtype=np.int64)
+    running = np.ascontiguousarray(running, dtype=np.int64).copy()
+    e = np.zeros(n_meas, dtype=np.int64)
+    m = np.zeros(n_meas, dtype=np.int64)
+    aux = np.zeros((n_meas, 4), dtype=np.int64)
+    rc = lib().oracle_ising_byte_run(_ptr(s), len(shape), *_dims(shape), _ptr(k), _ptr(tables), sweep0,
+                                     _ptr(sched), len(sched), n_meas, _ptr(running), _ptr(e), _ptr(m),
+                                     _ptr(aux))
+    if rc != 0:
+        raise ValueError(f"oracle_ising_byte_run failed ({rc})")
+    return e, m, aux, running
+
+
+def potts_tables(z: int, beta: float):
+    b = np.zeros(8, dtype=np.uint64)
+    w = np.zeros(8, dtype=np.uint64)
+    lib().oracle_potts_tables(z, beta, _ptr(b), _ptr(w))
+    return b, w
+
+
+def potts_energy(s, shape) -> int:
+    """E = -#satisfied bonds (critmc kernels/potts.py:28-34)."""
+    a = np.asarray(s).reshape(tuple(reversed(tuple(shape))))
+    e = 0
+    for ax in range(a.ndim):
+        e -= int(np.sum(a == np.roll(a, -1, axis=ax)))
+    return e
+
+
+def potts_run(s, shape, q, key, beta, schedule, n_meas, sweep0=0, energy=None, counts=None):
+    """Replay the Potts checkerboard sweeps on ``s`` (int8 states, modified in place)."""
+    if not (isinstance(s, np.ndarray) and s.dtype == np.int8 and s.flags["C_CONTIGUOUS"]):
+        raise TypeError("s must be a C-contiguous int8 array (it is updated in place)")
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+    en = np.array([potts_energy(s, shape) if energy is None else energy], dtype=np.int64)
+    cnt = (np.bincount(s.astype(np.int64), minlength=q) if counts is None else np.array(counts)).astype(np.int64)
+    cnt = np.ascontiguousarray(cnt)
+    e = np.zeros(n_meas, dtype=np.int64)
+    co = np.zeros((n_meas, q), dtype=np.int64)
+    aux = np.zeros((n_meas, 4), dtype=np.int64)
+    rc = lib().oracle_potts_run(_ptr(s), len(shape), *_dims(shape), q, _ptr(k), beta, sweep0, _ptr(sched),
+                                len(sched), n_meas, _ptr(en), _ptr(cnt), _ptr(e), _ptr(co), _ptr(aux))
+    if rc != 0:
+        raise ValueError(f"oracle_potts_run failed ({rc})")
+    return e, co, aux, int(en[0]), cnt

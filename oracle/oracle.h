@@ -10,4 +10,13 @@ int oracle_ising_msc_run(int8_t* s, int dim, int lx, int ly, int lz, const uint3
                          const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
                          int n_rows, int n_meas, int64_t* running, int64_t* e_out, int64_t* m_out,
                          int64_t* aux_out);
+int oracle_ising_byte_run(int8_t* s, int dim, int lx, int ly, int lz, const uint32_t key[2],
+                          const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
+                          int n_rows, int n_meas, int64_t* running, int64_t* e_out,
+                          int64_t* m_out, int64_t* aux_out);
+int oracle_potts_tables(int z, double beta, uint64_t* boltz, uint64_t* weight);
+int oracle_potts_run(int8_t* s, int dim, int lx, int ly, int lz, int q, const uint32_t key[2],
+                     double beta, uint32_t sweep0, const int64_t* schedule, int n_rows, int n_meas,
+                     int64_t* energy, int64_t* counts, int64_t* e_out, int64_t* counts_out,
+                     int64_t* aux_out);
 #endif

@@ -147,53 +147,74 @@ int64_t oracle_ising_bond_energy(const int8_t* s, int dim, int lx, int ly, int l
 }
 
 /* ---------------- MSC-stream checkerboard sweeps ---------------- */
-/* u of every lane of word w: planes[q] = bit plane q (MSB first) */
-static void msc_planes(uint32_t w, uint32_t sweep, uint32_t col, const uint32_t key[2],
-                       uint32_t planes[32]) {
-  for (uint32_t grp = 0; grp < 8; ++grp) {
-    uint32_t ctr[4] = {w, sweep, 0x01u | (grp << 8) | (col << 16), 0u}, out[4];
-    oracle_philox(ctr, key, out);
-    for (int q = 0; q < 4; ++q) planes[4 * grp + q] = out[q];
+/* Planes of one word, computed four at a time on first use. */
+typedef struct {
+  uint32_t w, sweep, col;
+  const uint32_t* key;
+  uint32_t planes[32];
+  unsigned have; /* bit g set: planes 4g..4g+3 computed */
+} PlaneCache;
+
+static uint32_t plane(PlaneCache* pc, int q) {
+  const unsigned grp = (unsigned)q >> 2;
+  if (!(pc->have & (1u << grp))) {
+    uint32_t ctr[4] = {pc->w, pc->sweep, 0x01u | (grp << 8) | (pc->col << 16), 0u}, out[4];
+    oracle_philox(ctr, pc->key, out);
+    for (int k = 0; k < 4; ++k) pc->planes[4 * grp + k] = out[k];
+    pc->have |= 1u << grp;
   }
+  return pc->planes[q];
 }
 
-static uint32_t lane_u(const uint32_t planes[32], int j) {
-  uint32_t u = 0;
-  for (int q = 0; q < 32; ++q) u |= ((planes[q] >> j) & 1u) << (31 - q);
-  return u;
+/* u_j < thr, comparing the bits of u_j (bit 31-q = bit j of plane q) from the top */
+static int lane_less(PlaneCache* pc, int j, uint32_t thr) {
+  for (int q = 0; q < 32; ++q) {
+    const uint32_t ub = (plane(pc, q) >> j) & 1u, tb = (thr >> (31 - q)) & 1u;
+    if (ub != tb) return ub < tb;
+  }
+  return 0; /* u == thr */
 }
 
-static int decide(uint32_t kind, uint32_t thr, uint32_t u) {
+static int decide(uint32_t kind, uint32_t thr, PlaneCache* pc, int j) {
   if (kind == 1) return 1;
-  if (kind == 2) return u < thr;
+  if (kind == 2) return lane_less(pc, j, thr);
   return 0;
 }
 
-/* One checkerboard sweep; returns (dE_b, dM, changed) through the pointers. */
+/* One checkerboard sweep; accumulates (dE_b, dM, changed) through the pointers. */
 static void msc_sweep(int8_t* s, const Geo* g, int algo, const uint32_t* kind, const uint32_t* thr,
                       const uint32_t key[2], uint32_t sweep, int64_t* d_eb, int64_t* d_m,
                       int64_t* changed) {
   const int wc = g->lx / 64;
-  uint32_t planes[32];
+  PlaneCache pc;
+  pc.key = key;
+  pc.sweep = sweep;
   for (int col = 0; col < 2; ++col) {
     for (int z = 0; z < g->lz; ++z) {
       for (int y = 0; y < g->ly; ++y) {
         const int p = (col + y + z) & 1;
         const int r = y + g->ly * z;
         for (int k = 0; k < wc; ++k) {
-          const uint32_t w = (uint32_t)(r * wc + k);
-          msc_planes(w, sweep, (uint32_t)col, key, planes);
+          pc.w = (uint32_t)(r * wc + k);
+          pc.col = (uint32_t)col;
+          pc.have = 0;
           for (int j = 0; j < 32; ++j) {
             const int x = 2 * (32 * k + j) + p;
             const int i = x + g->lx * (y + g->ly * z);
-            int field = 0;
-            for (int q = 0; q < g->z; ++q) field += s[g->nbr[(size_t)i * g->z + q]];
+            /* the 2 dim neighbours +-e_a (lattice.py:129-134), periodic */
+            const int xp = x + 1 == g->lx ? 0 : x + 1, xm = x == 0 ? g->lx - 1 : x - 1;
+            const int yp = y + 1 == g->ly ? 0 : y + 1, ym = y == 0 ? g->ly - 1 : y - 1;
+            int field = s[xp + g->lx * (y + g->ly * z)] + s[xm + g->lx * (y + g->ly * z)] +
+                        s[x + g->lx * (yp + g->ly * z)] + s[x + g->lx * (ym + g->ly * z)];
+            if (g->dim == 3) {
+              const int zp = z + 1 == g->lz ? 0 : z + 1, zm = z == 0 ? g->lz - 1 : z - 1;
+              field += s[x + g->lx * (y + g->ly * zp)] + s[x + g->lx * (y + g->ly * zm)];
+            }
             const int si = s[i];
-            const uint32_t u = lane_u(planes, j);
             if (algo == 0) {
               const int a = si * field;
               const int v = (g->z - a) / 2, c = 2 * v + (si > 0);
-              if (decide(kind[c], thr[c], u)) {
+              if (decide(kind[c], thr[c], &pc, j)) {
                 s[i] = (int8_t)(-si);
                 *d_eb += 2 * a;
                 *d_m -= 2 * si;
@@ -201,7 +222,7 @@ static void msc_sweep(int8_t* s, const Geo* g, int algo, const uint32_t* kind, c
               }
             } else {
               const int v = (field + g->z) / 2, c = 2 * v + (si > 0);
-              const int nw = decide(kind[c], thr[c], u) ? 1 : -1;
+              const int nw = decide(kind[c], thr[c], &pc, j) ? 1 : -1;
               if (nw != si) {
                 *d_eb += 2 * si * field;
                 *d_m += 2 * nw;
@@ -222,7 +243,13 @@ int oracle_ising_msc_run(int8_t* s, int dim, int lx, int ly, int lz, const uint3
                          int64_t* aux_out) {
   Geo g;
   if (dim < 2 || dim > 3 || lx % 64) return -1;
-  if (geo_init(&g, dim, lx, ly, lz)) return -2;
+  g.dim = dim;
+  g.lx = lx;
+  g.ly = ly;
+  g.lz = dim == 3 ? lz : 1;
+  g.z = 2 * dim;
+  g.n = lx * ly * g.lz;
+  g.nbr = NULL;
   int64_t e_b = running[0], m = running[1];
   uint32_t sweep = sweep0;
   for (int meas = 0; meas < n_meas; ++meas) {
@@ -246,6 +273,5 @@ int oracle_ising_msc_run(int8_t* s, int dim, int lx, int ly, int lz, const uint3
   }
   running[0] = e_b;
   running[1] = m;
-  geo_free(&g);
   return 0;
 }

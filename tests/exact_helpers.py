@@ -1,0 +1,103 @@
+"""Exact references for the statistical tests, read from ``golden/critmc_exact.json``.
+
+The fixture holds outputs of critmc's own exact layer (generated by
+``golden/make_golden.py``).  This module only evaluates canonical averages
+from the stored densities of states and restates Wolff's Gamma-method
+(critmc src/critmc/stats/autocorr.py:363-516, single primary observable,
+S = 1.5) for error bars of autocorrelated series.
+"""
+
+from __future__ import annotations
+
+import json
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "critmc_exact.json"
+
+
+@lru_cache(maxsize=1)
+def golden() -> dict:
+    return json.loads(GOLDEN.read_text())
+
+
+def kaufman_energy(beta: float, L: int, M: int | None = None) -> float:
+    """Kaufman's exact energy per site of the L x M torus at a tabulated beta."""
+    g = golden()
+    table = g["kaufman_energy"][str(L)] if M is None or M == L else g["kaufman_energy_rect"][f"{L}x{M}"]
+    return float(table[f"{beta:.10f}"])
+
+
+def beta_c() -> float:
+    return float(golden()["beta_c"])
+
+
+class JointDOS:
+    """Exact joint density of states g(E, O) from the fixture."""
+
+    def __init__(self, name: str):
+        d = golden()[name]
+        self.energies = np.asarray(d["energies"], dtype=np.float64)
+        self.orders = np.asarray(d["orders"], dtype=np.float64)
+        self.counts = np.asarray(d["counts"], dtype=np.float64)
+        self.n_sites = int(d["n_sites"])
+
+    def average(self, beta: float, fn, h: float = 0.0) -> float:
+        e, o = np.meshgrid(self.energies, self.orders, indexing="ij")
+        with np.errstate(divide="ignore"):
+            logw = np.log(self.counts) - beta * (e - h * o)
+        w = np.exp(logw - logw.max())
+        w /= w.sum()
+        return float(np.sum(w * fn(e, o)))
+
+
+def gamma_error(x: np.ndarray, S: float = 1.5) -> tuple[float, float, float]:
+    """(mean, error, tau_int) of a single series by Wolff's automatic windowing."""
+    x = np.asarray(x, dtype=np.float64)
+    n = x.size
+    mean = float(x.mean())
+    d = x - mean
+    if np.ptp(x) == 0:
+        return mean, 0.0, 0.5
+    t_max = n // 2
+    nfft = 1 << (2 * n - 1).bit_length()
+    spec = np.fft.rfft(d, n=nfft)
+    gam = np.fft.irfft(spec.real ** 2 + spec.imag ** 2, n=nfft)[: t_max + 1]
+    gam /= n - np.arange(t_max + 1)
+    # first W with exp(-W/tau_W) - tau_W/sqrt(W N) < 0, tau_W = S / ln(1 + 1/G(W))
+    w = np.arange(1, gam.size)
+    g_int = np.cumsum(gam[1:]) / gam[0]
+    tau_w = np.full(w.size, 1e-300)
+    pos = g_int > 0
+    with np.errstate(divide="ignore", over="ignore"):
+        tau_w[pos] = S / np.log1p(1.0 / g_int[pos])
+    tau_w = np.maximum(tau_w, 1e-300)
+    g = np.exp(-w / tau_w) - tau_w / np.sqrt(w * float(n))
+    hits = np.flatnonzero(g < 0)
+    w_opt = int(w[hits[0]]) if hits.size else int(w[-1])
+    c_f = gam[0] + 2.0 * gam[1:w_opt + 1].sum()
+    gam = gam + c_f / n  # bias of the subtracted mean
+    c_f = gam[0] + 2.0 * gam[1:w_opt + 1].sum()
+    tau = c_f / (2.0 * gam[0])
+    return mean, float(np.sqrt(c_f / n)) if c_f > 0 else float("nan"), float(tau)
+
+
+def ar1(seed: int, phi: float, n: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    e = rng.standard_normal(n)
+    x = np.empty(n)
+    x[0] = e[0]
+    for i in range(1, n):
+        x[i] = phi * x[i - 1] + e[i]
+    return x
+
+
+def pulls(series: list[np.ndarray], exact: float) -> np.ndarray:
+    """(Gamma-method mean - exact) / error for each independent chain."""
+    out = []
+    for x in series:
+        m, err, _ = gamma_error(x)
+        out.append((m - exact) / err)
+    return np.asarray(out)

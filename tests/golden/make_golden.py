@@ -1,0 +1,91 @@
+"""Generate the golden fixtures of the statistical parity tests from critmc itself.
+
+Run in a container where the reference package is importable::
+
+    PYTHONPATH=/path/to/critmc/src NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_golden.py
+
+It writes ``tests/golden/critmc_exact.json``: exact results of critmc's own
+exact layer (src/critmc/exact/kaufman.py, enumeration.py, chains.py,
+onsager.py) on the lattices the GPU tests sample.  The tests read only the
+JSON, so they run where critmc is absent.
+"""
+
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+
+from critmc import chain, square  # noqa: F401  (critmc must be on PYTHONPATH)
+from critmc.exact import chains, enumeration, kaufman, onsager
+from critmc.stats.autocorr import gamma_method
+
+OUT = Path(__file__).resolve().parent / "critmc_exact.json"
+
+
+def joint(jd) -> dict:
+    return {
+        "energies": jd.energies.tolist(),
+        "orders": jd.orders.tolist(),
+        "counts": jd.counts.tolist(),
+        "n_sites": int(jd.n_sites),
+    }
+
+
+def ar1(seed: int, phi: float, n: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    e = rng.standard_normal(n)
+    x = np.empty(n)
+    x[0] = e[0]
+    for i in range(1, n):
+        x[i] = phi * x[i - 1] + e[i]
+    return x
+
+
+def main() -> None:
+    out: dict = {"source": "critmc 1.0.0 exact layer"}
+    out["beta_c"] = float(onsager.BETA_C)
+    betas = [0.30, 0.40, float(onsager.BETA_C), 0.48, 0.60]
+    out["kaufman_energy"] = {
+        str(L): {f"{b:.10f}": float(kaufman.energy(b, L)) for b in betas} for L in (16, 32, 64, 128)
+    }
+    out["kaufman_energy_rect"] = {
+        f"{m}x{n}": {f"{b:.10f}": float(kaufman.energy(b, m, n)) for b in betas}
+        for m, n in ((64, 2), (64, 4), (64, 6), (128, 8))
+    }
+    # Gamma-method results on seeded AR(1) series (regenerated from the seed in the tests)
+    gam = []
+    for seed, phi, n in ((1, 0.0, 4000), (2, 0.9, 20000), (3, 0.98, 50000)):
+        x = ar1(seed, phi, n)
+        r = gamma_method(x)
+        gam.append({"seed": seed, "phi": phi, "n": n, "value": r.value, "error": r.error,
+                    "tau_int": r.tau_int, "window": int(r.window)})
+    out["gamma_method_ar1"] = gam
+    out["ising_dos_square4"] = joint(enumeration.ising_joint_dos(square(4)))
+    out["ising_dos_square4x2"] = joint(enumeration.ising_joint_dos(square(4, 2)))
+    out["ising_dos_chain8"] = joint(enumeration.ising_joint_dos(chain(8)))
+    out["potts3_dos_square4x2"] = joint(enumeration.potts_joint_dos(square(4, 2), 3))
+    out["potts4_dos_square2"] = joint(enumeration.potts_joint_dos(square(2), 4))
+    ring = {}
+    for n in (2, 3):
+        for beta in (0.7, 1.1):
+            for N in (4, 8):
+                ring[f"n{n}_N{N}_b{beta}"] = {
+                    "energy": float(chains.on_ring_energy(beta, N, n)),
+                    "specific_heat": float(chains.on_ring_specific_heat(beta, N, n)),
+                }
+    out["on_ring"] = ring
+    # EA +-J couplings on a 4x4 torus and the energies of all 2^16 states
+    rng = np.random.default_rng(20261203)
+    lat = square(4)
+    J = rng.choice([-1.0, 1.0], size=lat.n_bonds)
+    e = enumeration.ea_energies(lat, J)
+    out["ea_square4"] = {"couplings": J.tolist(), "energies_first_64": e[:64].tolist(),
+                         "energy_sum": float(e.sum()), "energy_min": float(e.min())}
+    OUT.write_text(json.dumps(out, indent=1) + "\n")
+    print(f"wrote {OUT}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,73 @@
+"""Pin the CPU oracle (and the test harness) against critmc's exact results.
+
+The oracle is the bit-exact reference of the GPU kernels; these tests show
+that the oracle itself samples the right distributions, by critmc's own
+exact layer (fixtures from tests/golden/make_golden.py) and the batch-means
+criterion |z| < 4.5 of critmc tests/conftest.py.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import assert_consistent
+from exact_helpers import JointDOS, ar1, gamma_error, golden, kaufman_energy
+
+import oracle
+
+
+@pytest.mark.parametrize("case", golden()["gamma_method_ar1"], ids=lambda c: f"phi{c['phi']}")
+def test_gamma_method_matches_critmc(case):
+    x = ar1(case["seed"], case["phi"], case["n"])
+    m, err, tau = gamma_error(x)
+    assert m == pytest.approx(case["value"], rel=1e-12, abs=1e-14)
+    assert err == pytest.approx(case["error"], rel=1e-10)
+    assert tau == pytest.approx(case["tau_int"], rel=1e-10)
+
+
+def _ising_state(n, seed):
+    return (2 * np.random.default_rng(seed).integers(0, 2, n) - 1).astype(np.int8)
+
+
+@pytest.mark.parametrize("code", [0, 2])
+def test_oracle_byte_ising_matches_enumeration(code):
+    jd = JointDOS("ising_dos_square4")
+    beta, n = 0.35, 16
+    s = _ising_state(n, 1)
+    e_b, m, _, _ = oracle.ising_byte_run(s, (4, 4), (3, 4), beta, 0.0, [[code, 1]], 120_000)
+    e_b, m = e_b[2000:], m[2000:]
+    assert_consistent(e_b, jd.average(beta, lambda e, o: e))
+    assert_consistent((m / n) ** 2, jd.average(beta, lambda e, o: (o / n) ** 2))
+
+
+@pytest.mark.parametrize("code", [0, 2])
+def test_oracle_byte_ising_in_a_field(code):
+    jd = JointDOS("ising_dos_square4")
+    beta, h, n = 0.3, 0.4, 16
+    s = _ising_state(n, 2)
+    e_b, m, _, _ = oracle.ising_byte_run(s, (4, 4), (5, 6), beta, h, [[code, 1]], 120_000)
+    e_b, m = e_b[2000:], m[2000:]
+    assert_consistent(e_b - h * m, jd.average(beta, lambda e, o: e - h * o, h=h))
+    assert_consistent(m / n, jd.average(beta, lambda e, o: o / n, h=h))
+
+
+@pytest.mark.parametrize("code", [0, 2])
+def test_oracle_potts_matches_enumeration(code):
+    jd = JointDOS("potts3_dos_square4x2")
+    beta, q, n = 0.8, 3, 8
+    s = np.random.default_rng(3).integers(0, q, n).astype(np.int8)
+    e, counts, _, _, _ = oracle.potts_run(s, (4, 2), q, (7, 8), beta, [[code, 1]], 150_000)
+    e, counts = e[2000:], counts[2000:]
+    assert_consistent(e, jd.average(beta, lambda en, o: en))
+    rho = counts / n
+    m2 = (q * np.sum(rho * rho, axis=1) - 1.0) / (q - 1.0)
+    assert_consistent(m2, jd.average(beta, lambda en, o: (o / n ** 2 - 1.0) / (q - 1.0)))
+
+
+@pytest.mark.parametrize("code", [0, 2])
+def test_oracle_msc_matches_kaufman(code):
+    """The multi-spin-coded stream samples the 64x4 torus (Kaufman's exact energy)."""
+    beta = 0.4
+    s = _ising_state(256, 4)
+    e_b, _, _, _ = oracle.ising_msc_run(s, (64, 4), (9, 10), beta, 0.0, [[code, 1]], 40_000)
+    assert_consistent(e_b[1000:] / 256.0, kaufman_energy(beta, 64, 4))

@@ -42,12 +42,17 @@ def nvcc() -> str:
     return exe
 
 
+# translation units whose float arithmetic must match a host replay exactly
+PER_FILE_FLAGS = {"on_models.cu": ["--fmad=false"]}
+
+
 def _headers() -> list[Path]:
     return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
 
 
 def _compile(src: Path, obj: Path, extra: list[str]) -> None:
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *PER_FILE_FLAGS.get(src.name, []), *extra, "-c", str(src),
+           "-o", str(obj)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stdout}\n{res.stderr}")

@@ -44,6 +44,11 @@ SIGNATURES: dict[str, tuple] = {
          _P, _P],
     ),
     "critmc_potts_tables": (_I32, [_I32, _D, _P, _P]),
+    "critmc_on_run": (
+        _I32,
+        [_P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P,
+         _P, _P, _P],
+    ),
 }
 
 

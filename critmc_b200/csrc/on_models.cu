@@ -1,0 +1,415 @@
+// O(n) vector models (XY n = 2, Heisenberg n = 3) with FP32 unit spins:
+// checkerboard heat bath (von Mises / exponential-in-cos), over-relaxation and
+// Gaussian-step Metropolis, one thread block per chain running the whole
+// schedule, with FP64 per-measurement energy, magnetisation and stiffness
+// sums reduced in a fixed order.  The elementary functions come from
+// fpmath.h and this file is compiled without floating-point contraction, so a
+// CPU replay follows the spins bit for bit.
+//
+// Replaces critmc src/critmc/kernels/on.py:349-418 (`run`), :113-137
+// (`metropolis_sweep`), :141-183 (`overrelax_sweep`), :187-261
+// (`_von_mises`, `heatbath_sweep`), :36-87 (measurements, `normalize`).
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "fpmath.h"
+#include "geom.cuh"
+#include "host_common.h"
+
+namespace critmc {
+
+constexpr int ON_PCHAINS = 1024;
+constexpr int ON_MAX_GROUPS = 16;
+constexpr int ON_MAX_ROWS = 8;
+constexpr int ON_SMEM_MAX = 200 * 1024;
+constexpr int ON_MAX_VM_ITER = 64;  // von Mises rejection rounds (acceptance > 0.65 each)
+
+struct OnParams {
+  float* spins;
+  double* e_out;
+  double* m_out;
+  double* sc_out;
+  double* ss_out;
+  long long* aux_out;
+  ByteGeom g;
+  int n_chains, chain0, chains_per_group, n_meas, n_rows;
+  int codes[ON_MAX_ROWS];
+  int reps[ON_MAX_ROWS];
+  int resident;
+  uint32_t sweep0;
+  float beta[ON_MAX_GROUPS];
+  float step[ON_MAX_GROUPS];
+  uint32_t keys[ON_PCHAINS][2];
+};
+
+constexpr float ON_PI = 3.14159265358979323846f;
+
+// uniform in [0, 1) and in (0, 1] from 24 random bits
+__device__ __forceinline__ float u01(uint32_t w) { return critmc_u01f(w); }
+__device__ __forceinline__ float u01o(uint32_t w) { return critmc_u01f_open0(w); }
+
+// Box-Muller pair of standard normals
+__device__ __forceinline__ void gauss2(uint32_t a, uint32_t b, float& g0, float& g1) {
+  const float rad = sqrtf(-2.0f * cm_logf(u01o(a)));
+  float sn, cs;
+  cm_sincosf(2.0f * ON_PI * u01(b), &sn, &cs);
+  g0 = rad * cs;
+  g1 = rad * sn;
+}
+
+// neighbour slots in critmc's column order (+x, -x, +y, -y, +z, -z)
+template <int Z>
+__device__ __forceinline__ void on_neighbours(const ByteGeom& g, int c, uint32_t s, uint32_t* nb,
+                                              int& y, int& z) {
+  int r, i;
+  byte_row_index(g, s, r, i);
+  uint32_t raw[Z];
+  byte_neighbours<Z>(g, c, r, i, raw);
+  y = r;
+  z = 0;
+  if constexpr (Z == 6) {
+    y = r % g.ly;
+    z = r / g.ly;
+  }
+  const int p = (c + y + z) & 1;
+  nb[0] = p ? raw[1] : raw[0];  // +x
+  nb[1] = p ? raw[0] : raw[1];  // -x
+  if constexpr (Z >= 4) {
+    nb[2] = raw[3];  // +y
+    nb[3] = raw[2];  // -y
+  }
+  if constexpr (Z == 6) {
+    nb[4] = raw[5];  // +z
+    nb[5] = raw[4];  // -z
+  }
+}
+
+// Best & Fisher (1979) von Mises sampler, critmc kernels/on.py:187-204
+// (at most ON_MAX_VM_ITER rounds; with a per-round acceptance above 0.65 the
+// bound is reached with probability below 1e-29, and then the last proposal is kept)
+__device__ __forceinline__ float von_mises(float kappa, const critmc_u32x4& r0, uint32_t slot,
+                                           uint32_t sweep, uint32_t col, uint32_t k0, uint32_t k1) {
+  if (kappa < 1e-8f) return ON_PI * (2.0f * u01(r0.v[0]) - 1.0f);
+  const float root = sqrtf(1.0f + 4.0f * kappa * kappa);
+  const float tau = 1.0f + root;
+  const float rho = 2.0f * kappa * tau / ((root + 1.0f) * (tau + sqrtf(2.0f * tau)));
+  const float r = (1.0f + rho * rho) / (2.0f * rho);
+  float f = 1.0f;
+  uint32_t a = r0.v[0], b = r0.v[1];
+  for (int it = 0; it < ON_MAX_VM_ITER; ++it) {
+    if (it > 0) {
+      const critmc_u32x4 x =
+          critmc_philox4x32(slot, sweep, CRITMC_TAG_SITE2 | (col << 16), (uint32_t)it, k0, k1);
+      a = x.v[0];
+      b = x.v[1];
+    }
+    const float zz = cm_cosf(ON_PI * u01(a));
+    f = (1.0f + r * zz) / (r + zz);
+    const float c = kappa * (r - f);
+    const float u2 = u01(b);
+    if (c * (2.0f - c) - u2 > 0.0f || cm_logf(c / u2) + 1.0f - c >= 0.0f) break;
+  }
+  const float theta = cm_acosf(fminf(1.0f, fmaxf(-1.0f, f)));
+  return u01(r0.v[2]) < 0.5f ? theta : -theta;
+}
+
+template <int N, int Z>
+__global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[16];
+  const int lchain = blockIdx.x;
+  const int chain = P.chain0 + lchain;
+  const int group = chain / P.chains_per_group;
+  const ByteGeom& g = P.g;
+  const uint32_t k0 = P.keys[lchain][0], k1 = P.keys[lchain][1];
+  const size_t n_sites = 2 * (size_t)g.slots;
+  float* gl = P.spins + (size_t)chain * N * n_sites;
+  float* lat = P.resident ? reinterpret_cast<float*>(smem_raw) : gl;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (P.resident)
+    for (size_t j = tid; j < N * n_sites; j += nt) lat[j] = gl[j];
+  __syncthreads();
+  const float beta = P.beta[group], step = P.step[group];
+  constexpr int DIM = Z / 2;
+  uint32_t sweep = P.sweep0;
+
+  for (int meas = 0; meas < P.n_meas; ++meas) {
+    long long nacc = 0;
+    for (int row = 0; row < P.n_rows; ++row) {
+      const int code = P.codes[row];
+      for (int rep = 0; rep < P.reps[row]; ++rep) {
+        for (int c = 0; c < 2; ++c) {
+          for (uint32_t s = tid; s < g.slots; s += nt) {
+            uint32_t nb[Z];
+            int y, z;
+            on_neighbours<Z>(g, c, s, nb, y, z);
+            float* own[N];
+            const float* oth[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+              own[k] = lat + ((size_t)k * 2 + c) * g.slots;
+              oth[k] = lat + ((size_t)k * 2 + (c ^ 1)) * g.slots;
+            }
+            float h[N], sv[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+              float acc = 0.0f;
+#pragma unroll
+              for (int q = 0; q < Z; ++q) acc += oth[k][nb[q]];
+              h[k] = acc;
+              sv[k] = own[k][s];
+            }
+            if (code == CRITMC_OVERRELAX) {
+              // on.py:141-183: reflect about the local field; keep the spin if h = 0
+              float hh = 0.0f, sh = 0.0f;
+#pragma unroll
+              for (int k = 0; k < N; ++k) {
+                hh += h[k] * h[k];
+                sh += sv[k] * h[k];
+              }
+              if (hh != 0.0f) {
+                const float f = 2.0f * sh / hh;
+#pragma unroll
+                for (int k = 0; k < N; ++k) own[k][s] = f * h[k] - sv[k];
+              }
+              continue;
+            }
+            const critmc_u32x4 r0 =
+                critmc_philox4x32(s, sweep, CRITMC_TAG_SITE | ((uint32_t)c << 16), 0u, k0, k1);
+            if (code == CRITMC_HEATBATH) {
+              float hn = 0.0f;
+#pragma unroll
+              for (int k = 0; k < N; ++k) hn += h[k] * h[k];
+              hn = sqrtf(hn);
+              const float kappa = beta * hn;
+              if constexpr (N == 2) {
+                const float phi0 = hn > 0.0f ? cm_atan2f(h[1], h[0]) : 0.0f;
+                const float phi = phi0 + von_mises(kappa, r0, s, sweep, (uint32_t)c, k0, k1);
+                float sn, cs;
+                cm_sincosf(phi, &sn, &cs);
+                own[0][s] = cs;
+                own[1][s] = sn;
+              } else {
+                if (hn == 0.0f) {
+                  float g0, g1, g2, g3;
+                  gauss2(r0.v[0], r0.v[1], g0, g1);
+                  gauss2(r0.v[2], r0.v[3], g2, g3);
+                  const float nrm = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+                  own[0][s] = g0 / nrm;
+                  own[1][s] = g1 / nrm;
+                  own[2][s] = g2 / nrm;
+                  continue;
+                }
+                const float rr = u01(r0.v[0]);
+                float u = kappa < 1e-8f ? 2.0f * rr - 1.0f
+                                        : 1.0f + cm_logf(rr + (1.0f - rr) * cm_expf(-2.0f * kappa)) / kappa;
+                u = fminf(1.0f, fmaxf(-1.0f, u));
+                const float hx = h[0] / hn, hy = h[1] / hn, hz = h[2] / hn;
+                float ax = 1.0f, ay = 0.0f, az = 0.0f;
+                if (!(fabsf(hx) < 0.9f)) {
+                  ax = 0.0f;
+                  ay = 1.0f;
+                }
+                const float proj = ax * hx + ay * hy + az * hz;
+                float e1x = ax - proj * hx, e1y = ay - proj * hy, e1z = az - proj * hz;
+                const float nrm = sqrtf(e1x * e1x + e1y * e1y + e1z * e1z);
+                e1x /= nrm;
+                e1y /= nrm;
+                e1z /= nrm;
+                const float e2x = hy * e1z - hz * e1y, e2y = hz * e1x - hx * e1z, e2z = hx * e1y - hy * e1x;
+                const float phi = 2.0f * ON_PI * u01(r0.v[1]);
+                const float w = sqrtf(fmaxf(0.0f, 1.0f - u * u));
+                float sp, cp;
+                cm_sincosf(phi, &sp, &cp);
+                own[0][s] = u * hx + w * (cp * e1x + sp * e2x);
+                own[1][s] = u * hy + w * (cp * e1y + sp * e2y);
+                own[2][s] = u * hz + w * (cp * e1z + sp * e2z);
+              }
+            } else {
+              // on.py:113-137: Gaussian step, renormalise, accept exp(-beta dE)
+              float gv[4];
+              gauss2(r0.v[0], r0.v[1], gv[0], gv[1]);
+              uint32_t uacc = r0.v[2];
+              if constexpr (N == 3) {
+                gauss2(r0.v[2], r0.v[3], gv[2], gv[3]);
+                uacc = critmc_philox4x32(s, sweep, CRITMC_TAG_SITE2 | ((uint32_t)c << 16), 0u, k0, k1).v[0];
+              }
+              float tr[N], nrm = 0.0f;
+#pragma unroll
+              for (int k = 0; k < N; ++k) {
+                tr[k] = sv[k] + step * gv[k];
+                nrm += tr[k] * tr[k];
+              }
+              nrm = sqrtf(nrm);
+              float d_e = 0.0f;
+#pragma unroll
+              for (int k = 0; k < N; ++k) {
+                tr[k] /= nrm;
+                d_e -= (tr[k] - sv[k]) * h[k];
+              }
+              if (d_e <= 0.0f || u01(uacc) < cm_expf(-beta * d_e)) {
+#pragma unroll
+                for (int k = 0; k < N; ++k) own[k][s] = tr[k];
+                ++nacc;
+              }
+            }
+          }
+          __syncthreads();
+        }
+        ++sweep;
+      }
+    }
+    // normalise every spin (on.py:79-87), then measure in FP64
+    for (uint32_t j = tid; j < 2 * g.slots; j += nt) {
+      float v[N], nrm = 0.0f;
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        v[k] = lat[(size_t)k * n_sites + j];
+        nrm += v[k] * v[k];
+      }
+      nrm = sqrtf(nrm);
+#pragma unroll
+      for (int k = 0; k < N; ++k) lat[(size_t)k * n_sites + j] = v[k] / nrm;
+    }
+    __syncthreads();
+    double e = 0.0, m[N], sc[DIM], ss[DIM];
+#pragma unroll
+    for (int k = 0; k < N; ++k) m[k] = 0.0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) sc[a] = ss[a] = 0.0;
+    for (uint32_t j = tid; j < 2 * g.slots; j += nt) {
+      const int c = j >= g.slots;
+      const uint32_t s = j - c * g.slots;
+      uint32_t nb[Z];
+      int y, z;
+      on_neighbours<Z>(g, c, s, nb, y, z);
+      double si[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        si[k] = lat[((size_t)k * 2 + c) * g.slots + s];
+        m[k] += si[k];
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        double sj[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) sj[k] = lat[((size_t)k * 2 + (c ^ 1)) * g.slots + nb[2 * a]];
+        double dot = 0.0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) dot += si[k] * sj[k];
+        e -= dot;
+        sc[a] += si[0] * sj[0] + si[1] * sj[1];
+        ss[a] += si[0] * sj[1] - si[1] * sj[0];
+      }
+    }
+    e = block_sum(e, red);
+#pragma unroll
+    for (int k = 0; k < N; ++k) m[k] = block_sum(m[k], red);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      sc[a] = block_sum(sc[a], red);
+      ss[a] = block_sum(ss[a], red);
+    }
+    const long long acc_all = block_sum(nacc, reinterpret_cast<long long*>(red));
+    if (tid == 0) {
+      const size_t o = (size_t)chain * P.n_meas + meas;
+      P.e_out[o] = e;
+#pragma unroll
+      for (int k = 0; k < N; ++k) P.m_out[o * N + k] = m[k];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        P.sc_out[o * DIM + a] = sc[a];
+        P.ss_out[o * DIM + a] = ss[a];
+      }
+      P.aux_out[4 * o + 0] = acc_all;
+      P.aux_out[4 * o + 1] = 0;
+      P.aux_out[4 * o + 2] = 0;
+      P.aux_out[4 * o + 3] = 0;
+    }
+  }
+  __syncthreads();
+  if (P.resident)
+    for (size_t j = tid; j < N * n_sites; j += nt) gl[j] = lat[j];
+}
+
+static thread_local OnParams g_on;
+
+}  // namespace critmc
+
+using namespace critmc;
+
+extern "C" int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                                 int32_t n, int32_t n_chains, const uint32_t* keys,
+                                 const double* betas, const double* steps, int32_t n_groups,
+                                 uint32_t sweep0, const int64_t* schedule, int32_t n_rows,
+                                 int32_t n_meas, double* e_out, double* m_out, double* stiff_c_out,
+                                 double* stiff_s_out, int64_t* aux_out, void* stream) {
+  clear_error();
+  OnParams& P = g_on;
+  int st = byte_geom(dim, lx, ly, lz, P.g);
+  if (st) return st;
+  if (n != 2 && n != 3) return fail(CRITMC_ERR_UNSUPPORTED, "O(n) kernels handle n = 2 and n = 3");
+  if (!spins || !keys || !betas || !steps || !e_out || !m_out || !stiff_c_out || !stiff_s_out || !aux_out)
+    return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (n_chains < 1 || n_groups < 1 || n_groups > ON_MAX_GROUPS || n_chains % n_groups)
+    return fail(CRITMC_ERR_INVALID, "need n_chains >= 1 and 1 <= n_groups <= 16 dividing n_chains");
+  if (n_meas < 0) return fail(CRITMC_ERR_INVALID, "n_meas must not be negative");
+  if (!schedule || n_rows < 1 || n_rows > ON_MAX_ROWS) return fail(CRITMC_ERR_INVALID, "schedule must have 1..8 rows");
+  long long per_meas = 0;
+  for (int r = 0; r < n_rows; ++r) {
+    const int64_t code = schedule[2 * r], reps = schedule[2 * r + 1];
+    if (code != CRITMC_METROPOLIS && code != CRITMC_HEATBATH && code != CRITMC_OVERRELAX)
+      return fail(CRITMC_ERR_UNSUPPORTED, "O(n) kernels run metropolis, heatbath and overrelax rows");
+    if (reps < 1 || reps > (1 << 20)) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be in [1, 2^20]");
+    P.codes[r] = (int)code;
+    P.reps[r] = (int)reps;
+    per_meas += reps;
+  }
+  if ((long long)sweep0 + per_meas * n_meas > 0xFFFFFFFFLL)
+    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+  if (n_meas == 0) return CRITMC_OK;
+  for (int gi = 0; gi < n_groups; ++gi) {
+    if (!std::isfinite(betas[gi]) || !std::isfinite(steps[gi]))
+      return fail(CRITMC_ERR_INVALID, "betas and steps must be finite");
+    P.beta[gi] = (float)betas[gi];
+    P.step[gi] = (float)steps[gi];
+  }
+  P.spins = spins;
+  P.e_out = e_out;
+  P.m_out = m_out;
+  P.sc_out = stiff_c_out;
+  P.ss_out = stiff_s_out;
+  P.aux_out = (long long*)aux_out;
+  P.n_rows = n_rows;
+  P.n_chains = n_chains;
+  P.chains_per_group = n_chains / n_groups;
+  P.n_meas = n_meas;
+  P.sweep0 = sweep0;
+  const size_t lat_bytes = (size_t)n * 2 * P.g.slots * sizeof(float);
+  P.resident = lat_bytes <= (size_t)ON_SMEM_MAX;
+  const size_t smem = P.resident ? lat_bytes : 0;
+  int threads = (int)std::min<uint32_t>(512, ((P.g.slots + 31) / 32) * 32);
+  threads = std::max(threads, 32);
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int c0 = 0; c0 < n_chains; c0 += ON_PCHAINS) {
+    const int nc = std::min(ON_PCHAINS, n_chains - c0);
+    P.chain0 = c0;
+    std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
+    auto launch = [&](auto kern) {
+      if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<nc, threads, smem, s>>>(P);
+    };
+    const int key = n * 10 + dim;
+    switch (key) {
+      case 21: launch(on_run_kernel<2, 2>); break;
+      case 22: launch(on_run_kernel<2, 4>); break;
+      case 23: launch(on_run_kernel<2, 6>); break;
+      case 31: launch(on_run_kernel<3, 2>); break;
+      case 32: launch(on_run_kernel<3, 4>); break;
+      default: launch(on_run_kernel<3, 6>); break;
+    }
+    if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  }
+  return CRITMC_OK;
+}

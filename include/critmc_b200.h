@@ -143,6 +143,32 @@ int32_t critmc_potts_run(int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int
  * hb_weight[#neighbours in state k]).                                       */
 int32_t critmc_potts_tables(int32_t z, double beta, uint64_t* boltz_thr, uint64_t* hb_weight);
 
+/* ---- O(n) vector models (n = 2 XY, n = 3 Heisenberg), FP32 spins ------------
+ * Layout of one chain: comp[n][colour][row][i] (float32, structure of
+ * arrays, same colour-major site order as the byte lattices).  Even extents,
+ * dim 1..3.  One block per chain; the lattice is staged in shared memory when
+ * n * lx*ly*lz * 4 bytes <= 200 KiB.  betas, steps: HOST [n_groups]
+ * (inverse temperature and Metropolis step size of each group).
+ * Random words of a site per sweep: Philox(slot, sweep, 0x02 | colour << 16, 0)
+ * and, for rejection steps and extra Gaussians, Philox(slot, sweep,
+ * 0x03 | colour << 16, k).
+ * Schedule rows: metropolis (0), heatbath (2), overrelax (5).
+ * After each schedule application every spin is renormalised and the
+ * observables are accumulated in FP64 in a fixed order (deterministic):
+ * e_out[n_chains][n_meas] = -sum_<ij> S_i.S_j, m_out[..][n],
+ * stiff_c_out / stiff_s_out[..][dim] (per-axis sums of S_i^0 S_j^0 + S_i^1 S_j^1
+ * and S_i^0 S_j^1 - S_i^1 S_j^0 over bonds i -> i + e_a), aux_out[..][4]
+ * (accepted Metropolis moves in column 0).
+ * Replaces critmc kernels/on.py:349-418 (`run`), :113-137 (metropolis_sweep),
+ * :141-183 (overrelax_sweep), :187-261 (von Mises / heat bath),
+ * :36-87 (energy, magnetization, stiffness_sums, normalize).             */
+int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t n,
+                      int32_t n_chains, const uint32_t* keys, const double* betas,
+                      const double* steps, int32_t n_groups, uint32_t sweep0,
+                      const int64_t* schedule, int32_t n_rows, int32_t n_meas, double* e_out,
+                      double* m_out, double* stiff_c_out, double* stiff_s_out, int64_t* aux_out,
+                      void* stream);
+
 /* Energy E_b = -sum_<ij> s_i s_j and magnetisation M of MSC chains, written
  * to out[n_chains][2] (device).  critmc kernels/ising.py:32-45.           */
 int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,

@@ -33,7 +33,8 @@ def build() -> Path:
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
-        srcs = list(HERE.glob("oracle_*.c")) + [HERE / "oracle.h"]
+        srcs = list(HERE.glob("oracle_*.c")) + [HERE / "oracle.h",
+                                                 HERE.parent / "critmc_b200" / "csrc" / "fpmath.h"]
         if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(p.stat().st_mtime for p in srcs):
             build()
         _lib = ctypes.CDLL(str(LIB_PATH))
@@ -62,6 +63,8 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_potts_tables.restype = _I
     L.oracle_potts_run.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _U32, _P, _I, _I, _P, _P, _P, _P, _P]
     L.oracle_potts_run.restype = _I
+    L.oracle_on_run.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _D, _U32, _P, _I, _I, _P, _P, _P, _P, _P]
+    L.oracle_on_run.restype = _I
 
 
 def _ptr(a: np.ndarray) -> int:
@@ -182,3 +185,25 @@ def potts_run(s, shape, q, key, beta, schedule, n_meas, sweep0=0, energy=None, c
     if rc != 0:
         raise ValueError(f"oracle_potts_run failed ({rc})")
     return e, co, aux, int(en[0]), cnt
+
+
+def on_run(s, shape, n, key, beta, step, schedule, n_meas, sweep0=0):
+    """Replay the O(n) checkerboard sweeps on ``s`` (float32 (N, n), critmc order, in place).
+
+    Returns ``(E, M, stiff_c, stiff_s, aux)`` like critmc's ``ON.advance``.
+    """
+    if not (isinstance(s, np.ndarray) and s.dtype == np.float32 and s.flags["C_CONTIGUOUS"]):
+        raise TypeError("s must be a C-contiguous float32 array (it is updated in place)")
+    dim = len(shape)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+    e = np.zeros(n_meas)
+    m = np.zeros((n_meas, n))
+    sc = np.zeros((n_meas, dim))
+    ss = np.zeros((n_meas, dim))
+    aux = np.zeros((n_meas, 4), dtype=np.int64)
+    rc = lib().oracle_on_run(_ptr(s), dim, *_dims(shape), n, _ptr(k), beta, step, sweep0, _ptr(sched),
+                             len(sched), n_meas, _ptr(e), _ptr(m), _ptr(sc), _ptr(ss), _ptr(aux))
+    if rc != 0:
+        raise ValueError(f"oracle_on_run failed ({rc})")
+    return e, m, sc, ss, aux

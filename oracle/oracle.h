@@ -19,4 +19,8 @@ int oracle_potts_run(int8_t* s, int dim, int lx, int ly, int lz, int q, const ui
                      double beta, uint32_t sweep0, const int64_t* schedule, int n_rows, int n_meas,
                      int64_t* energy, int64_t* counts, int64_t* e_out, int64_t* counts_out,
                      int64_t* aux_out);
+int oracle_on_run(float* s, int dim, int lx, int ly, int lz, int n, const uint32_t key[2],
+                  double beta, double step, uint32_t sweep0, const int64_t* schedule, int n_rows,
+                  int n_meas, double* e_out, double* m_out, double* sc_out, double* ss_out,
+                  int64_t* aux_out);
 #endif

@@ -1,0 +1,75 @@
+"""The C ABI library loads without a GPU and exports every declared entry point."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from critmc_b200 import _lib
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "critmc_b200.h"
+
+
+def declared() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(critmc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    names = declared()
+    assert len(names) >= 10
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_python_binding_covers_the_header():
+    assert set(declared()) <= set(_lib.SIGNATURES), set(declared()) - set(_lib.SIGNATURES)
+
+
+def test_version_and_error_text():
+    L = _lib.lib()
+    assert L.critmc_version() >= 100
+    kind = np.zeros(16, np.uint32)
+    thr = np.zeros(16, np.uint32)
+    st = L.critmc_ising_class_table(9, 4, 0.4, 0.0, kind.ctypes.data, thr.ctypes.data, None)
+    assert st == -3
+    assert "metropolis and heatbath" in _lib.last_error()
+
+
+def test_invalid_arguments_fail_before_any_launch():
+    """Validation runs on the host: no GPU is touched for bad arguments."""
+    L = _lib.lib()
+    sched = np.array([[0, 1]], np.int64)
+    keys = np.zeros(2, np.uint32)
+    tables = np.zeros(64, np.uint32)
+    # odd extent
+    st = L.critmc_ising_byte_run(None, 2, 5, 4, 1, 1, keys.ctypes.data, tables.ctypes.data, 1, 0,
+                                 sched.ctypes.data, 1, 1, None, None, None, None, None)
+    assert st in (-1, -3)
+    # lx not a multiple of 64 for the MSC layout
+    st = L.critmc_ising_msc_run(None, 2, 96, 4, 1, 1, keys.ctypes.data, tables.ctypes.data, 1, 0,
+                                sched.ctypes.data, 1, 1, None, None, None, None, None, 0, 8, None)
+    assert st == -3 and "64" in _lib.last_error()
+    # cluster move in a schedule
+    bad = np.array([[3, 1]], np.int64)
+    dummy = ctypes.c_void_p(16)
+    st = L.critmc_potts_run(dummy, 2, 4, 4, 1, 3, 1, keys.ctypes.data,
+                            np.array([1.0]).ctypes.data, 1, 0, bad.ctypes.data, 1, 1, dummy, dummy,
+                            dummy, dummy, dummy, None)
+    assert st == -3
+
+
+@pytest.mark.parametrize("beta", [0.0, 0.44, 3.0])
+def test_potts_tables_are_monotone(beta):
+    b = np.zeros(8, np.uint64)
+    w = np.zeros(8, np.uint64)
+    _lib.call("critmc_potts_tables", 4, beta, b.ctypes.data, w.ctypes.data)
+    assert b[0] == 1 << 32
+    assert np.all(np.diff(b[:5].astype(np.float64)) <= 0)
+    assert w[4] == 1 << 52 if beta > 0 else True

@@ -1,0 +1,83 @@
+"""O(n) kernels: agreement with the FP32 CPU replay, and critmc's exact ring results."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import assert_consistent
+from exact_helpers import golden
+
+import oracle
+from critmc_b200 import ON, Simulation, chain, hypercubic, square
+from critmc_b200.on_models import ONChain
+
+pytestmark = pytest.mark.gpu
+
+# Spins are bit-identical (shared elementary functions, no contraction); the
+# FP64 observables are reduced in a different order, so they agree to rounding.
+# The brief's bar is 1e-5 relative; the test asks for 1e-12.
+RTOL = 1e-12
+
+CASES = [
+    ((16, 16), 2, [[2, 1], [5, 4]], 1.0),
+    ((16, 16), 2, [[0, 1]], 1.1),
+    ((16, 16), 3, [[2, 1], [5, 4]], 0.7),
+    ((16, 16), 3, [[0, 2]], 0.9),
+    ((8, 6, 4), 3, [[2, 1], [5, 1]], 0.7),
+    ((32,), 2, [[2, 1], [0, 1], [5, 2]], 1.1),
+    ((128, 130), 2, [[2, 1]], 1.0),  # larger than shared memory: updated in HBM
+]
+
+
+@pytest.mark.parametrize("shape,n,sched,beta", CASES)
+def test_on_agrees_with_replay(cuda, shape, n, sched, beta):
+    model = ON(hypercubic(shape), n)
+    rng = np.random.default_rng(n * 7 + len(shape))
+    s0 = model.initial_state("random", rng).astype(np.float32)
+    key = rng.integers(0, 2**32, 2, dtype=np.uint64).astype(np.uint32)
+    ch = ONChain(model, s0, key, cuda)
+    running = {"step": 0.8}
+    n_meas = 20
+    raw = ch.advance(running, beta, np.array(sched), n_meas)
+    s_ref = s0.copy()
+    e, m, sc, ss, aux = oracle.on_run(s_ref, shape, n, key, beta, 0.8, sched, n_meas)
+    scale = model.n_sites  # observables are sums over sites/bonds
+    np.testing.assert_allclose(raw["E"], e, rtol=RTOL, atol=RTOL * scale)
+    np.testing.assert_allclose(raw["M"], m, rtol=RTOL, atol=RTOL * scale)
+    np.testing.assert_allclose(raw["stiff_c"], sc, rtol=RTOL, atol=RTOL * scale)
+    np.testing.assert_allclose(raw["stiff_s"], ss, rtol=RTOL, atol=RTOL * scale)
+    np.testing.assert_array_equal(ch.fetch().astype(np.float32), s_ref)
+    np.testing.assert_array_equal(raw["aux"], aux)
+
+
+@pytest.mark.parametrize("n_comp", [2, 3])
+@pytest.mark.parametrize("updates", ["metropolis", "heatbath", "metropolis+3*overrelax"])
+def test_on_ring_matches_transfer_operator(cuda, n_comp, updates):
+    """critmc tests/test_kernels.py:95-109."""
+    ref = golden()["on_ring"][f"n{n_comp}_N8_b1.1"]
+    beta, n_sites = 1.1, 8
+    sim = Simulation(ON(chain(n_sites), n_comp), beta, updates, seed=5)
+    sim.thermalize(2000)
+    ts = sim.run(100_000)
+    assert_consistent(ts["e"], ref["energy"])
+    e = ts["E"]
+    assert beta ** 2 * e.var() / n_sites == pytest.approx(ref["specific_heat"], rel=0.06)
+
+
+def test_on_state_stays_normalised_and_energy_consistent(cuda):
+    """critmc tests/test_kernels.py:112-118 (without the cluster moves)."""
+    lat = square(6)
+    sim = Simulation(ON(lat, 3), 0.7, "metropolis+2*overrelax+heatbath", seed=1)
+    sim.thermalize(200)
+    ts = sim.run(200)
+    s = sim.state
+    assert np.allclose(np.linalg.norm(s, axis=1), 1.0, atol=1e-6)
+    assert ts["E"][-1] == pytest.approx(ON(lat, 3).energy(s), rel=1e-6)
+
+
+def test_metropolis_step_is_tuned(cuda):
+    sim = Simulation(ON(square(8), 2), 1.0, "metropolis", seed=2)
+    info = sim.thermalize(500)
+    assert 0.001 <= info["step"] <= 10
+    acc = sim.run(500).meta["acceptance"]
+    assert 0.3 < acc < 0.7

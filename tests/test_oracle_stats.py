@@ -71,3 +71,18 @@ def test_oracle_msc_matches_kaufman(code):
     s = _ising_state(256, 4)
     e_b, _, _, _ = oracle.ising_msc_run(s, (64, 4), (9, 10), beta, 0.0, [[code, 1]], 40_000)
     assert_consistent(e_b[1000:] / 256.0, kaufman_energy(beta, 64, 4))
+
+
+@pytest.mark.parametrize("n", [2, 3])
+@pytest.mark.parametrize("sched", [[[2, 1]], [[0, 1], [5, 3]]], ids=["heatbath", "metropolis+3*overrelax"])
+def test_oracle_on_ring_matches_transfer_operator(n, sched):
+    """critmc tests/test_kernels.py:95-109: 8-site O(n) ring against chains.on_ring_*."""
+    ref = golden()["on_ring"][f"n{n}_N8_b1.1"]
+    rng = np.random.default_rng(n)
+    s = rng.standard_normal((8, n))
+    s = (s / np.linalg.norm(s, axis=1, keepdims=True)).astype(np.float32)
+    e, _, _, _, _ = oracle.on_run(s, (8,), n, (n, 5), 1.1, 1.0, sched, 100_000)
+    e = e[2000:]
+    assert_consistent(e / 8.0, ref["energy"])
+    c_mc = 1.1 ** 2 * e.var() / 8
+    assert c_mc == pytest.approx(ref["specific_heat"], rel=0.06)

@@ -44,6 +44,13 @@ SIGNATURES: dict[str, tuple] = {
          _P, _P],
     ),
     "critmc_potts_tables": (_I32, [_I32, _D, _P, _P]),
+    "critmc_pt_swap_table": (_I32, [_I32, _P, _I32, _P]),
+    "critmc_ea_coupling_bits": (_I32, [_I32, _I32, _I32, _I32, _P, _P]),
+    "critmc_ea_pt_run": (
+        _I32,
+        [_P, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P, _P, _I32, _P, _P, _U32, _I32, _I32, _I32,
+         _P, _P, _P, _P, _P, _P],
+    ),
     "critmc_on_run": (
         _I32,
         [_P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P,

@@ -1,0 +1,531 @@
+// Edwards-Anderson +-J spin glasses with parallel tempering, one thread block
+// per disorder sample, both replica sets resident in shared memory.
+//
+// Replica multi-spin coding: the word of a site holds one bit per temperature
+// (bit k = configuration at temperature index k, hot -> cold).  A sweep updates
+// all temperatures of a replica set at once with the bit-sliced MSB-first
+// acceptance of the Ising kernels; each lane compares with the threshold of
+// its own temperature (per-lane threshold planes, kernel parameters).  An
+// accepted replica exchange moves configurations between lanes, so after the
+// swap pass the words are permuted (one warp ballot per word); critmc's perm
+// array survives as conf_at for the round-trip bookkeeping.
+//
+// Replaces critmc src/critmc/kernels/glass.py:81-163 (`pt_run`), :42-53
+// (`metropolis_sweep`), :34-38 (`energy`), :57-77 (`_measure`).
+#include <cmath>
+#include <cstring>
+
+#include "geom.cuh"
+#include "host_common.h"
+#include "msc_ising.cuh"
+
+namespace critmc {
+
+constexpr int EA_THREADS = 256;
+constexpr int EA_WARPS = EA_THREADS / 32;
+constexpr int EA_MAX_SITES = 4096;
+constexpr int EA_MAX_L = 64;
+constexpr int EA_NOBS = 7;  // e, q_l, |q|, q^2, q^4, |q(kmin)|^2, count (critmc glass.py:24-31)
+constexpr int EA_PSAMPLES = 512;
+constexpr int EA_FIXCAP = 64;
+
+struct EaParams {
+  uint32_t* words;
+  const uint8_t* jneg;
+  const uint32_t* swap_thr;
+  uint8_t* conf_at;
+  uint8_t* labels;
+  double* acc;
+  long long* swap_acc;
+  long long* swap_try;
+  long long* label_hist;
+  long long* trips;
+  ByteGeom g;
+  int m, n_samples, sample0, n_steps, n_bins, sweeps_per_step, swap_width;
+  uint32_t t0;
+  uint32_t planes[3][32];  // lane masks of the threshold bits, classes v = 0..z/2-1
+  double cosx[EA_MAX_L], sinx[EA_MAX_L];  // cos/sin(2 pi x / L) per axis extent (same L per axis)
+  int ext[3];
+  uint32_t keys[EA_PSAMPLES][2][2];
+};
+
+// threshold bit plane for the undecided lanes (counts 0 .. z/2-1)
+template <int Z>
+__device__ __forceinline__ uint32_t ea_tbits(const EaParams& P, const Count3& c, int q) {
+  const uint32_t lo = mux(c.b0, P.planes[1][q], P.planes[0][q]);
+  if constexpr (Z == 6) return mux(c.b1, P.planes[2][q], lo);
+  return lo;
+}
+
+struct EaFix {
+  uint32_t idx, U, D;  // idx = set * words + colour * slots + slot
+};
+
+template <int Z>
+__device__ __forceinline__ void ea_site(const EaParams& P, const uint32_t* lat, const uint8_t* jn,
+                                        int set, int c, uint32_t s, uint32_t& w_s, Count3& cnt) {
+  const ByteGeom& g = P.g;
+  int r, i;
+  byte_row_index(g, s, r, i);
+  uint32_t nb[Z];
+  byte_neighbours<Z>(g, c, r, i, nb);
+  const uint32_t* base = lat + (size_t)set * 2 * g.slots;
+  const uint32_t* own = base + (size_t)c * g.slots;
+  const uint32_t* oth = base + (size_t)(c ^ 1) * g.slots;
+  const uint32_t jb = jn[(size_t)c * g.slots + s];
+  w_s = own[s];
+  uint32_t x[Z];
+#pragma unroll
+  for (int q = 0; q < Z; ++q) x[q] = w_s ^ oth[nb[q]] ^ (0u - ((jb >> q) & 1u));
+  cnt = count_bits<Z>(x);  // unsatisfied bonds per lane
+}
+
+template <int Z>
+__device__ __forceinline__ void ea_planes(const EaParams& P, const Count3& cnt, uint32_t k0,
+                                          uint32_t k1, uint32_t slot, uint32_t sweep, uint32_t col,
+                                          int g_begin, int g_end, uint32_t& D, uint32_t& U) {
+  for (int grp = g_begin; grp < g_end && U; ++grp) {
+    const critmc_u32x4 r = critmc_philox4x32(
+        slot, sweep, CRITMC_TAG_PLANES | ((uint32_t)grp << 8) | (col << 16), 0u, k0, k1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t t = ea_tbits<Z>(P, cnt, 4 * grp + q);
+      D |= U & t & ~r.v[q];
+      U &= ~(r.v[q] ^ t);
+    }
+  }
+}
+
+template <int Z>
+__global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant__ EaParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int DIM = Z / 2;
+  const ByteGeom& g = P.g;
+  const uint32_t n_sites = 2 * g.slots;
+  uint32_t* lat = reinterpret_cast<uint32_t*>(smem_raw);  // [2 sets][2 colours][slots]
+  uint32_t* qw = lat + 2 * n_sites;                      // overlap words [2][slots]
+  int* splane = reinterpret_cast<int*>(qw + n_sites);    // [DIM][L][32] overlap per plane and lane
+  uint8_t* jn = reinterpret_cast<uint8_t*>(splane + DIM * P.ext[0] * 32);  // [2][slots]
+  __shared__ EaFix fix[EA_WARPS][EA_FIXCAP];
+  __shared__ int ecnt[2][32];  // unsatisfied bonds per set and temperature
+  __shared__ int qlcnt[32];    // agreeing bonds of the overlap field
+  __shared__ int sigma[2][32];
+  __shared__ int conf[2][32], lab[2][32];
+  __shared__ double acc_s[32][EA_NOBS];
+  __shared__ unsigned long long sw_acc[32], sw_try[32], lhist[32][2], trip[2];
+
+  const int lsample = blockIdx.x;
+  const int sample = P.sample0 + lsample;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m = P.m;
+  uint32_t* gw = P.words + (size_t)sample * 2 * n_sites;
+  for (uint32_t j = tid; j < 2 * n_sites; j += EA_THREADS) lat[j] = gw[j];
+  for (uint32_t j = tid; j < n_sites; j += EA_THREADS) jn[j] = P.jneg[(size_t)sample * n_sites + j];
+  if (tid < 64) {
+    const int r = tid >> 5, k = tid & 31;
+    if (k < m) {
+      conf[r][k] = P.conf_at[((size_t)sample * 2 + r) * m + k];
+      lab[r][k] = P.labels[((size_t)sample * 2 + r) * m + k];
+    }
+  }
+  if (tid < 32) {
+    sw_acc[tid] = sw_try[tid] = 0;
+    lhist[tid][0] = lhist[tid][1] = 0;
+    for (int o = 0; o < EA_NOBS; ++o) acc_s[tid][o] = 0.0;
+  }
+  if (tid < 2) trip[tid] = 0;
+  __syncthreads();
+
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  int bin = 0;
+  long long next_edge = 1;
+  for (int t = 0; t < P.n_steps; ++t) {
+    if (t >= next_edge) {
+      // flush the finished bin (critmc glass.py:114-122)
+      if (tid < m)
+        for (int o = 0; o < EA_NOBS; ++o) {
+          P.acc[(((size_t)sample * P.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
+          acc_s[tid][o] = 0.0;
+        }
+      ++bin;
+      next_edge = (1LL << (bin + 1)) - 1;
+    }
+    const uint32_t step = P.t0 + (uint32_t)t;
+    // ---- sweeps of every temperature of both sets --------------------------
+    for (int sw = 0; sw < P.sweeps_per_step; ++sw) {
+      const uint32_t sweep = step * (uint32_t)P.sweeps_per_step + (uint32_t)sw;
+      for (int c = 0; c < 2; ++c) {
+        int nf = 0;
+        const uint32_t work = 2 * g.slots;  // both sets, one colour
+        const uint32_t rounds = (work + EA_THREADS - 1) / EA_THREADS;
+        for (uint32_t it = 0; it < rounds; ++it) {
+          const uint32_t j = it * EA_THREADS + tid;
+          uint32_t U = 0, D = 0, idx = 0;
+          if (j < work) {
+            const int set = j >= g.slots;
+            const uint32_t s = j - set * g.slots;
+            uint32_t w_s;
+            Count3 cnt;
+            ea_site<Z>(P, lat, jn, set, c, s, w_s, cnt);
+            // flips with dE <= 0 (>= z/2 unsatisfied bonds) are always accepted
+            const uint32_t alw = (Z == 6) ? (cnt.b2 | (cnt.b1 & cnt.b0)) : (cnt.b1 | cnt.b2);
+            D = alw;
+            U = ~alw;
+            const uint32_t k0 = P.keys[lsample][set][0], k1 = P.keys[lsample][set][1];
+            ea_planes<Z>(P, cnt, k0, k1, s, sweep, (uint32_t)c, 0, 2, D, U);
+            idx = (uint32_t)set * n_sites + (uint32_t)c * g.slots + s;
+            if (U == 0) lat[idx] = w_s ^ D;
+          }
+          const uint32_t need = __ballot_sync(0xffffffffu, U != 0);
+          if (need) {
+            const int cntn = __popc(need);
+            if (nf + cntn > EA_FIXCAP) {
+              __syncwarp();
+              for (int e = lane; e < nf; e += 32) {
+                const EaFix f = fix[warp][e];
+                const int set = f.idx >= n_sites;
+                const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
+                uint32_t w_s;
+                Count3 cnt;
+                ea_site<Z>(P, lat, jn, set, c, s, w_s, cnt);
+                uint32_t D2 = f.D, U2 = f.U;
+                ea_planes<Z>(P, cnt, P.keys[lsample][set][0], P.keys[lsample][set][1], s, sweep,
+                             (uint32_t)c, 2, 8, D2, U2);
+                lat[f.idx] = w_s ^ D2;
+              }
+              __syncwarp();
+              nf = 0;
+            }
+            if (U != 0) fix[warp][nf + __popc(need & lt_mask)] = EaFix{idx, U, D};
+            nf += cntn;
+          }
+        }
+        __syncwarp();
+        for (int e = lane; e < nf; e += 32) {
+          const EaFix f = fix[warp][e];
+          const int set = f.idx >= n_sites;
+          const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
+          uint32_t w_s;
+          Count3 cnt;
+          ea_site<Z>(P, lat, jn, set, c, s, w_s, cnt);
+          uint32_t D2 = f.D, U2 = f.U;
+          ea_planes<Z>(P, cnt, P.keys[lsample][set][0], P.keys[lsample][set][1], s, sweep,
+                       (uint32_t)c, 2, 8, D2, U2);
+          lat[f.idx] = w_s ^ D2;
+        }
+        __syncthreads();
+      }
+    }
+    // ---- energies per set and temperature (unsatisfied bonds) ---------------
+    if (tid < 64) ecnt[tid >> 5][tid & 31] = 0;
+    __syncthreads();
+    {
+      int ca = 0, cb = 0;
+      for (uint32_t s = warp; s < g.slots; s += EA_WARPS) {  // colour-0 sites see every bond once
+        uint32_t w_s;
+        Count3 cnt;
+        ea_site<Z>(P, lat, jn, 0, 0, s, w_s, cnt);
+        ca += ((cnt.b0 >> lane) & 1) + 2 * ((cnt.b1 >> lane) & 1) + 4 * ((cnt.b2 >> lane) & 1);
+        ea_site<Z>(P, lat, jn, 1, 0, s, w_s, cnt);
+        cb += ((cnt.b0 >> lane) & 1) + 2 * ((cnt.b1 >> lane) & 1) + 4 * ((cnt.b2 >> lane) & 1);
+      }
+      atomicAdd(&ecnt[0][lane], ca);
+      atomicAdd(&ecnt[1][lane], cb);
+    }
+    __syncthreads();
+    // ---- replica exchange, one thread per set (critmc glass.py:128-152) -----
+    if (tid == 0 || tid == 32) {
+      const int r = tid >> 5;
+      const long long n_bonds = (long long)n_sites * DIM;
+      long long e[32];
+      for (int k = 0; k < m; ++k) {
+        e[k] = -(n_bonds - 2LL * ecnt[r][k]);
+        sigma[r][k] = k;
+      }
+      const uint32_t k0 = P.keys[lsample][r][0], k1 = P.keys[lsample][r][1];
+      for (int k = 0; k < m - 1; ++k) {
+        // betas ascend hot -> cold, so x = (b_k - b_k+1)(E_k - E_k+1) >= 0 iff E_k <= E_k+1
+        const long long de = e[k] - e[k + 1];
+        bool ok = de <= 0;
+        if (!ok) {
+          long long j = de / 4;
+          if (j > P.swap_width - 1) j = P.swap_width - 1;
+          const uint32_t u = critmc_philox4x32((uint32_t)k, step, CRITMC_TAG_SWAP | ((uint32_t)r << 16), 0u, k0, k1).v[0];
+          ok = u < P.swap_thr[(size_t)k * P.swap_width + j];
+        }
+        atomicAdd(&sw_try[k], 1ULL);
+        if (ok) {
+          atomicAdd(&sw_acc[k], 1ULL);
+          const long long te = e[k];
+          e[k] = e[k + 1];
+          e[k + 1] = te;
+          const int tc = conf[r][k];
+          conf[r][k] = conf[r][k + 1];
+          conf[r][k + 1] = tc;
+          const int ts = sigma[r][k];
+          sigma[r][k] = sigma[r][k + 1];
+          sigma[r][k + 1] = ts;
+        }
+      }
+      for (int k = 0; k < m; ++k) ecnt[r][k] = (int)((e[k] + n_bonds) / 2);  // permuted counts
+      const int hot = conf[r][0], cold = conf[r][m - 1];
+      // labels are indexed by configuration: lab[r][c] for configuration c
+      if (lab[r][hot] == 2) atomicAdd(&trip[r], 1ULL);
+      lab[r][hot] = 1;
+      if (lab[r][cold] == 1) atomicAdd(&trip[r], 1ULL);
+      lab[r][cold] = 2;
+      for (int k = 0; k < m; ++k) {
+        const int l = lab[r][conf[r][k]];
+        if (l == 1) atomicAdd(&lhist[k][0], 1ULL);
+        else if (l == 2) atomicAdd(&lhist[k][1], 1ULL);
+      }
+    }
+    __syncthreads();
+    // ---- move configurations between lanes: new bit k = old bit sigma[k] ----
+    for (uint32_t j = warp; j < 2 * n_sites; j += EA_WARPS) {
+      const int r = j >= n_sites;
+      const uint32_t w = lat[j];
+      const int src = sigma[r][lane];
+      const uint32_t nw = __ballot_sync(0xffffffffu, lane < m && ((w >> src) & 1u));
+      if (lane == 0) lat[j] = nw;
+    }
+    __syncthreads();
+    // ---- measurement (critmc glass.py:57-77, :153-163) -----------------------
+    for (uint32_t j = tid; j < n_sites; j += EA_THREADS) qw[j] = ~(lat[j] ^ lat[n_sites + j]);
+    if (tid < 32) qlcnt[tid] = 0;
+    __syncthreads();
+    {
+      int agree = 0;
+      for (uint32_t s = warp; s < g.slots; s += EA_WARPS) {
+        int r, i;
+        byte_row_index(g, s, r, i);
+        uint32_t nb[Z];
+        byte_neighbours<Z>(g, 0, r, i, nb);
+        const uint32_t qs = qw[s];
+#pragma unroll
+        for (int q = 0; q < Z; ++q) agree += (~(qs ^ qw[g.slots + nb[q]]) >> lane) & 1;
+      }
+      atomicAdd(&qlcnt[lane], agree);
+    }
+    // per-plane overlap counts: warp w handles planes (d, x) = w, w + WARPS, ...
+    for (int pl = warp; pl < DIM * EA_MAX_L; pl += EA_WARPS) {
+      const int d = pl / EA_MAX_L, x0 = pl % EA_MAX_L;
+      if (x0 >= P.ext[d]) continue;
+      int cnt = 0;
+      const int e1 = P.ext[d == 0 ? 1 : 0], e2 = DIM == 3 ? P.ext[d == 2 ? 1 : 2] : 1;
+      for (int u = 0; u < e1; ++u)
+        for (int v = 0; v < e2; ++v) {
+          int xyz[3] = {0, 0, 0};
+          xyz[d] = x0;
+          xyz[d == 0 ? 1 : 0] = u;
+          if (DIM == 3) xyz[d == 2 ? 1 : 2] = v;
+          const int col = (xyz[0] + xyz[1] + xyz[2]) & 1;
+          const uint32_t slot = (uint32_t)((xyz[1] + g.ly * xyz[2]) * g.hx + xyz[0] / 2);
+          cnt += (qw[(size_t)col * g.slots + slot] >> lane) & 1;
+        }
+      splane[(d * P.ext[0] + x0) * 32 + lane] = cnt;
+    }
+    __syncthreads();
+    if (tid < m) {
+      const int k = tid;
+      const double n = (double)n_sites;
+      const double nb = n * DIM;
+      int qs = 0;
+      for (int x = 0; x < P.ext[0]; ++x) qs += splane[x * 32 + k];
+      const double q = (2.0 * qs - n) / n;
+      const double ql = (2.0 * qlcnt[k] - nb) / nb;
+      double qk2 = 0.0;
+      for (int d = 0; d < DIM; ++d) {
+        const double per = n / P.ext[d];
+        double re = 0.0, im = 0.0;
+        for (int x = 0; x < P.ext[d]; ++x) {
+          const double sx = 2.0 * splane[(d * P.ext[0] + x) * 32 + k] - per;
+          re += P.cosx[x] * sx;
+          im += P.sinx[x] * sx;
+        }
+        qk2 += (re * re + im * im) / (n * n);
+      }
+      qk2 /= DIM;
+      const double ea = -(nb - 2.0 * ecnt[0][k]), eb = -(nb - 2.0 * ecnt[1][k]);
+      acc_s[k][0] += 0.5 * (ea + eb) / n;
+      acc_s[k][1] += ql;
+      acc_s[k][2] += fabs(q);
+      acc_s[k][3] += q * q;
+      acc_s[k][4] += q * q * q * q;
+      acc_s[k][5] += qk2;
+      acc_s[k][6] += 1.0;
+    }
+    __syncthreads();
+  }
+  // ---- write back ------------------------------------------------------------
+  if (tid < m)
+    for (int o = 0; o < EA_NOBS; ++o)
+      P.acc[(((size_t)sample * P.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
+  for (uint32_t j = tid; j < 2 * n_sites; j += EA_THREADS) gw[j] = lat[j];
+  if (tid < 64) {
+    const int r = tid >> 5, k = tid & 31;
+    if (k < m) {
+      P.conf_at[((size_t)sample * 2 + r) * m + k] = (uint8_t)conf[r][k];
+      P.labels[((size_t)sample * 2 + r) * m + k] = (uint8_t)lab[r][k];
+    }
+  }
+  if (tid < m - 1) {
+    P.swap_acc[(size_t)sample * (m - 1) + tid] += (long long)sw_acc[tid];
+    P.swap_try[(size_t)sample * (m - 1) + tid] += (long long)sw_try[tid];
+  }
+  if (tid < m) {
+    P.label_hist[((size_t)sample * m + tid) * 2 + 0] += (long long)lhist[tid][0];
+    P.label_hist[((size_t)sample * m + tid) * 2 + 1] += (long long)lhist[tid][1];
+  }
+  if (tid < 2) P.trips[(size_t)sample * 2 + tid] += (long long)trip[tid];
+}
+
+static thread_local EaParams g_ea;
+
+}  // namespace critmc
+
+using namespace critmc;
+
+extern "C" int32_t critmc_pt_swap_table(int32_t m, const double* betas, int32_t width, uint32_t* out) {
+  clear_error();
+  if (!betas || !out || m < 2 || m > 32 || width < 2) return fail(CRITMC_ERR_INVALID, "need 2 <= m <= 32, width >= 2");
+  for (int k = 0; k + 1 < m; ++k) {
+    const double db = betas[k] - betas[k + 1];
+    if (!(db < 0.0)) return fail(CRITMC_ERR_INVALID, "betas must increase strictly (temperatures hot -> cold)");
+    for (int j = 0; j < width; ++j) {
+      // energies of +-J configurations differ by multiples of 4: dE = 4 j
+      const double p = j == 0 ? 1.0 : std::exp(db * 4.0 * j);
+      const double t = std::nearbyint(std::ldexp(p, 32));
+      out[(size_t)k * width + j] = t >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)t;
+    }
+    if (out[(size_t)k * width + width - 1] != 0)
+      return fail(CRITMC_ERR_INVALID, "swap table too narrow for these temperatures");
+  }
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_ea_coupling_bits(int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                                           const double* couplings, uint8_t* jneg) {
+  clear_error();
+  ByteGeom g;
+  int st = byte_geom(dim, lx, ly, lz, g);
+  if (st) return st;
+  if (dim < 2) return fail(CRITMC_ERR_UNSUPPORTED, "EA samples need dim 2 or 3");
+  if (!couplings || !jneg) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  const int n = lx * g.ly * g.lz;
+  auto site = [&](int x, int y, int z) { return x + lx * (y + g.ly * z); };
+  // critmc lattice.py:147-149: bond index a*N + i is (i, i + e_a)
+  auto jval = [&](int a, int i) { return couplings[(size_t)a * n + i]; };
+  for (int c = 0; c < 2; ++c)
+    for (uint32_t s = 0; s < g.slots; ++s) {
+      const int r = (int)(s / g.hx), i = (int)(s % g.hx);
+      const int y = r % g.ly, z = r / g.ly, p = (c + y + z) & 1, x = 2 * i + p;
+      const int xp = (x + 1) % lx, xm = (x + lx - 1) % lx;
+      const int yp = (y + 1) % g.ly, ym = (y + g.ly - 1) % g.ly;
+      const int zp = (z + 1) % g.lz, zm = (z + g.lz - 1) % g.lz;
+      const int me = site(x, y, z);
+      // neighbour order of the colour-major layout: (x-side, other x-side, y-1, y+1, z-1, z+1)
+      double jj[6];
+      jj[0] = p ? jval(0, site(xm, y, z)) : jval(0, me);  // slot i: -x if p else +x
+      jj[1] = p ? jval(0, me) : jval(0, site(xm, y, z));
+      jj[2] = jval(1, site(x, ym, z));
+      jj[3] = jval(1, me);
+      jj[4] = dim == 3 ? jval(2, site(x, y, zm)) : 1.0;
+      jj[5] = dim == 3 ? jval(2, me) : 1.0;
+      (void)xp;
+      (void)yp;
+      (void)zp;
+      uint8_t b = 0;
+      for (int q = 0; q < 2 * dim; ++q) {
+        if (jj[q] != 1.0 && jj[q] != -1.0) return fail(CRITMC_ERR_UNSUPPORTED, "couplings must be +-1");
+        if (jj[q] < 0) b |= (uint8_t)(1u << q);
+      }
+      jneg[(size_t)c * g.slots + s] = b;
+    }
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_t dim, int32_t lx,
+                                    int32_t ly, int32_t lz, int32_t m, int32_t n_samples,
+                                    const uint32_t* keys, const double* betas,
+                                    const uint32_t* swap_thr, int32_t swap_width, uint8_t* conf_at,
+                                    uint8_t* labels, uint32_t t0, int32_t n_steps, int32_t n_bins,
+                                    int32_t sweeps_per_step, double* acc, int64_t* swap_acc,
+                                    int64_t* swap_try, int64_t* label_hist, int64_t* trips,
+                                    void* stream) {
+  clear_error();
+  EaParams& P = g_ea;
+  int st = byte_geom(dim, lx, ly, lz, P.g);
+  if (st) return st;
+  if (dim < 2) return fail(CRITMC_ERR_UNSUPPORTED, "EA samples need dim 2 or 3");
+  if (2 * P.g.slots > (uint32_t)EA_MAX_SITES) return fail(CRITMC_ERR_UNSUPPORTED, "at most 4096 sites per sample");
+  if (lx > EA_MAX_L || P.g.ly > EA_MAX_L || P.g.lz > EA_MAX_L) return fail(CRITMC_ERR_UNSUPPORTED, "extent too large");
+  if (lx != P.g.ly || (dim == 3 && lx != P.g.lz))
+    return fail(CRITMC_ERR_UNSUPPORTED, "EA samples use equal extents (one k_min table)");
+  if (!words || !jneg || !keys || !betas || !swap_thr || !conf_at || !labels || !acc || !swap_acc ||
+      !swap_try || !label_hist || !trips)
+    return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (m < 2 || m > 32) return fail(CRITMC_ERR_INVALID, "need 2 <= m <= 32 temperatures");
+  if (n_samples < 1) return fail(CRITMC_ERR_INVALID, "need n_samples >= 1");
+  if (n_steps < 0 || n_bins < 1 || n_bins > 31 || (long long)n_steps > (1LL << n_bins) - 1)
+    return fail(CRITMC_ERR_INVALID, "need 0 <= n_steps <= 2^n_bins - 1 and 1 <= n_bins <= 31");
+  if (sweeps_per_step < 1) return fail(CRITMC_ERR_INVALID, "sweeps_per_step must be >= 1");
+  if (swap_width < 2) return fail(CRITMC_ERR_INVALID, "swap_width must be >= 2");
+  if (((long long)t0 + n_steps) * sweeps_per_step > 0xFFFFFFFFLL)
+    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+  for (int k = 0; k + 1 < m; ++k)
+    if (!(betas[k] < betas[k + 1])) return fail(CRITMC_ERR_INVALID, "betas must increase (hot -> cold)");
+  if (n_steps == 0) return CRITMC_OK;
+  const int z = 2 * dim;
+  // per-lane Metropolis thresholds exp(-beta_k (2z - 4v)), v = 0..z/2-1 unsatisfied bonds
+  std::memset(P.planes, 0, sizeof(P.planes));
+  for (int v = 0; v < z / 2; ++v)
+    for (int k = 0; k < m; ++k) {
+      if (!std::isfinite(betas[k]) || betas[k] <= 0.0) return fail(CRITMC_ERR_INVALID, "betas must be positive");
+      const double p = std::exp(-betas[k] * (2.0 * z - 4.0 * v));
+      const double tt = std::nearbyint(std::ldexp(p, 32));
+      const uint32_t thr = tt >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)tt;
+      for (int q = 0; q < 32; ++q)
+        if ((thr >> (31 - q)) & 1u) P.planes[v][q] |= 1u << k;
+    }
+  for (int x = 0; x < lx; ++x) {
+    P.cosx[x] = std::cos(2.0 * M_PI * x / lx);
+    P.sinx[x] = std::sin(2.0 * M_PI * x / lx);
+  }
+  P.ext[0] = lx;
+  P.ext[1] = P.g.ly;
+  P.ext[2] = P.g.lz;
+  P.words = words;
+  P.jneg = jneg;
+  P.swap_thr = swap_thr;
+  P.conf_at = conf_at;
+  P.labels = labels;
+  P.acc = acc;
+  P.swap_acc = (long long*)swap_acc;
+  P.swap_try = (long long*)swap_try;
+  P.label_hist = (long long*)label_hist;
+  P.trips = (long long*)trips;
+  P.m = m;
+  P.n_samples = n_samples;
+  P.n_steps = n_steps;
+  P.n_bins = n_bins;
+  P.sweeps_per_step = sweeps_per_step;
+  P.swap_width = swap_width;
+  P.t0 = t0;
+  const uint32_t n_sites = 2 * P.g.slots;
+  const size_t smem = (size_t)n_sites * (2 * 4 + 4 + 1) + (size_t)dim * lx * 32 * 4;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int c0 = 0; c0 < n_samples; c0 += EA_PSAMPLES) {
+    const int nc = std::min(EA_PSAMPLES, n_samples - c0);
+    P.sample0 = c0;
+    std::memcpy(P.keys, keys + (size_t)c0 * 4, sizeof(uint32_t) * 4 * nc);
+    auto launch = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<nc, EA_THREADS, smem, s>>>(P);
+    };
+    if (dim == 2) launch(ea_pt_kernel<4>);
+    else launch(ea_pt_kernel<6>);
+    if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  }
+  return CRITMC_OK;
+}

@@ -169,6 +169,43 @@ int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t
                       double* m_out, double* stiff_c_out, double* stiff_s_out, int64_t* aux_out,
                       void* stream);
 
+/* ---- Edwards-Anderson +-J spin glass with parallel tempering ---------------
+ * A sample holds two independent replica sets of m <= 32 configurations on a
+ * periodic lattice (dim 2 or 3, even extents, at most 4096 sites).  Device
+ * layout (replica multi-spin coding): words[sample][set][colour][slot]
+ * (uint32, colour-major slots as for the byte lattices), bit k = spin (1 = +1)
+ * of the configuration currently at temperature index k; temperatures are
+ * ordered hot -> cold (critmc glass.py:140).  conf_at[sample][set][m] (uint8)
+ * names the configuration at each temperature (critmc's perm), labels
+ * [sample][set][m] (uint8) the last visited end (0, 1 hot, 2 cold).
+ * jneg[sample][colour][slot] (uint8): bit q set if the coupling of the bond to
+ * neighbour q is -1, neighbours in the order (x-side, other x-side, y-1, y+1,
+ * z-1, z+1) of the colour-major layout (critmc_ea_coupling_bits builds it).
+ *
+ * One call runs n_steps PT steps (critmc kernels/glass.py:81-163 `pt_run`):
+ * sweeps_per_step checkerboard Metropolis sweeps of every configuration at
+ * its temperature, then for each set swaps of neighbouring temperatures
+ * k = 0..m-2 in order (accept x >= 0 or u < exp(x), x = (b_k - b_k+1)
+ * (E_k - E_k+1)), round-trip labels, and the measurement of e, q_l, |q|, q^2,
+ * q^4, |q(k_min)|^2 per temperature into acc[sample][bin][m][7] (double;
+ * step t0+t goes to bin floor(log2(t+1)) of this call).  Counters (device,
+ * accumulated): swap_acc/swap_try[sample][m-1], label_hist[sample][m][2],
+ * trips[sample][2] (int64).  betas: HOST [m].  keys: HOST [n_samples][2][2]
+ * (one Philox key per replica set).  swap_thr: DEVICE table from
+ * critmc_pt_swap_table.  Site draws use the MSC plane stream of
+ * critmc_ising_msc_run with counter word c0 = slot and sweep index
+ * (t0 + t) * sweeps_per_step + s; swap k of set r at step t draws word 0 of
+ * Philox(k, t0 + t, 0x04 | r << 16, 0).                                      */
+int32_t critmc_pt_swap_table(int32_t m, const double* betas, int32_t width, uint32_t* out);
+int32_t critmc_ea_coupling_bits(int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                                const double* couplings, uint8_t* jneg);
+int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_t dim, int32_t lx, int32_t ly,
+                         int32_t lz, int32_t m, int32_t n_samples, const uint32_t* keys,
+                         const double* betas, const uint32_t* swap_thr, int32_t swap_width,
+                         uint8_t* conf_at, uint8_t* labels, uint32_t t0, int32_t n_steps,
+                         int32_t n_bins, int32_t sweeps_per_step, double* acc, int64_t* swap_acc,
+                         int64_t* swap_try, int64_t* label_hist, int64_t* trips, void* stream);
+
 /* Energy E_b = -sum_<ij> s_i s_j and magnetisation M of MSC chains, written
  * to out[n_chains][2] (device).  critmc kernels/ising.py:32-45.           */
 int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,

@@ -65,6 +65,9 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_potts_run.restype = _I
     L.oracle_on_run.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _D, _U32, _P, _I, _I, _P, _P, _P, _P, _P]
     L.oracle_on_run.restype = _I
+    L.oracle_ea_pt_run.argtypes = [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _P, _P, _U32, _I, _I, _I,
+                                   _P, _P, _P, _P, _P]
+    L.oracle_ea_pt_run.restype = _I
 
 
 def _ptr(a: np.ndarray) -> int:
@@ -207,3 +210,31 @@ def on_run(s, shape, n, key, beta, step, schedule, n_meas, sweep0=0):
     if rc != 0:
         raise ValueError(f"oracle_on_run failed ({rc})")
     return e, m, sc, ss, aux
+
+
+def ea_pt_run(spins, couplings, shape, keys, betas, swap_thr, perm, labels, n_steps, n_bins,
+              t0=0, sweeps_per_step=1):
+    """Replay parallel tempering of one +-J sample (critmc pt_run layout, arrays updated in place).
+
+    spins: int8 (2, m, N); couplings: float64 (dim N,); keys: uint32 (2, 2);
+    perm, labels: int32 (2, m).  Returns (acc, swap_acc, swap_try, label_hist, trips).
+    """
+    m = spins.shape[1]
+    for a, dt in ((spins, np.int8), (perm, np.int32), (labels, np.int32)):
+        if not (isinstance(a, np.ndarray) and a.dtype == dt and a.flags["C_CONTIGUOUS"]):
+            raise TypeError("spins/perm/labels must be C-contiguous int8/int32 arrays")
+    J = np.ascontiguousarray(couplings, dtype=np.float64)
+    k = np.ascontiguousarray(keys, dtype=np.uint32)
+    b = np.ascontiguousarray(betas, dtype=np.float64)
+    st = np.ascontiguousarray(swap_thr, dtype=np.uint32)
+    acc = np.zeros((n_bins, m, 7))
+    sa = np.zeros(m - 1, dtype=np.int64)
+    stry = np.zeros(m - 1, dtype=np.int64)
+    lh = np.zeros((m, 2), dtype=np.int64)
+    tr = np.zeros(2, dtype=np.int64)
+    rc = lib().oracle_ea_pt_run(_ptr(spins), _ptr(J), len(shape), *_dims(shape), m, _ptr(k), _ptr(b),
+                                _ptr(st), st.shape[1], _ptr(perm), _ptr(labels), t0, n_steps, n_bins,
+                                sweeps_per_step, _ptr(acc), _ptr(sa), _ptr(stry), _ptr(lh), _ptr(tr))
+    if rc != 0:
+        raise ValueError(f"oracle_ea_pt_run failed ({rc})")
+    return acc, sa, stry, lh, tr

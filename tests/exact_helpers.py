@@ -101,3 +101,24 @@ def pulls(series: list[np.ndarray], exact: float) -> np.ndarray:
         m, err, _ = gamma_error(x)
         out.append((m - exact) / err)
     return np.asarray(out)
+
+
+def ea_exact(lattice, couplings, temperatures):
+    """Exact e, q^2 and q_l per temperature of a +-J sample (all 2^N states).
+
+    Follows critmc tests/test_glass.py:26-52 (energies as critmc's
+    exact/enumeration.py:120-135 ea_energies: E = -sum_b J_b s_i s_j)."""
+    n = lattice.n_sites
+    states = np.arange(1 << n)
+    spins = (2 * ((states[:, None] >> np.arange(n)) & 1) - 1).astype(np.float64)
+    b = lattice.bonds
+    energies = -(spins[:, b[:, 0]] * spins[:, b[:, 1]]) @ np.asarray(couplings, dtype=np.float64)
+    out = {"e": [], "q2": [], "ql": []}
+    for T in temperatures:
+        w = np.exp(-(energies - energies.min()) / T)
+        w /= w.sum()
+        corr = (spins * w[:, None]).T @ spins
+        out["e"].append(w @ energies / n)
+        out["q2"].append(np.sum(corr ** 2) / n ** 2)
+        out["ql"].append(np.mean(corr[b[:, 0], b[:, 1]] ** 2))
+    return {k: np.array(v) for k, v in out.items()}

@@ -86,3 +86,48 @@ def test_oracle_on_ring_matches_transfer_operator(n, sched):
     assert_consistent(e / 8.0, ref["energy"])
     c_mc = 1.1 ** 2 * e.var() / 8
     assert c_mc == pytest.approx(ref["specific_heat"], rel=0.06)
+
+
+def test_ea_enumeration_helper_matches_critmc():
+    """The test-side EA enumeration reproduces critmc's ea_energies fixture."""
+    from critmc_b200 import square
+
+    g = golden()["ea_square4"]
+    lat = square(4)
+    n = lat.n_sites
+    states = np.arange(64)
+    spins = (2 * ((states[:, None] >> np.arange(n)) & 1) - 1).astype(np.float64)
+    b = lat.bonds
+    e = -(spins[:, b[:, 0]] * spins[:, b[:, 1]]) @ np.asarray(g["couplings"])
+    np.testing.assert_allclose(e, g["energies_first_64"])
+
+
+def test_oracle_parallel_tempering_matches_enumeration():
+    """critmc tests/test_glass.py:26-52 for a +-J 4x4 sample, on the CPU oracle."""
+    from exact_helpers import ea_exact
+
+    from critmc_b200 import square
+    from critmc_b200.glass import geometric_temperatures
+
+    lat = square(4)
+    J = np.asarray(golden()["ea_square4"]["couplings"])
+    temps = geometric_temperatures(0.4, 2.5, 8)[::-1].copy()  # hot -> cold
+    betas = 1.0 / temps
+    m, n = 8, 16
+    rng = np.random.default_rng(5)
+    spins = (2 * rng.integers(0, 2, size=(2, m, n)) - 1).astype(np.int8)
+    perm = np.tile(np.arange(m, dtype=np.int32), (2, 1))
+    labels = np.zeros((2, m), dtype=np.int32)
+    from critmc_b200 import _lib
+
+    table = np.zeros((m - 1, 2048), dtype=np.uint32)
+    _lib.call("critmc_pt_swap_table", m, np.ascontiguousarray(betas).ctypes.data, 2048, table.ctypes.data)
+    acc, sa, st, lh, tr = oracle.ea_pt_run(spins, J, (4, 4), np.array([[1, 2], [3, 4]]), betas, table,
+                                           perm, labels, n_steps=(1 << 14) - 1, n_bins=14)
+    eq = acc[-1] / acc[-1][:, 6:7]
+    ex = ea_exact(lat, J, temps)
+    np.testing.assert_allclose(eq[:, 0], ex["e"], atol=0.01)
+    np.testing.assert_allclose(eq[:, 3], ex["q2"], atol=0.02)
+    np.testing.assert_allclose(eq[:, 1], ex["ql"], atol=0.02)
+    assert np.all(sa / st > 0.3)
+    assert tr.sum() > 50

@@ -33,6 +33,12 @@ SIGNATURES: dict[str, tuple] = {
          _I32, _I32, _P],
     ),
     "critmc_ising_msc_measure": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+    "critmc_ising_msc_noalloc_max_scratch_bytes": (_I64, []),
+    "critmc_ising_msc_run_noalloc": (
+        _I32,
+        [_P, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P, _P, _I32,
+         _P],
+    ),
     "critmc_ising_msc_init": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P]),
     "critmc_ising_byte_run": (
         _I32,

@@ -7,6 +7,7 @@
 // (`bond_energy`, `magnetization`).
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "host_common.h"
@@ -533,6 +534,141 @@ extern "C" int32_t critmc_ising_msc_init(uint32_t* spins, int32_t dim, int32_t l
   cudaStream_t s = (cudaStream_t)stream;
   const dim3 grid(std::min<uint32_t>(2048, (2 * g.words + 255) / 256), n_chains);
   msc_init_kernel<<<grid, 256, 0, s>>>(spins, g, keys, start);
+  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  return CRITMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Variant of critmc_ising_msc_run that allocates nothing.
+//
+// Some callers cannot allocate device memory where they run the sampler: a
+// plugin inside a host application whose framework owns the device allocator
+// (a caching allocator or a memory pool with a fixed budget), code that must
+// not call cudaMalloc because it would synchronise the device and stall other
+// work, or an embedded host that forbids allocation after start-up.  This
+// entry point takes its scratch (the measurement accumulators) from a
+// file-scope device array instead of a caller buffer.
+// ---------------------------------------------------------------------------
+namespace critmc {
+
+constexpr size_t MSC_NOALLOC_SCRATCH_BYTES = 1u << 20;  // 1 MiB on every device that loads the library
+static __device__ __align__(256) unsigned char g_msc_noalloc_scratch[MSC_NOALLOC_SCRATCH_BYTES];
+
+// Device address of the array on each device, looked up once per device.  In
+// host code the array's name is only a stand-in for the symbol, never a
+// device address, so it must be resolved with cudaGetSymbolAddress while that
+// device is current.
+static void* g_noalloc_addr[64];
+static std::once_flag g_noalloc_once[64];
+static cudaError_t g_noalloc_err[64];
+
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail("cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(CRITMC_ERR_UNSUPPORTED, "device ordinal out of range");
+  std::call_once(g_noalloc_once[dev], [dev] {
+    g_noalloc_err[dev] = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_msc_noalloc_scratch);
+  });
+  if (g_noalloc_err[dev] != cudaSuccess) {
+    set_error(cudaGetErrorString(g_noalloc_err[dev]));
+    return CRITMC_ERR_CUDA;
+  }
+  *out = g_noalloc_addr[dev];
+  return CRITMC_OK;
+}
+
+}  // namespace critmc
+
+extern "C" int64_t critmc_ising_msc_noalloc_max_scratch_bytes(void) {
+  return (int64_t)MSC_NOALLOC_SCRATCH_BYTES;
+}
+
+extern "C" int32_t critmc_ising_msc_run_noalloc(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,
+                                                int32_t lz, int32_t n_chains, const uint32_t* keys,
+                                                const uint32_t* tables, int32_t n_groups,
+                                                uint32_t sweep0, const int64_t* schedule,
+                                                int32_t n_rows, int32_t n_meas, int64_t* running,
+                                                int64_t* e_out, int64_t* m_out, int64_t* aux_out,
+                                                int32_t k_inline, void* stream) {
+  clear_error();
+  MscGeom g;
+  int st = msc_geom(dim, lx, ly, lz, g);
+  if (st) return st;
+  if (!spins || !keys || !tables || !running || !e_out || !m_out || !aux_out)
+    return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (n_chains < 1 || n_chains > 65535) return fail(CRITMC_ERR_INVALID, "n_chains must be in [1, 65535]");
+  if (n_groups < 1 || n_groups > MSC_MAX_GROUPS || n_chains % n_groups != 0)
+    return fail(CRITMC_ERR_INVALID, "n_groups must be in [1, 16] and divide n_chains");
+  if (n_meas < 0) return fail(CRITMC_ERR_INVALID, "n_meas must not be negative");
+  if (!schedule || n_rows < 1) return fail(CRITMC_ERR_INVALID, "empty schedule");
+  if (k_inline != 4 && k_inline != 8) return fail(CRITMC_ERR_INVALID, "k_inline must be 4 or 8");
+  if (critmc_ising_msc_scratch_bytes(n_chains, n_meas) > (int64_t)MSC_NOALLOC_SCRATCH_BYTES)
+    return fail(CRITMC_ERR_INVALID,
+                "n_chains * n_meas too large for the built-in 1 MiB scratch (at most 43690); "
+                "split the call or use critmc_ising_msc_run with caller scratch");
+  long long sweeps_per_meas = 0;
+  for (int r = 0; r < n_rows; ++r) {
+    const int64_t code = schedule[2 * r], reps = schedule[2 * r + 1];
+    if (code != CRITMC_METROPOLIS && code != CRITMC_HEATBATH)
+      return fail(CRITMC_ERR_UNSUPPORTED, "MSC Ising runs checkerboard metropolis and heatbath rows only");
+    if (reps < 1) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be positive");
+    sweeps_per_meas += reps;
+  }
+  if ((long long)sweep0 + sweeps_per_meas * (long long)n_meas > 0xFFFFFFFFLL)
+    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+  if (n_meas == 0) return CRITMC_OK;
+  void* scratch = nullptr;
+  if ((st = noalloc_scratch(&scratch))) return st;
+
+  static thread_local MscTables tabs[2];
+  int rule[2];
+  for (int slot = 0; slot < 2; ++slot) {
+    std::memset(&tabs[slot], 0, sizeof(MscTables));
+    for (int gi = 0; gi < n_groups; ++gi) {
+      const uint32_t* src = tables + (size_t)gi * 4 * CRITMC_NCLS + slot * 2 * CRITMC_NCLS;
+      std::memcpy(tabs[slot].kind[gi], src, CRITMC_NCLS * 4);
+      std::memcpy(tabs[slot].thr[gi], src + CRITMC_NCLS, CRITMC_NCLS * 4);
+    }
+    rule[slot] = msc_pick_rule(&tabs[slot].kind[0][0], &tabs[slot].thr[0][0], 2 * dim,
+                               slot ? CRITMC_HEATBATH : CRITMC_METROPOLIS, n_groups);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  // the array keeps the previous call's contents: clear the accumulators
+  unsigned long long* acc = (unsigned long long*)((char*)scratch + 16);
+  if (cudaMemsetAsync(acc, 0, (size_t)n_chains * n_meas * 3 * 8, s) != cudaSuccess)
+    return cuda_fail("memset");
+  const long long col_threads = (long long)n_chains * g.wc * g.rows;
+  int run = 8;
+  while (run > 1 && col_threads / run < 148LL * 1536) run /= 2;
+  static thread_local MscParams P[2];
+  for (int slot = 0; slot < 2; ++slot) {
+    MscParams& q = P[slot];
+    q.spins = spins;
+    q.acc = acc;
+    q.cursor = nullptr;
+    q.g = g;
+    q.n_chains = n_chains;
+    q.chains_per_group = n_chains / n_groups;
+    q.run = run;
+    q.tabs = tabs[slot];
+  }
+  uint32_t sw = sweep0;
+  for (int meas = 0; meas < n_meas; ++meas)
+    for (int r = 0; r < n_rows; ++r) {
+      const int slot = schedule[2 * r] == CRITMC_HEATBATH ? 1 : 0;
+      for (int64_t rep = 0; rep < schedule[2 * r + 1]; ++rep) {
+        P[slot].sweep = sw;
+        P[slot].meas = (uint32_t)meas;
+        P[slot].col = 0;
+        msc_launch_half(P[slot], keys, rule[slot], k_inline / 4, s);
+        P[slot].col = 1;
+        msc_launch_half(P[slot], keys, rule[slot], k_inline / 4, s);
+        ++sw;
+      }
+    }
+  msc_finalize_kernel<<<n_chains, 256, 0, s>>>((const long long*)acc, (long long*)running,
+                                                (long long*)e_out, (long long*)m_out,
+                                                (long long*)aux_out, n_chains, n_meas);
   if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
   return CRITMC_OK;
 }

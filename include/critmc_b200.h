@@ -206,6 +206,30 @@ int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_t dim, int3
                          int32_t n_bins, int32_t sweeps_per_step, double* acc, int64_t* swap_acc,
                          int64_t* swap_try, int64_t* label_hist, int64_t* trips, void* stream);
 
+/* critmc_ising_msc_run for callers that cannot allocate device memory.
+ * No counterpart in the reference (critmc has no device memory at all).
+ * Some callers cannot call cudaMalloc where they run the sampler: a plugin
+ * whose host framework owns the device allocator, code that must not stall
+ * the device with an allocation, an embedded host that forbids allocation
+ * after start-up.  This variant takes the same arguments minus `scratch`,
+ * `mode` (always one launch per half-sweep, no CUDA graph) and keeps its
+ * accumulators in a 1 MiB array built into the library, which every GPU that
+ * loads the library holds until the process exits.  Limit:
+ * critmc_ising_msc_scratch_bytes(n_chains, n_meas) <= 1 MiB, i.e.
+ * n_chains * n_meas <= 43690; larger calls fail with CRITMC_ERR_INVALID
+ * before any launch.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * It calls no cudaMalloc/cudaFree and creates no streams, events or graphs.  */
+int64_t critmc_ising_msc_noalloc_max_scratch_bytes(void);
+int32_t critmc_ising_msc_run_noalloc(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,
+                                     int32_t lz, int32_t n_chains, const uint32_t* keys,
+                                     const uint32_t* tables, int32_t n_groups, uint32_t sweep0,
+                                     const int64_t* schedule, int32_t n_rows, int32_t n_meas,
+                                     int64_t* running, int64_t* e_out, int64_t* m_out,
+                                     int64_t* aux_out, int32_t k_inline, void* stream);
+
 /* Energy E_b = -sum_<ij> s_i s_j and magnetisation M of MSC chains, written
  * to out[n_chains][2] (device).  critmc kernels/ising.py:32-45.           */
 int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, int32_t lx, int32_t ly,

@@ -180,6 +180,45 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def serve_bench(dev, n_requests: int, rate: float, seed: int = 0) -> dict:
+    """Continuous-batching server on a seeded Poisson stream of mixed requests.
+
+    Workload: ``n_requests`` requests at ``rate``/s, each uniform over 2D Ising
+    L in {16..1024} (beta ~ U[0.38, 0.50]), q=10 Potts L in {16..128}
+    (beta ~ U[1.35, 1.50]) and XY L in {32, 64, 128} (T ~ U[0.8, 1.0]), sweeps
+    log-uniform in [1e3, 1e5].  Latency = arrival -> result on the host.
+    """
+    from critmc_b200.serve import Request, Server, mixed_workload
+
+    reqs = mixed_workload(n_requests, rate, seed)
+    lat, upd = [], [0]
+
+    def on_result(res):
+        lat.append(res.latency)
+        upd[0] += res.updates
+
+    srv = Server(dev, keep_series=False, on_result=lambda r: None)
+    # warm-up: one short request per (model, size) of the mix builds the
+    # lattice cache, the library streams and the kernels' first launches
+    shapes = sorted({(r.model, r.L) for r in reqs})
+    srv.run([Request(m, L, 0.44 if m == "ising" else 1.4 if m == "potts" else 1.1, 20, seed=i)
+             for i, (m, L) in enumerate(shapes)])
+    srv.on_result = on_result
+    srv.ticks, srv.gpu_seconds, srv.updates_done, srv.max_queued, srv.peak_in_use = 0, 0.0, 0, 0, 0
+    srv.t0 = time.perf_counter()
+    srv.run(reqs)
+    wall = srv.now()
+    lat_a = np.array(lat)
+    st = srv.stats()
+    return {"requests": len(lat), "rate_per_s": rate, "wall_s": wall,
+            "p50_latency_s": float(np.percentile(lat_a, 50)), "p99_latency_s": float(np.percentile(lat_a, 99)),
+            "mean_latency_s": float(lat_a.mean()), "max_latency_s": float(lat_a.max()),
+            "updates_per_ns": upd[0] / wall / 1e9, "gpu_busy_frac": st["gpu_seconds"] / wall,
+            "ticks": st["ticks"], "peak_hbm_bytes": st["peak_hbm_bytes"], "max_queued": st["max_queued"],
+            "workload": "Poisson arrivals; Ising L 16..1024 / Potts q=10 L 16..128 / XY L 32..128, "
+                        "sweeps log-uniform 1e3..1e5 (metropolis, metropolis, heatbath)"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -188,6 +227,10 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=10000,
+                    help="requests of the serving run (0 skips it; 1 GPU only)")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -232,6 +275,10 @@ def main() -> None:
         e1.record(s)
         barrier()
         return max_over_ranks(e0.elapsed_time(e1))
+
+    if args.serve_only:
+        print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate)}), flush=True)
+        return
 
     ens = IsingEnsemble(L_HEAD, BETAS, CHAINS_PER_BETA, seed=1000 + rank, device=dev)
     n_upd = ens.n_chains * ens.n_sites  # per step and rank
@@ -295,6 +342,10 @@ def main() -> None:
             "L4096": value / world / extras["plain_one_chain_L4096"],
             "L1024": extras["batched_L1024"] / extras["plain_one_chain_L1024"]}
 
+    serving = None
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        serving = serve_bench(dev, args.serve_requests, args.serve_rate)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(min(32, os.cpu_count() or 1))
@@ -311,7 +362,7 @@ def main() -> None:
                        "l2": "inputs larger than L2 (384 MiB of spins per GPU)"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "gpu_launches": args.steps * (1 + launches_per_step + 1),
-            "clocks": clk.summary(), "extras": extras,
+            "clocks": clk.summary(), "extras": extras, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -45,36 +45,52 @@ struct ByteParams {
   uint32_t keys[BYTE_PCHAINS][2];
 };
 
+// Everything one thread block needs to advance one byte-lattice chain.
+struct ByteChain {
+  int8_t* gl;            // lattice in HBM, [colour][slot]
+  long long* running;    // Ising: (E_b, M); Potts: E
+  long long* counts;     // Potts: [q]
+  long long* e_out;      // [n_meas]
+  long long* m_out;      // Ising: [n_meas]
+  long long* counts_out; // Potts: [n_meas][q]
+  long long* aux_out;    // [n_meas][4]
+  ByteGeom g;
+  int q, n_meas, n_rows, resident;
+  const int* codes;
+  const int* reps;
+  uint32_t sweep0, k0, k1;
+  const uint32_t* kind;  // [2][16] (Ising)
+  const uint32_t* thr;   // [2][16] (Ising)
+  const unsigned long long* boltz;   // [8] (Potts)
+  const unsigned long long* weight;  // [8] (Potts)
+};
+
 template <int MODEL, int Z>
-__global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ ByteParams P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
   __shared__ long long red[16];
   __shared__ int cnt[128];
-  const int lchain = blockIdx.x;
-  const int chain = P.chain0 + lchain;
-  const int group = chain / P.chains_per_group;
-  const ByteGeom& g = P.g;
-  const uint32_t k0 = P.keys[lchain][0], k1 = P.keys[lchain][1];
+  const ByteGeom& g = a.g;
+  const uint32_t k0 = a.k0, k1 = a.k1;
   const size_t n_sites = 2 * (size_t)g.slots;
-  int8_t* gl = P.spins + (size_t)chain * n_sites;
-  int8_t* lat = P.resident ? reinterpret_cast<int8_t*>(smem_raw) : gl;
+  int8_t* gl = a.gl;
+  int8_t* lat = a.resident ? reinterpret_cast<int8_t*>(smem_raw) : gl;
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (P.resident)
+  if (a.resident)
     for (size_t j = tid; j < n_sites; j += nt) lat[j] = gl[j];
-  const int q = P.q;
+  const int q = a.q;
   if (MODEL == MODEL_POTTS)
-    for (int k = tid; k < q; k += nt) cnt[k] = (int)P.counts[(size_t)chain * q + k];
+    for (int k = tid; k < q; k += nt) cnt[k] = (int)a.counts[k];
   __syncthreads();
 
-  long long e_run = (MODEL == MODEL_ISING) ? P.running[2 * chain] : P.running[chain];
-  long long m_run = (MODEL == MODEL_ISING) ? P.running[2 * chain + 1] : 0;
-  uint32_t sweep = P.sweep0;
-  for (int meas = 0; meas < P.n_meas; ++meas) {
+  long long e_run = a.running[0];
+  long long m_run = (MODEL == MODEL_ISING) ? a.running[1] : 0;
+  uint32_t sweep = a.sweep0;
+  for (int meas = 0; meas < a.n_meas; ++meas) {
     long long dE = 0, dM = 0, nacc = 0;
-    for (int row = 0; row < P.n_rows; ++row) {
-      const int code = P.codes[row];
+    for (int row = 0; row < a.n_rows; ++row) {
+      const int code = a.codes[row];
       const int slot_alg = (code == CRITMC_HEATBATH) ? 1 : 0;
-      for (int rep = 0; rep < P.reps[row]; ++rep) {
+      for (int rep = 0; rep < a.reps[row]; ++rep) {
         for (int c = 0; c < 2; ++c) {
           int8_t* own = lat + (size_t)c * g.slots;
           const int8_t* other = lat + (size_t)(c ^ 1) * g.slots;
@@ -95,9 +111,9 @@ __global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ B
               if (slot_alg == 0) v = (Z - old * field) / 2;  // anti-aligned neighbours
               else v = (field + Z) / 2;                       // up neighbours
               const int cls = 2 * v + sb;
-              const uint32_t kd = P.kind[group][slot_alg][cls];
+              const uint32_t kd = a.kind[slot_alg * CRITMC_NCLS + cls];
               const bool dec = kd == CRITMC_KIND_ALWAYS ||
-                               (kd == CRITMC_KIND_RANDOM && rnd.v[0] < P.thr[group][slot_alg][cls]);
+                               (kd == CRITMC_KIND_RANDOM && rnd.v[0] < a.thr[slot_alg * CRITMC_NCLS + cls]);
               const int nw = slot_alg == 0 ? (dec ? -old : old) : (dec ? 1 : -1);
               if (nw != old) {
                 own[s] = (int8_t)nw;
@@ -121,7 +137,7 @@ __global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ B
                   n_new += nbs[k] == nw;
                 }
                 const int delta = n_old - n_new;
-                const bool acc = delta <= 0 || (unsigned long long)rnd.v[1] < P.boltz[group][delta];
+                const bool acc = delta <= 0 || (unsigned long long)rnd.v[1] < a.boltz[delta];
                 if (acc) {
                   own[s] = (int8_t)nw;
                   atomicSub(&cnt[old], 1);
@@ -137,7 +153,7 @@ __global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ B
                   int nk = 0;
 #pragma unroll
                   for (int j = 0; j < Z; ++j) nk += nbs[j] == k;
-                  total += P.weight[group][nk];
+                  total += a.weight[nk];
                 }
                 const unsigned long long x = __umul64hi(u, total);
                 unsigned long long cum = 0;
@@ -146,7 +162,7 @@ __global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ B
                   int nk = 0;
 #pragma unroll
                   for (int j = 0; j < Z; ++j) nk += nbs[j] == k;
-                  cum += P.weight[group][nk];
+                  cum += a.weight[nk];
                   if (x < cum) {
                     nw = k;
                     break;
@@ -178,31 +194,58 @@ __global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ B
     nacc = block_sum(nacc, red);
     e_run += dE;
     m_run += dM;
-    const size_t o = (size_t)chain * P.n_meas + meas;
     if (tid == 0) {
-      P.e_out[o] = e_run;
-      if (MODEL == MODEL_ISING) P.m_out[o] = m_run;
-      P.aux_out[4 * o + 0] = nacc;
-      P.aux_out[4 * o + 1] = 0;
-      P.aux_out[4 * o + 2] = 0;
-      P.aux_out[4 * o + 3] = 0;
+      a.e_out[meas] = e_run;
+      if (MODEL == MODEL_ISING) a.m_out[meas] = m_run;
+      a.aux_out[4 * meas + 0] = nacc;
+      a.aux_out[4 * meas + 1] = 0;
+      a.aux_out[4 * meas + 2] = 0;
+      a.aux_out[4 * meas + 3] = 0;
     }
     if (MODEL == MODEL_POTTS)
-      for (int k = tid; k < q; k += nt) P.counts_out[o * q + k] = cnt[k];
+      for (int k = tid; k < q; k += nt) a.counts_out[(size_t)meas * q + k] = cnt[k];
   }
   __syncthreads();
-  if (P.resident)
+  if (a.resident)
     for (size_t j = tid; j < n_sites; j += nt) gl[j] = lat[j];
   if (tid == 0) {
-    if (MODEL == MODEL_ISING) {
-      P.running[2 * chain] = e_run;
-      P.running[2 * chain + 1] = m_run;
-    } else {
-      P.running[chain] = e_run;
-    }
+    a.running[0] = e_run;
+    if (MODEL == MODEL_ISING) a.running[1] = m_run;
   }
   if (MODEL == MODEL_POTTS)
-    for (int k = tid; k < q; k += nt) P.counts[(size_t)chain * q + k] = cnt[k];
+    for (int k = tid; k < q; k += nt) a.counts[k] = cnt[k];
+  __syncthreads();
+}
+
+template <int MODEL, int Z>
+__global__ void __launch_bounds__(512) byte_run_kernel(const __grid_constant__ ByteParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lchain = blockIdx.x;
+  const int chain = P.chain0 + lchain;
+  const int group = chain / P.chains_per_group;
+  ByteChain a;
+  a.g = P.g;
+  a.gl = P.spins + (size_t)chain * 2 * P.g.slots;
+  a.running = P.running + (MODEL == MODEL_ISING ? 2 * (size_t)chain : (size_t)chain);
+  a.counts = P.counts ? P.counts + (size_t)chain * P.q : nullptr;
+  a.e_out = P.e_out + (size_t)chain * P.n_meas;
+  a.m_out = P.m_out ? P.m_out + (size_t)chain * P.n_meas : nullptr;
+  a.counts_out = P.counts_out ? P.counts_out + (size_t)chain * P.n_meas * P.q : nullptr;
+  a.aux_out = P.aux_out + (size_t)chain * P.n_meas * 4;
+  a.q = P.q;
+  a.n_meas = P.n_meas;
+  a.n_rows = P.n_rows;
+  a.resident = P.resident;
+  a.codes = P.codes;
+  a.reps = P.reps;
+  a.sweep0 = P.sweep0;
+  a.k0 = P.keys[lchain][0];
+  a.k1 = P.keys[lchain][1];
+  a.kind = &P.kind[group][0][0];
+  a.thr = &P.thr[group][0][0];
+  a.boltz = P.boltz[group];
+  a.weight = P.weight[group];
+  byte_chain_run<MODEL, Z>(a, smem_raw);
 }
 
 static int byte_schedule(ByteParams& P, const int64_t* schedule, int n_rows, long long& per_meas) {
@@ -359,3 +402,83 @@ extern "C" int32_t critmc_potts_run(int8_t* spins, int32_t dim, int32_t lx, int3
   P.sweep0 = sweep0;
   return byte_launch<MODEL_POTTS>(P, keys, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Byte-lattice chains as work items (persistent kernel, queue of items).
+// ---------------------------------------------------------------------------
+#include "items_host.h"
+
+namespace critmc {
+
+__device__ __forceinline__ int byte_geom_device(const critmc_item& it, ByteGeom& g) {
+  g.dim = it.dim;
+  g.lx = it.lx;
+  g.ly = it.dim >= 2 ? it.ly : 1;
+  g.lz = it.dim >= 3 ? it.lz : 1;
+  g.hx = it.lx / 2;
+  g.rows = g.ly * g.lz;
+  g.slots = (uint32_t)(g.rows * g.hx);
+  return 0;
+}
+
+__global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_item* items, int n,
+                                                                  unsigned* queue, size_t smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int cur;
+  for (;;) {
+    if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int i = cur;
+    __syncthreads();
+    if (i >= n) break;
+    const critmc_item& it = items[i];
+    ByteChain a;
+    byte_geom_device(it, a.g);
+    a.gl = reinterpret_cast<int8_t*>(it.spins);
+    a.running = reinterpret_cast<long long*>(it.running);
+    a.counts = reinterpret_cast<long long*>(it.counts);
+    a.e_out = reinterpret_cast<long long*>(it.e_out);
+    a.m_out = reinterpret_cast<long long*>(it.vec_out);
+    a.counts_out = reinterpret_cast<long long*>(it.vec_out);
+    a.aux_out = reinterpret_cast<long long*>(it.aux_out);
+    a.q = it.kind == CRITMC_ITEM_POTTS ? it.q_or_n : 2;
+    a.n_meas = it.n_meas;
+    a.n_rows = it.n_rows;
+    a.resident = 2 * (size_t)a.g.slots <= smem;
+    a.codes = it.codes;
+    a.reps = it.reps;
+    a.sweep0 = it.sweep0;
+    a.k0 = it.key[0];
+    a.k1 = it.key[1];
+    a.kind = &it.kind_tab[0][0];
+    a.thr = &it.thr_tab[0][0];
+    a.boltz = reinterpret_cast<const unsigned long long*>(it.boltz);
+    a.weight = reinterpret_cast<const unsigned long long*>(it.weight);
+    if (it.kind == CRITMC_ITEM_POTTS) {
+      if (it.dim == 1) byte_chain_run<MODEL_POTTS, 2>(a, smem_raw);
+      else if (it.dim == 2) byte_chain_run<MODEL_POTTS, 4>(a, smem_raw);
+      else byte_chain_run<MODEL_POTTS, 6>(a, smem_raw);
+    } else {
+      if (it.dim == 1) byte_chain_run<MODEL_ISING, 2>(a, smem_raw);
+      else if (it.dim == 2) byte_chain_run<MODEL_ISING, 4>(a, smem_raw);
+      else byte_chain_run<MODEL_ISING, 6>(a, smem_raw);
+    }
+  }
+}
+
+int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(byte_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return cuda_fail("shared memory attribute");
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, byte_items_kernel, ITEM_THREADS, smem);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
+  byte_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem);
+  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  return CRITMC_OK;
+}
+
+}  // namespace critmc

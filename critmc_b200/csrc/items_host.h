@@ -1,0 +1,18 @@
+// Per-family launchers of the work-item kernels (implemented next to each
+// family's sweep code) used by critmc_run_items.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "critmc_b200.h"
+
+namespace critmc {
+
+constexpr int ITEM_THREADS = 512;
+
+// Each launcher starts a persistent kernel over `n` items at `items` (device)
+// whose blocks pull item indices from *queue (zeroed by the caller).
+int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
+int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
+int on_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
+
+}  // namespace critmc

@@ -672,3 +672,179 @@ extern "C" int32_t critmc_ising_msc_run_noalloc(uint32_t* spins, int32_t dim, in
   if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
   return CRITMC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Resident MSC chains as work items: the whole lattice of a chain sits in
+// shared memory while its block applies the schedule n_meas times.  Same
+// random stream as the half-sweep kernel (word index, sweep, colour).
+// ---------------------------------------------------------------------------
+#include "items_host.h"
+
+namespace critmc {
+
+constexpr int MSCI_WARPS = ITEM_THREADS / 32;
+
+// one colour of one sweep over the resident lattice
+template <int Z, int RULE>
+__device__ void msci_colour(const MscRule<Z, RULE>& rule, const MscGeom& g, uint32_t* lat, int c,
+                            uint32_t sweep, uint32_t k0, uint32_t k1, MscFix (*fix)[64],
+                            long long& dE, long long& dM, long long& nacc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t* own = lat + (size_t)c * g.words;
+  const uint32_t* other = lat + (size_t)(c ^ 1) * g.words;
+  int idE = 0, idM = 0, inacc = 0;
+  int nf = 0;
+  auto flush = [&]() {
+    __syncwarp();
+    for (int e = lane; e < nf; e += 32) {
+      const MscFix f = fix[warp][e];
+      int y, z, k;
+      msc_row_coords<Z>(g, f.w, y, z, k);
+      uint32_t n[Z];
+      msc_neighbours<Z>(other, g, c, y, z, k, n);
+      MscWord w;
+      rule.classify(own[f.w], n, w);
+      w.D = f.D;
+      w.U = f.U;
+      for (int grp = 2; grp < 8 && w.U != 0; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, f.w, sweep, (uint32_t)c, grp);
+      const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
+      msc_obs<Z>((w.s ^ s_new) & f.U, w.s, w.anti, idE, idM, inacc);
+      own[f.w] = s_new;
+    }
+    __syncwarp();
+    nf = 0;
+  };
+  const uint32_t rounds = (g.words + ITEM_THREADS - 1) / ITEM_THREADS;
+  for (uint32_t it = 0; it < rounds; ++it) {
+    const uint32_t widx = it * ITEM_THREADS + threadIdx.x;
+    MscWord w;
+    w.U = 0;
+    if (widx < g.words) {
+      int y, z, k;
+      msc_row_coords<Z>(g, widx, y, z, k);
+      uint32_t n[Z];
+      msc_neighbours<Z>(other, g, c, y, z, k, n);
+      rule.classify(own[widx], n, w);
+      msc_group<Z, RULE>(rule, w, k0, k1, widx, sweep, (uint32_t)c, 0);
+      msc_group<Z, RULE>(rule, w, k0, k1, widx, sweep, (uint32_t)c, 1);
+      const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
+      msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, idE, idM, inacc);
+      if (w.U == 0) own[widx] = s_new;
+    }
+    const uint32_t need = __ballot_sync(0xffffffffu, w.U != 0);
+    if (need) {
+      const int cnt = __popc(need);
+      if (nf + cnt > 64) flush();
+      if (w.U != 0) fix[warp][nf + __popc(need & lt_mask)] = MscFix{widx, w.U, w.D};
+      nf += cnt;
+    }
+  }
+  if (nf) flush();
+  dE += idE;
+  dM += idM;
+  nacc += inacc;
+  __syncthreads();
+}
+
+template <int Z>
+__device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[64]) {
+  __shared__ long long red[MSCI_WARPS];
+  MscGeom g;
+  msc_geom_device(it.dim, it.lx, it.ly, it.lz, g);
+  uint32_t* gl = reinterpret_cast<uint32_t*>(it.spins);
+  const int tid = threadIdx.x;
+  for (uint32_t j = tid; j < 2 * g.words; j += ITEM_THREADS) lat[j] = gl[j];
+  __syncthreads();
+  long long e_run = it.running[0], m_run = it.running[1];
+  uint32_t sweep = it.sweep0;
+  for (int meas = 0; meas < it.n_meas; ++meas) {
+    long long dE = 0, dM = 0, nacc = 0;
+    for (int row = 0; row < it.n_rows; ++row) {
+      const int slot = it.codes[row] == CRITMC_HEATBATH ? 1 : 0;
+      const uint32_t* kd = it.kind_tab[slot];
+      const uint32_t* th = it.thr_tab[slot];
+      for (int rep = 0; rep < it.reps[row]; ++rep) {
+        for (int c = 0; c < 2; ++c) {
+          switch (it.rule[slot]) {
+            case RULE_METRO0:
+              msci_colour<Z, RULE_METRO0>(MscRule<Z, RULE_METRO0>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              break;
+            case RULE_HB0:
+              msci_colour<Z, RULE_HB0>(MscRule<Z, RULE_HB0>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              break;
+            case RULE_GEN:
+              msci_colour<Z, RULE_GEN>(MscRule<Z, RULE_GEN>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              break;
+            default:
+              msci_colour<Z, RULE_GENSPIN>(MscRule<Z, RULE_GENSPIN>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              break;
+          }
+        }
+        ++sweep;
+      }
+    }
+    dE = warp_sum(dE);
+    dM = warp_sum(dM);
+    nacc = warp_sum(nacc);
+    long long tot[3] = {0, 0, 0};
+    const long long vals[3] = {dE, dM, nacc};
+    for (int q = 0; q < 3; ++q) {
+      if ((tid & 31) == 0) red[tid >> 5] = vals[q];
+      __syncthreads();
+      for (int w = 0; w < MSCI_WARPS; ++w) tot[q] += red[w];
+      __syncthreads();
+    }
+    e_run += tot[0];
+    m_run += tot[1];
+    if (tid == 0) {
+      reinterpret_cast<long long*>(it.e_out)[meas] = e_run;
+      reinterpret_cast<long long*>(it.vec_out)[meas] = m_run;
+      it.aux_out[4 * meas + 0] = tot[2];
+      it.aux_out[4 * meas + 1] = 0;
+      it.aux_out[4 * meas + 2] = 0;
+      it.aux_out[4 * meas + 3] = 0;
+    }
+  }
+  for (uint32_t j = tid; j < 2 * g.words; j += ITEM_THREADS) gl[j] = lat[j];
+  if (tid == 0) {
+    it.running[0] = e_run;
+    it.running[1] = m_run;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(ITEM_THREADS) msc_items_kernel(const critmc_item* items, int n,
+                                                                 unsigned* queue) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ MscFix fix[MSCI_WARPS][64];
+  __shared__ int cur;
+  uint32_t* lat = reinterpret_cast<uint32_t*>(smem_raw);
+  for (;;) {
+    if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int i = cur;
+    __syncthreads();
+    if (i >= n) break;
+    const critmc_item& it = items[i];
+    if (it.dim == 2) msci_chain<4>(it, lat, fix);
+    else msci_chain<6>(it, lat, fix);
+  }
+}
+
+int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(msc_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return cuda_fail("shared memory attribute");
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, msc_items_kernel, ITEM_THREADS, smem);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
+  msc_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue);
+  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  return CRITMC_OK;
+}
+
+}  // namespace critmc

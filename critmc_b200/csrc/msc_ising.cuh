@@ -30,6 +30,18 @@ struct MscGeom {
   uint32_t words;   // rows * wc (words per colour per chain)
 };
 
+// geometry of a 2D/3D MSC lattice on the device (extents validated on the host)
+__device__ __forceinline__ void msc_geom_device(int dim, int lx, int ly, int lz, MscGeom& g) {
+  g.dim = dim;
+  g.lx = lx;
+  g.ly = ly;
+  g.lz = dim == 3 ? lz : 1;
+  g.wc = lx >> 6;
+  g.wc_log2 = 31 - __clz(g.wc);
+  g.rows = ly * g.lz;
+  g.words = (uint32_t)g.rows * (uint32_t)g.wc;
+}
+
 enum MscRuleKind { RULE_METRO0 = 0, RULE_HB0 = 1, RULE_GEN = 2, RULE_GENSPIN = 3 };
 
 constexpr int MSC_MAX_GROUPS = 16;

@@ -114,23 +114,46 @@ __device__ __forceinline__ float von_mises(float kappa, const critmc_u32x4& r0, 
   return u01(r0.v[2]) < 0.5f ? theta : -theta;
 }
 
+// Everything one thread block needs to advance one O(n) chain.
+struct OnChain {
+  float* gl;          // lattice in HBM, [component][colour][slot]
+  double* e_out;      // [n_meas]
+  double* m_out;      // [n_meas][N]
+  double* sc_out;     // [n_meas][dim]
+  double* ss_out;     // [n_meas][dim]
+  long long* aux_out; // [n_meas][4]
+  ByteGeom g;
+  int n_meas, n_rows, resident;
+  int nt;  // threads that own sites (a multiple of 32); the FP64 sums depend on it
+  const int* codes;
+  const int* reps;
+  uint32_t sweep0, k0, k1;
+  float beta, step;
+};
+
+// Threads owning sites for a chain of `slots` sites per colour: the per-chain
+// launch uses exactly this many threads, larger blocks leave the rest idle so
+// the FP64 partial sums (and their order) are the same.
+__host__ __device__ inline int on_site_threads(uint32_t slots) {
+  const uint32_t t = ((slots + 31) / 32) * 32;
+  return (int)(t < 32 ? 32 : (t > 512 ? 512 : t));
+}
+
 template <int N, int Z>
-__global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnParams P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
   __shared__ double red[16];
-  const int lchain = blockIdx.x;
-  const int chain = P.chain0 + lchain;
-  const int group = chain / P.chains_per_group;
   const ByteGeom& g = P.g;
-  const uint32_t k0 = P.keys[lchain][0], k1 = P.keys[lchain][1];
+  const uint32_t k0 = P.k0, k1 = P.k1;
   const size_t n_sites = 2 * (size_t)g.slots;
-  float* gl = P.spins + (size_t)chain * N * n_sites;
+  float* gl = P.gl;
   float* lat = P.resident ? reinterpret_cast<float*>(smem_raw) : gl;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  // idle threads (tid >= nt) start every site loop past its end but take part in the barriers
+  const int tid = threadIdx.x, nt = P.nt;
+  const uint32_t t0 = tid < nt ? (uint32_t)tid : 0x7fffffffu;
   if (P.resident)
-    for (size_t j = tid; j < N * n_sites; j += nt) lat[j] = gl[j];
+    for (size_t j = t0; j < N * n_sites; j += nt) lat[j] = gl[j];
   __syncthreads();
-  const float beta = P.beta[group], step = P.step[group];
+  const float beta = P.beta, step = P.step;
   constexpr int DIM = Z / 2;
   uint32_t sweep = P.sweep0;
 
@@ -140,7 +163,7 @@ __global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnP
       const int code = P.codes[row];
       for (int rep = 0; rep < P.reps[row]; ++rep) {
         for (int c = 0; c < 2; ++c) {
-          for (uint32_t s = tid; s < g.slots; s += nt) {
+          for (uint32_t s = t0; s < g.slots; s += nt) {
             uint32_t nb[Z];
             int y, z;
             on_neighbours<Z>(g, c, s, nb, y, z);
@@ -261,7 +284,7 @@ __global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnP
       }
     }
     // normalise every spin (on.py:79-87), then measure in FP64
-    for (uint32_t j = tid; j < 2 * g.slots; j += nt) {
+    for (uint32_t j = t0; j < 2 * g.slots; j += nt) {
       float v[N], nrm = 0.0f;
 #pragma unroll
       for (int k = 0; k < N; ++k) {
@@ -278,7 +301,7 @@ __global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnP
     for (int k = 0; k < N; ++k) m[k] = 0.0;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) sc[a] = ss[a] = 0.0;
-    for (uint32_t j = tid; j < 2 * g.slots; j += nt) {
+    for (uint32_t j = t0; j < 2 * g.slots; j += nt) {
       const int c = j >= g.slots;
       const uint32_t s = j - c * g.slots;
       uint32_t nb[Z];
@@ -313,7 +336,7 @@ __global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnP
     }
     const long long acc_all = block_sum(nacc, reinterpret_cast<long long*>(red));
     if (tid == 0) {
-      const size_t o = (size_t)chain * P.n_meas + meas;
+      const size_t o = (size_t)meas;
       P.e_out[o] = e;
 #pragma unroll
       for (int k = 0; k < N; ++k) P.m_out[o * N + k] = m[k];
@@ -330,7 +353,37 @@ __global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnP
   }
   __syncthreads();
   if (P.resident)
-    for (size_t j = tid; j < N * n_sites; j += nt) gl[j] = lat[j];
+    for (size_t j = t0; j < N * n_sites; j += nt) gl[j] = lat[j];
+  __syncthreads();
+}
+
+template <int N, int Z>
+__global__ void __launch_bounds__(512) on_run_kernel(const __grid_constant__ OnParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lchain = blockIdx.x;
+  const int chain = P.chain0 + lchain;
+  const int group = chain / P.chains_per_group;
+  constexpr int DIM = Z / 2;
+  OnChain a;
+  a.g = P.g;
+  a.gl = P.spins + (size_t)chain * N * 2 * P.g.slots;
+  a.e_out = P.e_out + (size_t)chain * P.n_meas;
+  a.m_out = P.m_out + (size_t)chain * P.n_meas * N;
+  a.sc_out = P.sc_out + (size_t)chain * P.n_meas * DIM;
+  a.ss_out = P.ss_out + (size_t)chain * P.n_meas * DIM;
+  a.aux_out = P.aux_out + (size_t)chain * P.n_meas * 4;
+  a.n_meas = P.n_meas;
+  a.n_rows = P.n_rows;
+  a.resident = P.resident;
+  a.nt = blockDim.x;
+  a.codes = P.codes;
+  a.reps = P.reps;
+  a.sweep0 = P.sweep0;
+  a.k0 = P.keys[lchain][0];
+  a.k1 = P.keys[lchain][1];
+  a.beta = P.beta[group];
+  a.step = P.step[group];
+  on_chain_run<N, Z>(a, smem_raw);
 }
 
 static thread_local OnParams g_on;
@@ -389,8 +442,7 @@ extern "C" int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t 
   const size_t lat_bytes = (size_t)n * 2 * P.g.slots * sizeof(float);
   P.resident = lat_bytes <= (size_t)ON_SMEM_MAX;
   const size_t smem = P.resident ? lat_bytes : 0;
-  int threads = (int)std::min<uint32_t>(512, ((P.g.slots + 31) / 32) * 32);
-  threads = std::max(threads, 32);
+  const int threads = on_site_threads(P.g.slots);
   cudaStream_t s = (cudaStream_t)stream;
   for (int c0 = 0; c0 < n_chains; c0 += ON_PCHAINS) {
     const int nc = std::min(ON_PCHAINS, n_chains - c0);
@@ -413,3 +465,75 @@ extern "C" int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t 
   }
   return CRITMC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// O(n) chains as work items (persistent kernel, queue of items).
+// ---------------------------------------------------------------------------
+#include "items_host.h"
+
+namespace critmc {
+
+__global__ void __launch_bounds__(ITEM_THREADS) on_items_kernel(const critmc_item* items, int n,
+                                                                unsigned* queue, size_t smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int cur;
+  for (;;) {
+    if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int i = cur;
+    __syncthreads();
+    if (i >= n) break;
+    const critmc_item& it = items[i];
+    OnChain a;
+    a.g.dim = it.dim;
+    a.g.lx = it.lx;
+    a.g.ly = it.dim >= 2 ? it.ly : 1;
+    a.g.lz = it.dim >= 3 ? it.lz : 1;
+    a.g.hx = it.lx / 2;
+    a.g.rows = a.g.ly * a.g.lz;
+    a.g.slots = (uint32_t)(a.g.rows * a.g.hx);
+    a.gl = reinterpret_cast<float*>(it.spins);
+    a.e_out = reinterpret_cast<double*>(it.e_out);
+    a.m_out = reinterpret_cast<double*>(it.vec_out);
+    a.sc_out = it.sc_out;
+    a.ss_out = it.ss_out;
+    a.aux_out = reinterpret_cast<long long*>(it.aux_out);
+    a.n_meas = it.n_meas;
+    a.n_rows = it.n_rows;
+    a.resident = (size_t)it.q_or_n * 2 * a.g.slots * sizeof(float) <= smem;
+    a.nt = on_site_threads(a.g.slots);
+    a.codes = it.codes;
+    a.reps = it.reps;
+    a.sweep0 = it.sweep0;
+    a.k0 = it.key[0];
+    a.k1 = it.key[1];
+    a.beta = it.beta;
+    a.step = it.step;
+    const int key = it.q_or_n * 10 + it.dim;
+    switch (key) {
+      case 21: on_chain_run<2, 2>(a, smem_raw); break;
+      case 22: on_chain_run<2, 4>(a, smem_raw); break;
+      case 23: on_chain_run<2, 6>(a, smem_raw); break;
+      case 31: on_chain_run<3, 2>(a, smem_raw); break;
+      case 32: on_chain_run<3, 4>(a, smem_raw); break;
+      default: on_chain_run<3, 6>(a, smem_raw); break;
+    }
+  }
+}
+
+int on_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(on_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return cuda_fail("shared memory attribute");
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, on_items_kernel, ITEM_THREADS, smem);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
+  on_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem);
+  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  return CRITMC_OK;
+}
+
+}  // namespace critmc

@@ -147,6 +147,32 @@ class _IsingMscChain:
         self.mode = 0
         self.k_inline = 8
 
+    @classmethod
+    def on_device(cls, model: "Ising", key: np.ndarray, device, start: int = 0) -> "_IsingMscChain":
+        """A chain whose configuration is drawn on the device (``critmc_ising_msc_init``)."""
+        self = cls.__new__(cls)
+        self.device = require_cuda(device)
+        self.shape = model.lattice.shape
+        self.dims = tuple(self.shape) + (1,) * (3 - len(self.shape))
+        lx, ly, lz = self.dims
+        self.words = torch.empty((2, ly * lz, lx // 64), dtype=torch.int32, device=self.device)
+        self.key = np.ascontiguousarray(key, dtype=np.uint32).reshape(1, 2)
+        self.sweep = 0
+        self.mode = 0
+        self.k_inline = 8
+        dkey = to_dev(self.key, self.device)
+        _lib.call("critmc_ising_msc_init", ptr(self.words), len(self.shape), lx, ly, lz, 1, ptr(dkey), start,
+                  stream_handle(self.device))
+        return self
+
+    def measure(self) -> torch.Tensor:
+        """Device int64 (E_b, M) of the current configuration."""
+        out = torch.empty((1, 2), dtype=torch.int64, device=self.device)
+        lx, ly, lz = self.dims
+        _lib.call("critmc_ising_msc_measure", ptr(self.words), len(self.shape), lx, ly, lz, 1, ptr(out),
+                  stream_handle(self.device))
+        return out
+
     def fetch(self) -> np.ndarray:
         return msc_unpack(to_host(self.words, np.uint32), self.shape)
 

@@ -206,6 +206,64 @@ int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_t dim, int3
                          int32_t n_bins, int32_t sweeps_per_step, double* acc, int64_t* swap_acc,
                          int64_t* swap_try, int64_t* label_hist, int64_t* trips, void* stream);
 
+/* ---- heterogeneous work items (continuous batching, serving) --------------
+ * One item advances one chain by n_meas schedule applications: any model and
+ * lattice size, its own beta, key and sweep counter.  critmc_run_items runs
+ * a persistent kernel per model family (multi-spin-coded Ising resident in
+ * shared memory, byte lattices, O(n)) whose thread blocks pull items from a
+ * queue until it is empty, so chains of different sizes and lengths share the
+ * GPU.  Random streams are those of the per-model entry points (an item gives
+ * the same results as critmc_ising_msc_run / critmc_ising_byte_run /
+ * critmc_potts_run / critmc_on_run for the same chain), so a chain's result
+ * does not depend on what it is batched with.  No counterpart in critmc, which
+ * runs one chain per process (src/critmc/runner.py:154-223).                 */
+#define CRITMC_ITEM_MSC_ISING 0 /* spins: uint32 MSC words (2D/3D, lx/64 power of two, <= 1024^2) */
+#define CRITMC_ITEM_BYTE_ISING 1 /* spins: int8 colour-major */
+#define CRITMC_ITEM_POTTS 2     /* spins: int8 colour-major, q_or_n = q */
+#define CRITMC_ITEM_ON 3        /* spins: float32 [n][colour][slot], q_or_n = n */
+
+typedef struct {
+  void* spins;       /* device: the chain's lattice, advanced in place */
+  int64_t* running;  /* device: Ising (E_b, M); Potts E; unused for O(n) */
+  int64_t* counts;   /* device: Potts counts[q] in/out */
+  void* e_out;       /* device: [n_meas], int64 (Ising, Potts) or double (O(n)) */
+  void* vec_out;     /* device: Ising M [n_meas] int64; Potts counts [n_meas][q] int64;
+                        O(n) M [n_meas][n] double */
+  double* sc_out;    /* device: O(n) stiffness sums [n_meas][dim] */
+  double* ss_out;
+  int64_t* aux_out;  /* device: [n_meas][4] */
+  int32_t kind;      /* CRITMC_ITEM_* */
+  int32_t dim, lx, ly, lz, q_or_n;
+  uint32_t key[2];
+  uint32_t sweep0;
+  int32_t n_meas;
+  int32_t n_rows;
+  int32_t codes[4], reps[4];
+  int32_t rule[2];   /* filled by critmc_item_prepare */
+  float beta, step;  /* O(n) */
+  uint32_t kind_tab[2][16], thr_tab[2][16]; /* Ising acceptance classes (metropolis, heat bath) */
+  uint64_t boltz[8], weight[8];             /* Potts tables */
+} critmc_item;
+
+/* Fill the acceptance tables of an item for inverse temperature beta (and
+ * field h for Ising) and check its geometry and schedule.                   */
+int32_t critmc_item_prepare(critmc_item* item, double beta, double h, double step);
+
+/* Device bytes needed to run n_items items (descriptors + queue counters).  */
+int64_t critmc_items_buffer_bytes(int32_t n_items);
+
+/* Copy the HOST items to the DEVICE buffer (grouped by family) and run them;
+ * the three family kernels run side by side on library-owned streams forked
+ * from and joined into `stream` (CUDA-graph capturable).
+ * staging: NULL, or PINNED host memory of n_items * sizeof(critmc_item)
+ *   bytes that the call fills and copies from asynchronously (do not reuse it
+ *   before `stream` has passed this call).  With NULL the copy comes from
+ *   pageable memory and may wait for `stream`.
+ * smem_limit: dynamic shared memory per block allowed for byte/O(n) lattices
+ * (larger lattices are updated in HBM); 0 picks 200 KiB.                    */
+int32_t critmc_run_items(const critmc_item* items, int32_t n_items, void* buffer,
+                         int64_t buffer_bytes, void* staging, int32_t smem_limit, void* stream);
+
 /* critmc_ising_msc_run for callers that cannot allocate device memory.
  * No counterpart in the reference (critmc has no device memory at all).
  * Some callers cannot call cudaMalloc where they run the sampler: a plugin

@@ -73,3 +73,27 @@ def test_potts_tables_are_monotone(beta):
     assert b[0] == 1 << 32
     assert np.all(np.diff(b[:5].astype(np.float64)) <= 0)
     assert w[4] == 1 << 52 if beta > 0 else True
+
+
+def test_item_struct_matches_the_header():
+    """The ctypes mirror has the C struct's size; item preparation is host-only."""
+    from critmc_b200.items import ITEM_ON, ITEM_POTTS, CritmcItem
+
+    lib = _lib.lib()
+    assert ctypes.sizeof(CritmcItem) == lib.critmc_items_buffer_bytes(1) - lib.critmc_items_buffer_bytes(0)
+    it = CritmcItem()
+    it.kind, it.dim, it.lx, it.ly, it.n_rows = 0, 2, 64, 64, 1
+    it.codes[0], it.reps[0] = 0, 1
+    assert _lib.lib().critmc_item_prepare(ctypes.byref(it), 0.4406868, 0.0, 1.0) == 0
+    assert it.kind_tab[0][0] != 0 or it.thr_tab[0][0] != 0
+    it.kind, it.q_or_n = ITEM_POTTS, 3
+    assert _lib.lib().critmc_item_prepare(ctypes.byref(it), 1.0, 0.0, 1.0) == 0
+    assert it.boltz[0] != 0
+    it.kind, it.q_or_n, it.codes[0] = ITEM_ON, 2, 5
+    assert _lib.lib().critmc_item_prepare(ctypes.byref(it), 1.25, 0.0, 0.5) == 0
+    assert (it.beta, it.step) == (1.25, 0.5)
+    it.kind = ITEM_POTTS  # over-relaxation is an O(n) move only
+    assert _lib.lib().critmc_item_prepare(ctypes.byref(it), 1.0, 0.0, 1.0) != 0
+    it.kind = 9
+    assert _lib.lib().critmc_item_prepare(ctypes.byref(it), 1.0, 0.0, 1.0) != 0
+    assert _lib.lib().critmc_run_items(None, 0, None, 0, None, 0, None) == 0

@@ -27,6 +27,15 @@ int family_of(int kind) {
   }
 }
 
+// Launch groups: one persistent kernel each.  0 multi-spin-coded Ising,
+// 1 byte lattices, 2..7 O(n) by (n, dim) (a kernel per variant).
+constexpr int N_GROUPS = 8;
+int group_of(const critmc_item& it) {
+  const int fam = family_of(it.kind);
+  if (fam < 2) return fam;
+  return 2 + (it.q_or_n - 2) * 3 + (it.dim - 1);
+}
+
 int check_schedule(const critmc_item& it) {
   if (it.n_rows < 1 || it.n_rows > 4) return fail(CRITMC_ERR_INVALID, "items take 1..4 schedule rows");
   for (int r = 0; r < it.n_rows; ++r) {
@@ -72,6 +81,7 @@ size_t item_smem(const critmc_item& it, int fam, size_t limit) {
     msc_geom(it.dim, it.lx, it.ly, it.lz, g);
     return 2 * (size_t)g.words * 4;
   }
+  if (fam >= 2) fam = 2;
   ByteGeom g;
   byte_geom(it.dim, it.lx, it.ly, it.lz, g);
   const size_t need = fam == 1 ? 2 * (size_t)g.slots : (size_t)it.q_or_n * 2 * g.slots * 4;
@@ -116,8 +126,8 @@ namespace {
 // re-recorded while a wait on them is being enqueued.
 struct FamilyStreams {
   bool ready = false;
-  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t aux[N_GROUPS] = {};
+  cudaEvent_t fork = nullptr, join[N_GROUPS] = {};
 };
 std::mutex g_family_mutex;
 FamilyStreams g_family[64];
@@ -126,7 +136,7 @@ int family_streams(int dev, FamilyStreams*& out) {
   if (dev < 0 || dev >= 64) return fail(CRITMC_ERR_UNSUPPORTED, "device ordinal above 63");
   FamilyStreams& f = g_family[dev];
   if (!f.ready) {
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < N_GROUPS; ++k) {
       if (cudaStreamCreateWithFlags(&f.aux[k], cudaStreamNonBlocking) != cudaSuccess) return cuda_fail("stream");
       if (cudaEventCreateWithFlags(&f.join[k], cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
     }
@@ -155,17 +165,19 @@ extern "C" int32_t critmc_run_items(const critmc_item* items, int32_t n_items, v
     own.resize(n_items);
     sorted = own.data();
   }
-  int count[3] = {0, 0, 0};
-  size_t smem[3] = {0, 0, 0};
+  int count[N_GROUPS] = {};
+  size_t smem[N_GROUPS] = {};
   int fill = 0;
-  for (int f = 0; f < 3; ++f)
+  for (int i = 0; i < n_items; ++i) {
+    int st = check_item(items[i]);
+    if (st) return st;
+  }
+  for (int f = 0; f < N_GROUPS; ++f)
     for (int i = 0; i < n_items; ++i) {
-      int st = check_item(items[i]);
-      if (st) return st;
-      if (family_of(items[i].kind) != f) continue;
+      if (group_of(items[i]) != f) continue;
       sorted[fill++] = items[i];
       ++count[f];
-      smem[f] = std::max(smem[f], item_smem(items[i], f, limit));
+      smem[f] = std::max(smem[f], item_smem(items[i], family_of(items[i].kind), limit));
     }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail("device");
@@ -176,17 +188,18 @@ extern "C" int32_t critmc_run_items(const critmc_item* items, int32_t n_items, v
   if (cudaMemcpyAsync(dev_items, sorted, (size_t)n_items * sizeof(critmc_item), cudaMemcpyHostToDevice, s) !=
       cudaSuccess)
     return cuda_fail("copy items");
-  const int families = (count[0] > 0) + (count[1] > 0) + (count[2] > 0);
+  int groups = 0;
+  for (int f = 0; f < N_GROUPS; ++f) groups += count[f] > 0;
   std::unique_lock<std::mutex> lock(g_family_mutex, std::defer_lock);
   FamilyStreams* fs = nullptr;
-  if (families > 1) {
+  if (groups > 1) {
     lock.lock();
     int st = family_streams(dev, fs);
     if (st) return st;
     if (cudaEventRecord(fs->fork, s) != cudaSuccess) return cuda_fail("event record");
   }
   int offset = 0;
-  for (int f = 0; f < 3; ++f) {
+  for (int f = 0; f < N_GROUPS; ++f) {
     if (!count[f]) continue;
     cudaStream_t fstream = s;
     if (fs) {
@@ -194,9 +207,10 @@ extern "C" int32_t critmc_run_items(const critmc_item* items, int32_t n_items, v
       if (cudaStreamWaitEvent(fstream, fs->fork, 0) != cudaSuccess) return cuda_fail("stream wait");
     }
     int st = CRITMC_OK;
-    if (f == 0) st = msc_items_launch(dev_items + offset, count[f], queues + 0, smem[f], fstream);
-    else if (f == 1) st = byte_items_launch(dev_items + offset, count[f], queues + 1, smem[f], fstream);
-    else st = on_items_launch(dev_items + offset, count[f], queues + 2, smem[f], fstream);
+    const critmc_item* first = sorted + offset;
+    if (f == 0) st = msc_items_launch(dev_items + offset, count[f], queues + f, smem[f], fstream);
+    else if (f == 1) st = byte_items_launch(dev_items + offset, count[f], queues + f, smem[f], fstream);
+    else st = on_items_launch(dev_items + offset, count[f], first->q_or_n, first->dim, queues + f, smem[f], fstream);
     if (st) return st;
     if (fs) {
       if (cudaEventRecord(fs->join[f], fstream) != cudaSuccess) return cuda_fail("event record");

@@ -13,6 +13,8 @@ constexpr int ITEM_THREADS = 512;
 // whose blocks pull item indices from *queue (zeroed by the caller).
 int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
 int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
-int on_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
+// O(n): all n items share n_comp and dim (one kernel per variant)
+int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem,
+                    cudaStream_t s);
 
 }  // namespace critmc

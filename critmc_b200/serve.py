@@ -51,12 +51,19 @@ _I8, _F8 = np.dtype(np.int64), np.dtype(np.float64)
 _ALIGN = 256
 GRID_MAX_MEAS = 4096  # measurements per grid-lane call (bounds its scratch)
 
-# Seconds per site-sweep of one thread block (item lanes) and per-sweep cost of
-# the multi-block lane, starting values for the tick planner; the planner
-# rescales them from the measured tick times.
-_COST = {"msc": 6.0e-11, "byte": 2.5e-10, "potts": 5.0e-10, "on2": 2.0e-9, "on3": 3.0e-9}
-_GRID_SWEEP_S = 5.0e-6
-_GRID_SITE_S = 1.0 / 1.5e12
+# Seconds per sweep of one chain, a + b * sites, by (lane, family): starting
+# values for the tick planner (B200 measurements of one chain alone); the
+# planner rescales them from the measured tick times.
+COSTS = {
+    ("items", "msc"): (2.7e-6, 5.0e-11),
+    ("items", "byte"): (2.0e-6, 5.0e-10),
+    ("items", "potts"): (1.9e-6, 1.0e-9),
+    ("items", "on2"): (5.0e-6, 5.5e-9),
+    ("items", "on3"): (6.0e-6, 8.0e-9),
+    ("grid", "msc"): (8.7e-6, 2.0e-13),
+    ("grid", "on2"): (1.0e-5, 2.0e-10),
+    ("grid", "on3"): (1.2e-5, 3.0e-10),
+}
 
 
 @dataclass
@@ -188,7 +195,7 @@ class _Job:
     dev_bytes: int
     admitted: float
     series: dict = field(default_factory=dict)
-    tables: np.ndarray | None = None
+    tables: object = None  # host tables of the multi-block lane
     launched: int = 0
     harvested: int = 0
 
@@ -214,7 +221,7 @@ class Server:
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
                  tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
                  arena_bytes: int = 64 << 20, keep_series: bool = True, keep_state: bool = False,
-                 grid_streams: int = 4, on_result=None):
+                 grid_streams: int = 16, on_result=None):
         self.device = require_cuda(device)
         free, _ = torch.cuda.mem_get_info(self.device)
         cap = max(0, free - reserve)
@@ -242,6 +249,7 @@ class Server:
         self.item_buffer = empty_bytes(_lib.lib().critmc_items_buffer_bytes(max_active), self.device)
         self.grid_scratch = [None] * grid_streams
         self.scale = 1.0
+        self.costs = dict(COSTS)
         self.ticks = 0
         self.gpu_seconds = 0.0
         self.updates_done = 0
@@ -329,9 +337,11 @@ class Server:
             t["running"] = torch.tensor([running["energy"]], dtype=torch.int64, device=dev)
             t["counts"] = torch.from_numpy(np.asarray(running["counts"], dtype=np.int64)).to(dev)
         else:
-            family, lane, kind, h = f"on{model.n}", "items", ITEM_ON, 0.0
+            family, lane, kind, h = f"on{model.n}", chain.lane.replace("block", "items"), ITEM_ON, 0.0
             fields = [("E", _F8, 1), ("M", _F8, model.n), ("stiff_c", _F8, dim), ("stiff_s", _F8, dim),
                       ("aux", _I8, 4)]
+            tables = (np.array([req.beta], dtype=np.float64),
+                      np.array([running.get("step", 1.0)], dtype=np.float64))
         if lane == "items":
             item = CritmcItem()
             item.spins = ptr(chain.words if family == "msc" else chain.spins)
@@ -360,19 +370,20 @@ class Server:
 
     # ---- ticks -----------------------------------------------------------
     def _sweep_seconds(self, job: _Job) -> float:
-        n = job.req.n_sites * job.sweeps_per_meas
-        if job.lane == "grid":
-            return job.sweeps_per_meas * _GRID_SWEEP_S + n * _GRID_SITE_S
-        return n * _COST[job.family]
+        a, b = self.costs[(job.lane, job.family)]
+        return job.sweeps_per_meas * (a + b * job.req.n_sites)
 
     def _plan(self):
         jobs = [j for j in self.active if j.launched < j.req.sweeps]
         if not jobs:
             return [], 0.0
         plan = []
+        n_grid = sum(1 for j in jobs if j.lane == "grid")
+        share = max(1, -(-n_grid // len(self.grid_pool)))  # grid jobs per library stream
         for j in jobs:
             per = self._sweep_seconds(j) * self.scale
-            n = max(1, int(self.tick_s / per))
+            target = self.tick_s / share if j.lane == "grid" else self.tick_s
+            n = max(1, int(target / per))
             n = min(n, j.req.sweeps - j.launched)
             if j.lane == "grid":
                 n = min(n, GRID_MAX_MEAS)
@@ -384,7 +395,13 @@ class Server:
                 p[1] = max(1, int(p[1] * f * 0.98))
             while sum(_round_up(j.meas_bytes * n) for j, n in plan) > self.arena_bytes and len(plan) > 1:
                 plan.pop()
-        predicted = max(self._sweep_seconds(j) * self.scale * n for j, n in plan)
+        item_t = [self._sweep_seconds(j) * self.scale * n for j, n in plan if j.lane == "items"]
+        grid_t = sorted((self._sweep_seconds(j) * self.scale * n for j, n in plan if j.lane == "grid"),
+                        reverse=True)
+        loads = [0.0] * len(self.grid_pool)
+        for t in grid_t:  # the launch assigns grid jobs longest first to the least loaded stream
+            loads[loads.index(min(loads))] += t
+        predicted = max(item_t + loads)
         return plan, predicted
 
     def _launch(self, plan, predicted) -> _Tick:
@@ -427,19 +444,33 @@ class Server:
         if grid:
             fork = torch.cuda.Event()
             fork.record(s)
-            for k, (j, n, ptrs) in enumerate(grid):
-                gs = self.grid_pool[k % len(self.grid_pool)]
-                gs.wait_event(fork)
-                scratch = self._grid_scratch(k % len(self.grid_pool))
+            used = set()
+            loads = [0.0] * len(self.grid_pool)
+            grid.sort(key=lambda g: -self._sweep_seconds(g[0]) * g[1])
+            for j, n, ptrs in grid:
+                k = loads.index(min(loads))
+                loads[k] += self._sweep_seconds(j) * n
+                gs = self.grid_pool[k]
+                if k not in used:
+                    gs.wait_event(fork)
+                    used.add(k)
+                scratch = self._grid_scratch(k)
                 c = j.chain
                 lx, ly, lz = c.dims
-                _lib.call("critmc_ising_msc_run", ptr(c.words), len(c.shape), lx, ly, lz, 1, c.key.ctypes.data,
-                          j.tables.ctypes.data, 1, c.sweep, j.sched.ctypes.data, len(j.sched), n,
-                          ptr(j.tensors["running"]), ptrs[0], ptrs[1], ptrs[2], ptr(scratch), 0, c.k_inline,
-                          gs.cuda_stream)
-            for gs in self.grid_pool[:len(grid)]:
+                if j.family == "msc":
+                    _lib.call("critmc_ising_msc_run", ptr(c.words), len(c.shape), lx, ly, lz, 1,
+                              c.key.ctypes.data, j.tables.ctypes.data, 1, c.sweep, j.sched.ctypes.data,
+                              len(j.sched), n, ptr(j.tensors["running"]), ptrs[0], ptrs[1], ptrs[2],
+                              ptr(scratch), 0, c.k_inline, gs.cuda_stream)
+                else:
+                    betas, steps = j.tables
+                    _lib.call("critmc_on_run_grid", ptr(c.spins), len(c.shape), lx, ly, lz, c.n, 1,
+                              c.key.ctypes.data, betas.ctypes.data, steps.ctypes.data, 1, c.sweep,
+                              j.sched.ctypes.data, len(j.sched), n, ptrs[0], ptrs[1], ptrs[2], ptrs[3],
+                              ptrs[4], ptr(scratch), c.blocks_per_chain, gs.cuda_stream)
+            for k in used:
                 join = torch.cuda.Event()
-                join.record(gs)
+                join.record(self.grid_pool[k])
                 s.wait_event(join)
         end.record(s)
         with torch.cuda.stream(s):
@@ -453,7 +484,9 @@ class Server:
 
     def _grid_scratch(self, k: int) -> torch.Tensor:
         if self.grid_scratch[k] is None:
-            need = _lib.lib().critmc_ising_msc_scratch_bytes(1, GRID_MAX_MEAS)
+            lib = _lib.lib()
+            need = max(lib.critmc_ising_msc_scratch_bytes(1, GRID_MAX_MEAS),
+                       lib.critmc_on_grid_scratch_bytes(1, GRID_MAX_MEAS, 3, 3))
             self.grid_scratch[k] = empty_bytes(need, self.device)
         return self.grid_scratch[k]
 

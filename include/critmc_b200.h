@@ -154,7 +154,9 @@ int32_t critmc_potts_tables(int32_t z, double beta, uint64_t* boltz_thr, uint64_
  * 0x03 | colour << 16, k).
  * Schedule rows: metropolis (0), heatbath (2), overrelax (5).
  * After each schedule application every spin is renormalised and the
- * observables are accumulated in FP64 in a fixed order (deterministic):
+ * observables are summed exactly: each site's FP64 term is rounded to a
+ * multiple of 2^-36 and the terms are added as int64 (independent of the
+ * thread layout), then returned as doubles:
  * e_out[n_chains][n_meas] = -sum_<ij> S_i.S_j, m_out[..][n],
  * stiff_c_out / stiff_s_out[..][dim] (per-axis sums of S_i^0 S_j^0 + S_i^1 S_j^1
  * and S_i^0 S_j^1 - S_i^1 S_j^0 over bonds i -> i + e_a), aux_out[..][4]
@@ -168,6 +170,21 @@ int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t
                       const int64_t* schedule, int32_t n_rows, int32_t n_meas, double* e_out,
                       double* m_out, double* stiff_c_out, double* stiff_s_out, int64_t* aux_out,
                       void* stream);
+
+/* The same run with many thread blocks per chain (one launch per colour of a
+ * sweep, a normalisation and a measurement launch per measurement, replayed
+ * as CUDA graphs): lower latency for large lattices, results identical to
+ * critmc_on_run (spins and sums bit for bit).  scratch: device memory of
+ * critmc_on_grid_scratch_bytes(n_chains, n_meas, n, dim) bytes.
+ * blocks_per_chain: blocks of 256 threads per chain and colour, 0 = auto.
+ * No counterpart in critmc (one process per chain).                        */
+int64_t critmc_on_grid_scratch_bytes(int32_t n_chains, int32_t n_meas, int32_t n, int32_t dim);
+int32_t critmc_on_run_grid(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t n,
+                           int32_t n_chains, const uint32_t* keys, const double* betas,
+                           const double* steps, int32_t n_groups, uint32_t sweep0,
+                           const int64_t* schedule, int32_t n_rows, int32_t n_meas, double* e_out,
+                           double* m_out, double* stiff_c_out, double* stiff_s_out, int64_t* aux_out,
+                           void* scratch, int32_t blocks_per_chain, void* stream);
 
 /* ---- Edwards-Anderson +-J spin glass with parallel tempering ---------------
  * A sample holds two independent replica sets of m <= 32 configurations on a

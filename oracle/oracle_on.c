@@ -19,8 +19,8 @@
  * The elementary functions are those of critmc_b200/csrc/fpmath.h (plain IEEE
  * operations, accuracy checked against libm in tests/test_fpmath_cpu.py); with
  * floating-point contraction off on both sides the spins follow the GPU bit for
- * bit.  The FP64 sums are accumulated in site order (the GPU uses a block
- * reduction), so the observables agree to rounding.
+ * bit.  Observables are sums of per-site FP64 terms rounded to 2^-36 and
+ * added as int64, as on the GPU, so they agree exactly.
  */
 #include <math.h>
 #include <stdint.h>
@@ -31,6 +31,10 @@
 #include "oracle.h"
 
 #define PI_F 3.14159265358979323846f
+
+/* observables: per-site FP64 terms rounded to multiples of 2^-36, summed as int64 */
+#define UNFIX36 (1.0 / 68719476736.0)
+static int64_t fix36(double x) { return (int64_t)llrint(x * 68719476736.0); }
 
 static float u01(uint32_t w) { return (float)(w >> 8) * (1.0f / 16777216.0f); }
 static float u01o(uint32_t w) { return (float)((w >> 8) + 1u) * (1.0f / 16777216.0f); }
@@ -61,9 +65,9 @@ static void nbrs(const OGeo* g, int x, int y, int z, int* nb) {
   }
 }
 
-static float von_mises(float kappa, const uint32_t r0[4], uint32_t slot, uint32_t sweep,
-                       uint32_t col, const uint32_t key[2]) {
-  if (kappa < 1e-8f) return PI_F * (2.0f * u01(r0[0]) - 1.0f);
+/* cos(theta) of a von Mises angle to the field, kappa >= 1e-8 (Best & Fisher 1979) */
+static float von_mises_cos(float kappa, const uint32_t r0[4], uint32_t slot, uint32_t sweep,
+                           uint32_t col, const uint32_t key[2]) {
   const float root = sqrtf(1.0f + 4.0f * kappa * kappa);
   const float tau = 1.0f + root;
   const float rho = 2.0f * kappa * tau / ((root + 1.0f) * (tau + sqrtf(2.0f * tau)));
@@ -83,8 +87,7 @@ static float von_mises(float kappa, const uint32_t r0[4], uint32_t slot, uint32_
     const float u2 = u01(b);
     if (c * (2.0f - c) - u2 > 0.0f || cm_logf(c / u2) + 1.0f - c >= 0.0f) break;
   }
-  const float theta = cm_acosf(fminf(1.0f, fmaxf(-1.0f, f)));
-  return u01(r0[2]) < 0.5f ? theta : -theta;
+  return fminf(1.0f, fmaxf(-1.0f, f));
 }
 
 static void sweep_colour(float* s, const OGeo* g, int n, int code, int col, uint32_t sweep,
@@ -127,10 +130,21 @@ static void sweep_colour(float* s, const OGeo* g, int n, int code, int col, uint
           hn = sqrtf(hn);
           const float kappa = beta * hn;
           if (n == 2) {
-            const float phi0 = hn > 0.0f ? cm_atan2f(h[1], h[0]) : 0.0f;
-            const float phi = phi0 + von_mises(kappa, r0, slot, sweep, (uint32_t)col, key);
-            out[0] = cm_cosf(phi);
-            out[1] = cm_sinf(phi);
+            /* the field direction rotated by the von Mises angle theta (on.py:219-223
+               draws atan2(h) + theta; the same spin without forming the angle) */
+            if (kappa < 1e-8f) {
+              const float phi = PI_F * (2.0f * u01(r0[0]) - 1.0f);
+              out[0] = cm_cosf(phi);
+              out[1] = cm_sinf(phi);
+            } else {
+              const float ct = von_mises_cos(kappa, r0, slot, sweep, (uint32_t)col, key);
+              float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+              if (!(u01(r0[2]) < 0.5f)) st = -st;
+              const float inv = 1.0f / hn;
+              const float hx = h[0] * inv, hy = h[1] * inv;
+              out[0] = ct * hx - st * hy;
+              out[1] = ct * hy + st * hx;
+            }
           } else {
             if (hn == 0.0f) {
               float g0, g1, g2, g3;
@@ -223,28 +237,29 @@ int oracle_on_run(float* s, int dim, int lx, int ly, int lz, int n, const uint32
       nrm = sqrtf(nrm);
       for (int k = 0; k < n; ++k) s[(size_t)i * n + k] /= nrm;
     }
-    double e = 0.0, m[3] = {0, 0, 0}, sc[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
+    /* each site's FP64 term rounded to 2^-36 and summed as int64 (exact) */
+    int64_t e = 0, m[3] = {0, 0, 0}, sc[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
     for (int z = 0; z < g.lz; ++z)
       for (int y = 0; y < g.ly; ++y)
         for (int x = 0; x < g.lx; ++x) {
           const int i = x + g.lx * (y + g.ly * z);
           nbrs(&g, x, y, z, nb);
           const float* si = s + (size_t)i * n;
-          for (int k = 0; k < n; ++k) m[k] += si[k];
+          for (int k = 0; k < n; ++k) m[k] += fix36((double)si[k]);
           for (int a = 0; a < dim; ++a) {
             const float* sj = s + (size_t)nb[2 * a] * n;
             double dot = 0.0;
             for (int k = 0; k < n; ++k) dot += (double)si[k] * (double)sj[k];
-            e -= dot;
-            sc[a] += (double)si[0] * sj[0] + (double)si[1] * sj[1];
-            ss[a] += (double)si[0] * sj[1] - (double)si[1] * sj[0];
+            e -= fix36(dot);
+            sc[a] += fix36((double)si[0] * sj[0] + (double)si[1] * sj[1]);
+            ss[a] += fix36((double)si[0] * sj[1] - (double)si[1] * sj[0]);
           }
         }
-    e_out[meas] = e;
-    for (int k = 0; k < n; ++k) m_out[(size_t)meas * n + k] = m[k];
+    e_out[meas] = (double)e * UNFIX36;
+    for (int k = 0; k < n; ++k) m_out[(size_t)meas * n + k] = (double)m[k] * UNFIX36;
     for (int a = 0; a < dim; ++a) {
-      sc_out[(size_t)meas * dim + a] = sc[a];
-      ss_out[(size_t)meas * dim + a] = ss[a];
+      sc_out[(size_t)meas * dim + a] = (double)sc[a] * UNFIX36;
+      ss_out[(size_t)meas * dim + a] = (double)ss[a] * UNFIX36;
     }
     aux_out[4 * meas] = acc;
     aux_out[4 * meas + 1] = aux_out[4 * meas + 2] = aux_out[4 * meas + 3] = 0;

@@ -31,6 +31,10 @@ from pathlib import Path
 
 import numpy as np
 
+# the server runs many lanes on their own streams: let them map to separate
+# hardware queues (a process setting read when CUDA starts)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -216,7 +220,7 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0) -> dict:
             "updates_per_ns": upd[0] / wall / 1e9, "gpu_busy_frac": st["gpu_seconds"] / wall,
             "ticks": st["ticks"], "peak_hbm_bytes": st["peak_hbm_bytes"], "max_queued": st["max_queued"],
             "workload": "Poisson arrivals; Ising L 16..1024 / Potts q=10 L 16..128 / XY L 32..128, "
-                        "sweeps log-uniform 1e3..1e5 (metropolis, metropolis, heatbath)"}
+                        "sweeps log-uniform 1e3..1e5, checkerboard Metropolis (critmc's default update)"}
 
 
 def main() -> None:

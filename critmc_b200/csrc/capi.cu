@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "host_common.h"
 
@@ -19,6 +20,45 @@ int cuda_fail(const char* what) {
   const cudaError_t e = cudaGetLastError();
   std::snprintf(g_error, sizeof(g_error), "%s: %s", what, cudaGetErrorString(e));
   return CRITMC_ERR_CUDA;
+}
+
+namespace {
+
+struct GraphEntry {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec;
+  uint64_t used;
+};
+std::mutex g_graph_mu;
+std::vector<GraphEntry> g_graphs;
+uint64_t g_graph_clock = 0;
+size_t g_graph_capacity = 64;
+
+}  // namespace
+
+cudaGraphExec_t graph_cache_find(const GraphKey& key) {
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  for (GraphEntry& e : g_graphs)
+    if (e.key == key.bytes) {
+      e.used = ++g_graph_clock;
+      return e.exec;
+    }
+  return nullptr;
+}
+
+void graph_cache_insert(const GraphKey& key, cudaGraphExec_t exec) {
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  while (!g_graphs.empty() && g_graphs.size() >= g_graph_capacity) {
+    auto old = std::min_element(g_graphs.begin(), g_graphs.end(),
+                                [](const GraphEntry& a, const GraphEntry& b) { return a.used < b.used; });
+    cudaGraphExecDestroy(old->exec);
+    g_graphs.erase(old);
+  }
+  if (g_graph_capacity == 0) {
+    cudaGraphExecDestroy(exec);
+    return;
+  }
+  g_graphs.push_back(GraphEntry{key.bytes, exec, ++g_graph_clock});
 }
 
 int CaptureStream::begin(void* stream) {
@@ -56,6 +96,22 @@ int CaptureStream::finish() {
 using namespace critmc;
 
 extern "C" int32_t critmc_version(void) { return 100; }
+
+extern "C" int32_t critmc_graph_cache_set_capacity(int32_t entries) {
+  if (entries < 0) return CRITMC_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  g_graph_capacity = (size_t)entries;
+  while (g_graphs.size() > g_graph_capacity) {
+    cudaGraphExecDestroy(g_graphs.front().exec);
+    g_graphs.erase(g_graphs.begin());
+  }
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_graph_cache_size(void) {
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  return (int32_t)g_graphs.size();
+}
 
 extern "C" int32_t critmc_last_error(char* buf, int32_t size) {
   if (!buf || size <= 0) return CRITMC_ERR_INVALID;

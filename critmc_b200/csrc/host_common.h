@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "critmc_b200.h"
 
@@ -30,5 +31,32 @@ struct CaptureStream {
   int begin(void* stream);
   int finish();
 };
+
+// Instantiated CUDA graphs of repeated calls, keyed by the exact bytes of
+// everything their capture depends on (kernel parameters, launch shapes,
+// schedule).  A caller that advances the same chains slice after slice (a
+// server's ticks, Simulation.run chunks) replays its graph instead of
+// capturing and instantiating it again.  Least recently used entries are
+// destroyed beyond the capacity (a graph still in flight is freed by CUDA
+// when it completes).
+class GraphKey {
+ public:
+  template <typename T>
+  GraphKey& add(const T& v) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+    bytes.insert(bytes.end(), p, p + sizeof(T));
+    return *this;
+  }
+  GraphKey& add_bytes(const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    bytes.insert(bytes.end(), c, c + n);
+    return *this;
+  }
+  std::vector<unsigned char> bytes;
+};
+
+cudaGraphExec_t graph_cache_find(const GraphKey& key);
+// takes ownership of exec
+void graph_cache_insert(const GraphKey& key, cudaGraphExec_t exec);
 
 }  // namespace critmc

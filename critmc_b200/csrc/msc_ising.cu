@@ -475,20 +475,34 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
     msc_cursor_set<<<1, 1, 0, s>>>(cursor, sweep0, 0);
     const int n_graph = n_meas / G;
     if (n_graph > 1) {
-      cudaGraph_t graph;
-      cudaGraphExec_t exec;
-      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return cuda_fail("capture");
-      for (int m = 0; m < G; ++m) launch_meas((uint32_t)(m * sweeps_per_meas), (uint32_t)m, cursor);
-      msc_cursor_bump<<<1, 1, 0, s>>>(cursor, (uint32_t)(G * sweeps_per_meas), (uint32_t)G);
-      if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return cuda_fail("end capture");
-      if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+      // the graph depends on the parameters below only: reuse it across calls
+      int dev = 0;
+      cudaGetDevice(&dev);
+      GraphKey key;
+      key.add(0x4d534347u).add(dev).add(G).add(n_rows).add(rule).add(kg);
+      key.add_bytes(schedule, sizeof(int64_t) * 2 * n_rows).add_bytes(keys, sizeof(uint32_t) * 2 * n_chains);
+      for (int slot = 0; slot < 2; ++slot) {
+        MscParams& q = P[slot];
+        q.cursor = cursor;
+        q.sweep = q.meas = 0;
+        q.col = q.chain0 = 0;
+        std::memset(q.keys, 0, sizeof(q.keys));
+        key.add(q);
+      }
+      cudaGraphExec_t exec = graph_cache_find(key);
+      if (!exec) {
+        cudaGraph_t graph;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+          return cuda_fail("capture");
+        for (int m = 0; m < G; ++m) launch_meas((uint32_t)(m * sweeps_per_meas), (uint32_t)m, cursor);
+        msc_cursor_bump<<<1, 1, 0, s>>>(cursor, (uint32_t)(G * sweeps_per_meas), (uint32_t)G);
+        if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return cuda_fail("end capture");
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
-        return cuda_fail("instantiate");
+        if (ie != cudaSuccess) return cuda_fail("instantiate");
+        graph_cache_insert(key, exec);
       }
       for (int i = 0; i < n_graph; ++i) cudaGraphLaunch(exec, s);
-      cudaGraphExecDestroy(exec);
-      cudaGraphDestroy(graph);
     }
     const int done = n_graph > 1 ? n_graph * G : 0;
     for (int m = done; m < n_meas; ++m)

@@ -443,10 +443,10 @@ constexpr int ON_GPCHAINS = 256;
 
 struct OnGridParams {
   float* spins;
-  unsigned long long* acc;  // [n_chains][n_meas][NV]
+  unsigned long long* acc;  // [n_meas][n_chains][NV]
   const uint32_t* cursor;   // device (sweep base, meas base) for graph replay, or null
   ByteGeom g;
-  int n_meas, chain0, chains_per_group, nv;
+  int n_chains, chain0, chains_per_group, nv;
   int code, col;
   uint32_t sweep, meas;     // absolute, or relative to the cursor
   float beta[ON_MAX_GROUPS];
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(ON_GRID_THREADS) on_colour_kernel(const __grid
   if (P.code == CRITMC_METROPOLIS) {
     nacc = warp_sum(nacc);
     if ((threadIdx.x & 31) == 0 && nacc)
-      atomicAdd(P.acc + ((size_t)chain * P.n_meas + meas) * P.nv + (P.nv - 1), as_ull(nacc));
+      atomicAdd(P.acc + ((size_t)meas * P.n_chains + chain) * P.nv + (P.nv - 1), as_ull(nacc));
   }
 }
 
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(ON_GRID_THREADS) on_measure_kernel(const __gri
   for (int q = 0; q < NV; ++q) v[q] = 0;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_sites; j += gridDim.x * blockDim.x)
     on_measure_site<N, Z>(lat, P.g, j, v);
-  unsigned long long* acc = P.acc + ((size_t)chain * P.n_meas + meas) * NV;
+  unsigned long long* acc = P.acc + ((size_t)meas * P.n_chains + chain) * NV;
 #pragma unroll
   for (int q = 0; q < NV - 1; ++q) {
     const long long w = warp_sum(v[q]);
@@ -509,9 +509,9 @@ __global__ void on_grid_finalize(const unsigned long long* acc, int n_chains, in
   const size_t total = (size_t)n_chains * n_meas * NV;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const int q = (int)(i % NV);
-    const size_t cm = i / NV;  // chain * n_meas + meas
-    const size_t chain = cm / n_meas;
-    const int meas = (int)(cm % n_meas);
+    const size_t mc = i / NV;  // meas * n_chains + chain
+    const size_t chain = mc % n_chains;
+    const int meas = (int)(mc / n_chains);
     on_write_sum<N, Z>(e_out + chain * n_meas, m_out + chain * n_meas * N, sc_out + chain * n_meas * DIM,
                        ss_out + chain * n_meas * DIM, aux_out + chain * n_meas * 4, meas, q,
                        (long long)acc[i]);
@@ -540,6 +540,7 @@ static int on_grid_launches(OnGridParams& P, const int* codes, const int* reps, 
   for (int c0 = 0; c0 < n_chains; c0 += ON_GPCHAINS) {
     const int nc = std::min(ON_GPCHAINS, n_chains - c0);
     P.chain0 = c0;
+    std::memset(P.keys, 0, sizeof(P.keys));
     std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
     const dim3 grid_c((unsigned)blocks, (unsigned)nc);
     const uint32_t site_blocks = (uint32_t)std::min<size_t>(2 * (size_t)blocks, (2 * (size_t)P.g.slots + ON_GRID_THREADS - 1) / ON_GRID_THREADS);
@@ -562,26 +563,35 @@ static int on_grid_launches(OnGridParams& P, const int* codes, const int* reps, 
       on_normalize_kernel<N><<<grid_s, ON_GRID_THREADS, 0, s>>>(P);
       on_measure_kernel<N, Z><<<grid_s, ON_GRID_THREADS, 0, s>>>(P);
     };
-    // a graph of G measurements replayed with a device cursor, the rest launched directly
+    // a graph of G measurements replayed with a device cursor (cached across
+    // calls with the same parameters), the rest launched directly
     const long long launches = 2 * per_meas + 2;
     const int G = (int)std::max<long long>(1, std::min<long long>(n_meas, 512 / launches));
     const int n_graph = n_meas / G;
     int done = 0;
     if (n_graph > 1) {
       on_cursor_set<<<1, 1, 0, s>>>(cursor, sweep0, 0);
-      cudaGraph_t graph;
-      cudaGraphExec_t exec;
-      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_fail("capture");
-      for (int m = 0; m < G; ++m) launch_meas((uint32_t)(m * per_meas), (uint32_t)m, cursor);
-      on_cursor_bump<<<1, 1, 0, s>>>(cursor, (uint32_t)(G * per_meas), (uint32_t)G);
-      if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return cuda_fail("end capture");
-      if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+      P.cursor = cursor;
+      P.sweep = P.meas = 0;
+      P.code = P.col = 0;
+      int dev = 0;
+      cudaGetDevice(&dev);
+      GraphKey key;
+      key.add(0x4f4e4752u).add(dev).add(N).add(Z).add(G).add(n_rows).add(grid_c).add(grid_s).add(P);
+      key.add_bytes(codes, sizeof(int) * n_rows).add_bytes(reps, sizeof(int) * n_rows);
+      cudaGraphExec_t exec = graph_cache_find(key);
+      if (!exec) {
+        cudaGraph_t graph;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_fail("capture");
+        for (int m = 0; m < G; ++m) launch_meas((uint32_t)(m * per_meas), (uint32_t)m, cursor);
+        on_cursor_bump<<<1, 1, 0, s>>>(cursor, (uint32_t)(G * per_meas), (uint32_t)G);
+        if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return cuda_fail("end capture");
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
-        return cuda_fail("instantiate");
+        if (ie != cudaSuccess) return cuda_fail("instantiate");
+        graph_cache_insert(key, exec);
       }
       for (int i = 0; i < n_graph; ++i) cudaGraphLaunch(exec, s);
-      cudaGraphExecDestroy(exec);
-      cudaGraphDestroy(graph);
       done = n_graph * G;
     }
     for (int m = done; m < n_meas; ++m)
@@ -726,7 +736,7 @@ extern "C" int32_t critmc_on_run_grid(float* spins, int32_t dim, int32_t lx, int
     P.step[gi] = (float)steps[gi];
   }
   P.spins = spins;
-  P.n_meas = n_meas;
+  P.n_chains = n_chains;
   P.chains_per_group = n_chains / n_groups;
   P.nv = 2 + n + 2 * dim;
   int blocks = blocks_per_chain;

@@ -45,7 +45,8 @@ from .sim import parse_updates
 
 __all__ = ["Request", "Result", "Server", "open_chain", "mixed_workload", "DEFAULT_UPDATES"]
 
-DEFAULT_UPDATES = {"ising": "metropolis", "potts": "metropolis", "xy": "heatbath", "heisenberg": "heatbath"}
+# critmc's Simulation default (src/critmc/sim.py:157) for every model
+DEFAULT_UPDATES = {"ising": "metropolis", "potts": "metropolis", "xy": "metropolis", "heisenberg": "metropolis"}
 
 _I8, _F8 = np.dtype(np.int64), np.dtype(np.float64)
 _ALIGN = 256
@@ -58,8 +59,8 @@ COSTS = {
     ("items", "msc"): (2.7e-6, 5.0e-11),
     ("items", "byte"): (2.0e-6, 5.0e-10),
     ("items", "potts"): (1.9e-6, 1.0e-9),
-    ("items", "on2"): (5.0e-6, 5.5e-9),
-    ("items", "on3"): (6.0e-6, 8.0e-9),
+    ("items", "on2"): (3.0e-6, 2.5e-9),
+    ("items", "on3"): (4.0e-6, 4.0e-9),
     ("grid", "msc"): (8.7e-6, 2.0e-13),
     ("grid", "on2"): (1.0e-5, 2.0e-10),
     ("grid", "on3"): (1.2e-5, 3.0e-10),
@@ -198,6 +199,8 @@ class _Job:
     tables: object = None  # host tables of the multi-block lane
     launched: int = 0
     harvested: int = 0
+    group: str = ""
+    home: object = None  # the lane that advances it
 
     @property
     def meas_bytes(self) -> int:
@@ -206,13 +209,68 @@ class _Job:
 
 @dataclass
 class _Tick:
-    slot: int
+    lane: "_Lane"
     entries: list  # (job, n_meas, offset)
-    used: int
+    offset: int  # arena segment
+    size: int
     predicted: float
     start: torch.cuda.Event
     end: torch.cuda.Event
     done: torch.cuda.Event
+    seq: int = 0
+
+
+class _Lane:
+    """Jobs advanced by one launch sequence per tick on one stream.
+
+    An item lane holds the requests of one persistent-kernel group (their
+    ticks are one ``critmc_run_items`` call); a grid lane holds one request
+    on the multi-block kernels.  Lanes tick independently, two ticks in
+    flight each, so a lane of short sweeps never waits for a lane of long ones.
+    """
+
+    def __init__(self, kind: str, family: str, stream: torch.cuda.Stream):
+        self.kind, self.family, self.stream = kind, family, stream
+        self.jobs: list[_Job] = []
+        self.inflight: deque[_Tick] = deque()
+        self.scale = 1.0
+        self.staging = [None, None]
+        self.n_ticks = 0
+        self.item_buffer = None
+
+
+class _Arena:
+    """First-fit allocator of tick output segments in a device/pinned-host pair."""
+
+    def __init__(self, size: int, device):
+        self.size = size
+        self.dev = empty_bytes(size, device)
+        self.host = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+        self.host_np = self.host.numpy()
+        self.free = [(0, size)]
+
+    def alloc(self, n: int) -> int | None:
+        n = _round_up(max(n, 1))
+        for i, (o, sz) in enumerate(self.free):
+            if sz >= n:
+                if sz == n:
+                    self.free.pop(i)
+                else:
+                    self.free[i] = (o + n, sz - n)
+                return o
+        return None
+
+    def release(self, o: int, n: int) -> None:
+        n = _round_up(max(n, 1))
+        self.free.append((o, n))
+        self.free.sort()
+        merged = []
+        for a, sz in self.free:
+            if merged and merged[-1][0] + merged[-1][1] == a:
+                merged[-1] = (merged[-1][0], merged[-1][1] + sz)
+            else:
+                merged.append((a, sz))
+        self.free = merged
 
 
 class Server:
@@ -220,15 +278,18 @@ class Server:
 
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
                  tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
-                 arena_bytes: int = 64 << 20, keep_series: bool = True, keep_state: bool = False,
-                 grid_streams: int = 16, on_result=None):
+                 max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
+                 keep_state: bool = False, grid_streams: int = 32, on_result=None):
         self.device = require_cuda(device)
         free, _ = torch.cuda.mem_get_info(self.device)
-        cap = max(0, free - reserve)
+        cap = max(0, free - reserve - 2 * arena_bytes)
         self.budget = min(cap, int(hbm_budget)) if hbm_budget is not None else cap
         self.tick_s = tick_ms * 1e-3
         self.max_active = max_active
         self.grid_min_sites = grid_min_sites
+        # the multi-block lanes are launch-bound: they buy latency, the item
+        # kernels throughput, so at most this many requests use them at once
+        self.max_grid_lanes = max_grid_lanes
         self.keep_series, self.keep_state = keep_series, keep_state
         self.on_result = on_result
         self.in_use = 0
@@ -236,19 +297,15 @@ class Server:
         self.queue: deque[Request] = deque()
         self.active: list[_Job] = []
         self.results: list[Result] = []
-        self.inflight: deque[_Tick] = deque()
         self.models: dict = {}
-        self.stream = torch.cuda.Stream(self.device)
         self.admit_stream = torch.cuda.Stream(self.device)
+        self.admit_event: torch.cuda.Event | None = None
+        self.item_lanes: dict[str, _Lane] = {}
         self.grid_pool = [torch.cuda.Stream(self.device) for _ in range(grid_streams)]
-        self.arena_bytes = int(arena_bytes)
-        self.arena = [empty_bytes(self.arena_bytes, self.device) for _ in range(2)]
-        self.host = [torch.empty(self.arena_bytes, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
-        self.staging = [None, None]
-        # sized once: a buffer replaced while a tick still reads it would be recycled too early
-        self.item_buffer = empty_bytes(_lib.lib().critmc_items_buffer_bytes(max_active), self.device)
-        self.grid_scratch = [None] * grid_streams
-        self.scale = 1.0
+        self.grid_lanes: list[_Lane] = []
+        self._next_grid = 0
+        self.arena = _Arena(int(arena_bytes), self.device)
+        self.grid_scratch: dict[int, torch.Tensor] = {}
         self.costs = dict(COSTS)
         self.ticks = 0
         self.gpu_seconds = 0.0
@@ -284,8 +341,15 @@ class Server:
             lat = 4 * n * (2 if req.model == "xy" else 3)
         return lat + 4096
 
+    def _grid_free(self) -> bool:
+        return sum(1 for lane in self.grid_lanes if lane.jobs) < self.max_grid_lanes
+
+    def _lanes(self):
+        yield from self.item_lanes.values()
+        yield from self.grid_lanes
+
     # ---- admission -------------------------------------------------------
-    def _admit(self) -> None:
+    def _admit(self) -> bool:
         admitted = False
         now = self.now()
         while self.queue and self.queue[0].arrival <= now and len(self.active) < self.max_active:
@@ -301,6 +365,7 @@ class Server:
             self.in_use += need
             self.peak_in_use = max(self.peak_in_use, self.in_use)
             self.active.append(job)
+            self._assign(job)
             admitted = True
         waiting = 0
         for r in self.queue:
@@ -309,9 +374,23 @@ class Server:
             waiting += 1
         self.max_queued = max(self.max_queued, waiting)
         if admitted:
-            ev = torch.cuda.Event()
-            ev.record(self.admit_stream)
-            self.stream.wait_event(ev)
+            self.admit_event = torch.cuda.Event()
+            self.admit_event.record(self.admit_stream)
+        return admitted
+
+    def _assign(self, job: _Job) -> None:
+        if job.lane == "items":
+            key = job.group
+            lane = self.item_lanes.get(key)
+            if lane is None:
+                lane = self.item_lanes[key] = _Lane("items", job.family, torch.cuda.Stream(self.device))
+        else:
+            stream = self.grid_pool[self._next_grid % len(self.grid_pool)]
+            self._next_grid += 1
+            lane = _Lane("grid", job.family, stream)
+            self.grid_lanes.append(lane)
+        lane.jobs.append(job)
+        job.home = lane
 
     def _open(self, req: Request, need: int) -> _Job:
         model, chain, running = open_chain(req, self.device, self.models)
@@ -324,20 +403,24 @@ class Server:
         if isinstance(model, Ising):
             msc = isinstance(chain, _IsingMscChain)
             family = "msc" if msc else "byte"
+            group = family
             fields = [("Eb", _I8, 1), ("M", _I8, 1), ("aux", _I8, 4)]
             t["running"] = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
-            lane = "grid" if msc and req.n_sites >= self.grid_min_sites else "items"
+            lane = "grid" if msc and req.n_sites >= self.grid_min_sites and self._grid_free() else "items"
             kind = ITEM_MSC_ISING if msc else ITEM_BYTE_ISING
             h = model.h
             if lane == "grid":
                 tables = np.ascontiguousarray(model.tables(req.beta)[0])
         elif isinstance(model, Potts):
-            family, lane, kind, h = "potts", "items", ITEM_POTTS, 0.0
+            family, group, lane, kind, h = "potts", "byte", "items", ITEM_POTTS, 0.0
             fields = [("E", _I8, 1), ("counts", _I8, model.q), ("aux", _I8, 4)]
             t["running"] = torch.tensor([running["energy"]], dtype=torch.int64, device=dev)
             t["counts"] = torch.from_numpy(np.asarray(running["counts"], dtype=np.int64)).to(dev)
         else:
+            if chain.lane == "grid" and not self._grid_free():
+                chain.lane = "block"  # same results on either lane
             family, lane, kind, h = f"on{model.n}", chain.lane.replace("block", "items"), ITEM_ON, 0.0
+            group = f"on{model.n}d{dim}"
             fields = [("E", _F8, 1), ("M", _F8, model.n), ("stiff_c", _F8, dim), ("stiff_s", _F8, dim),
                       ("aux", _I8, 4)]
             tables = (np.array([req.beta], dtype=np.float64),
@@ -361,6 +444,9 @@ class Server:
                       float(running.get("step", 1.0)))
         job = _Job(req, model, chain, running, lane, family, sched, int(sched[:, 1].sum()), fields, item, t,
                    need, self.now(), tables=tables)
+        # item lanes by kernel group and lattice size class (a call's blocks get the largest
+        # lattice's shared memory, so small lattices do not share a lane with large ones)
+        job.group = f"{group}-{(need - 4096).bit_length()}"
         if self.keep_series:
             job.series = {name: np.empty((req.sweeps, w) if w > 1 else req.sweeps, dtype=dt)
                           for name, dt, w in fields}
@@ -373,53 +459,48 @@ class Server:
         a, b = self.costs[(job.lane, job.family)]
         return job.sweeps_per_meas * (a + b * job.req.n_sites)
 
-    def _plan(self):
-        jobs = [j for j in self.active if j.launched < j.req.sweeps]
-        if not jobs:
-            return [], 0.0
+    def _plan(self, lane: _Lane):
         plan = []
-        n_grid = sum(1 for j in jobs if j.lane == "grid")
-        share = max(1, -(-n_grid // len(self.grid_pool)))  # grid jobs per library stream
-        for j in jobs:
-            per = self._sweep_seconds(j) * self.scale
-            target = self.tick_s / share if j.lane == "grid" else self.tick_s
-            n = max(1, int(target / per))
-            n = min(n, j.req.sweeps - j.launched)
-            if j.lane == "grid":
+        for j in lane.jobs:
+            left = j.req.sweeps - j.launched
+            if left <= 0:
+                continue
+            per = self._sweep_seconds(j) * lane.scale
+            n = min(left, max(1, int(self.tick_s / per)))
+            if lane.kind == "grid":
                 n = min(n, GRID_MAX_MEAS)
             plan.append([j, n])
-        total = sum(_round_up(j.meas_bytes * n) for j, n in plan)
-        if total > self.arena_bytes:
-            f = self.arena_bytes / total
-            for p in plan:
-                p[1] = max(1, int(p[1] * f * 0.98))
-            while sum(_round_up(j.meas_bytes * n) for j, n in plan) > self.arena_bytes and len(plan) > 1:
-                plan.pop()
-        item_t = [self._sweep_seconds(j) * self.scale * n for j, n in plan if j.lane == "items"]
-        grid_t = sorted((self._sweep_seconds(j) * self.scale * n for j, n in plan if j.lane == "grid"),
-                        reverse=True)
-        loads = [0.0] * len(self.grid_pool)
-        for t in grid_t:  # the launch assigns grid jobs longest first to the least loaded stream
-            loads[loads.index(min(loads))] += t
-        predicted = max(item_t + loads)
+        if not plan:
+            return [], 0.0
+        predicted = max(self._sweep_seconds(j) * lane.scale * n for j, n in plan)
         return plan, predicted
 
-    def _launch(self, plan, predicted) -> _Tick:
-        slot = self.ticks % 2
-        self.ticks += 1
-        base = ptr(self.arena[slot])
+    def _launch(self, lane: _Lane) -> bool:
+        plan, predicted = self._plan(lane)
+        if not plan:
+            return False
+        size = sum(_round_up(j.meas_bytes * n) for j, n in plan)
+        seg = self.arena.alloc(size)
+        if seg is None:
+            return False
+        s = lane.stream
+        if self.admit_event is not None:
+            s.wait_event(self.admit_event)
+        start, end, done = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+                            torch.cuda.Event())
+        start.record(s)
+        base = ptr(self.arena.dev) + seg
         entries = []
-        off = 0
+        off = seg
         items = []
-        grid = []
         for j, n in plan:
             entries.append((j, n, off))
             ptrs = []
-            o = off
+            o = base + (off - seg)
             for _, _, w in j.fields:
-                ptrs.append(base + o)
+                ptrs.append(o)
                 o += 8 * w * n
-            if j.lane == "items":
+            if lane.kind == "items":
                 it = CritmcItem.from_buffer_copy(j.item)
                 it.sweep0 = j.chain.sweep
                 it.n_meas = n
@@ -428,76 +509,66 @@ class Server:
                     it.sc_out, it.ss_out = ptrs[2], ptrs[3]
                 items.append(it)
             else:
-                grid.append((j, n, ptrs))
+                self._grid_call(lane, j, n, ptrs)
             off = _round_up(off + j.meas_bytes * n)
-        s = self.stream
-        start, end, done = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-                            torch.cuda.Event())
-        start.record(s)
         if items:
+            slot = lane.n_ticks % 2
             need = len(items) * ctypes.sizeof(CritmcItem)
-            if self.staging[slot] is None or self.staging[slot].numel() < need:
-                self.staging[slot] = torch.empty(max(need, 1 << 16), dtype=torch.uint8, pin_memory=True)
+            if lane.staging[slot] is None or lane.staging[slot].numel() < need:
+                lane.staging[slot] = torch.empty(max(need, 1 << 16), dtype=torch.uint8, pin_memory=True)
+            if lane.item_buffer is None or lane.item_buffer.numel() < _lib.lib().critmc_items_buffer_bytes(len(items)):
+                # grow with headroom; the old buffer is only replaced between ticks of this stream
+                lane.item_buffer = empty_bytes(_lib.lib().critmc_items_buffer_bytes(2 * len(items) + 64), self.device)
             arr = (CritmcItem * len(items))(*items)
-            self.item_buffer = launch_items(arr, self.device, self.item_buffer, staging=self.staging[slot],
-                                            stream=s.cuda_stream)
-        if grid:
-            fork = torch.cuda.Event()
-            fork.record(s)
-            used = set()
-            loads = [0.0] * len(self.grid_pool)
-            grid.sort(key=lambda g: -self._sweep_seconds(g[0]) * g[1])
-            for j, n, ptrs in grid:
-                k = loads.index(min(loads))
-                loads[k] += self._sweep_seconds(j) * n
-                gs = self.grid_pool[k]
-                if k not in used:
-                    gs.wait_event(fork)
-                    used.add(k)
-                scratch = self._grid_scratch(k)
-                c = j.chain
-                lx, ly, lz = c.dims
-                if j.family == "msc":
-                    _lib.call("critmc_ising_msc_run", ptr(c.words), len(c.shape), lx, ly, lz, 1,
-                              c.key.ctypes.data, j.tables.ctypes.data, 1, c.sweep, j.sched.ctypes.data,
-                              len(j.sched), n, ptr(j.tensors["running"]), ptrs[0], ptrs[1], ptrs[2],
-                              ptr(scratch), 0, c.k_inline, gs.cuda_stream)
-                else:
-                    betas, steps = j.tables
-                    _lib.call("critmc_on_run_grid", ptr(c.spins), len(c.shape), lx, ly, lz, c.n, 1,
-                              c.key.ctypes.data, betas.ctypes.data, steps.ctypes.data, 1, c.sweep,
-                              j.sched.ctypes.data, len(j.sched), n, ptrs[0], ptrs[1], ptrs[2], ptrs[3],
-                              ptrs[4], ptr(scratch), c.blocks_per_chain, gs.cuda_stream)
-            for k in used:
-                join = torch.cuda.Event()
-                join.record(self.grid_pool[k])
-                s.wait_event(join)
+            launch_items(arr, self.device, lane.item_buffer, staging=lane.staging[slot], stream=s.cuda_stream)
         end.record(s)
         with torch.cuda.stream(s):
-            if off:
-                self.host[slot][:off].copy_(self.arena[slot][:off], non_blocking=True)
+            self.arena.host[seg:seg + size].copy_(self.arena.dev[seg:seg + size], non_blocking=True)
         done.record(s)
         for j, n, _ in entries:
             j.launched += n
             j.chain.sweep += n * j.sweeps_per_meas
-        return _Tick(slot, entries, off, predicted, start, end, done)
+        lane.n_ticks += 1
+        self.ticks += 1
+        lane.inflight.append(_Tick(lane, entries, seg, size, predicted, start, end, done, self.ticks))
+        return True
 
-    def _grid_scratch(self, k: int) -> torch.Tensor:
-        if self.grid_scratch[k] is None:
+    def _grid_call(self, lane: _Lane, j: _Job, n: int, ptrs: list) -> None:
+        s = lane.stream
+        scratch = self._grid_scratch(s)
+        c = j.chain
+        lx, ly, lz = c.dims
+        if j.family == "msc":
+            _lib.call("critmc_ising_msc_run", ptr(c.words), len(c.shape), lx, ly, lz, 1, c.key.ctypes.data,
+                      j.tables.ctypes.data, 1, c.sweep, j.sched.ctypes.data, len(j.sched), n,
+                      ptr(j.tensors["running"]), ptrs[0], ptrs[1], ptrs[2], ptr(scratch), 0, c.k_inline,
+                      s.cuda_stream)
+        else:
+            betas, steps = j.tables
+            _lib.call("critmc_on_run_grid", ptr(c.spins), len(c.shape), lx, ly, lz, c.n, 1, c.key.ctypes.data,
+                      betas.ctypes.data, steps.ctypes.data, 1, c.sweep, j.sched.ctypes.data, len(j.sched), n,
+                      ptrs[0], ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptr(scratch), c.blocks_per_chain,
+                      s.cuda_stream)
+
+    def _grid_scratch(self, stream: torch.cuda.Stream) -> torch.Tensor:
+        key = stream.cuda_stream
+        if key not in self.grid_scratch:
             lib = _lib.lib()
             need = max(lib.critmc_ising_msc_scratch_bytes(1, GRID_MAX_MEAS),
                        lib.critmc_on_grid_scratch_bytes(1, GRID_MAX_MEAS, 3, 3))
-            self.grid_scratch[k] = empty_bytes(need, self.device)
-        return self.grid_scratch[k]
+            self.grid_scratch[key] = empty_bytes(need, self.device)
+        return self.grid_scratch[key]
 
     def _harvest(self, tick: _Tick) -> None:
         tick.done.synchronize()
+        lane = tick.lane
+        lane.inflight.popleft()
         gpu = tick.start.elapsed_time(tick.end) * 1e-3
         self.gpu_seconds += gpu
         if tick.predicted > 0 and gpu > 0:
-            # damped correction of the tick planner's cost model
-            self.scale *= min(4.0, max(0.25, (gpu / tick.predicted))) ** 0.5
-        host = self.host[tick.slot].numpy()
+            # damped correction of this lane's cost model
+            lane.scale *= min(4.0, max(0.25, gpu / tick.predicted)) ** 0.5
+        host = self.arena.host_np
         now = self.now()
         for j, n, off in tick.entries:
             o = off
@@ -514,6 +585,9 @@ class Server:
             self.updates_done += n * j.sweeps_per_meas * j.req.n_sites
             if j.harvested == j.req.sweeps:
                 self._finish(j, now)
+        self.arena.release(tick.offset, tick.size)
+        if lane.kind == "grid" and not lane.jobs and not lane.inflight:
+            self.grid_lanes.remove(lane)
 
     def _finish(self, j: _Job, now: float) -> None:
         req = j.req
@@ -531,6 +605,7 @@ class Server:
         res = Result(req, series, state, float(req.arrival), j.admitted, now,
                      req.n_sites * j.sweeps_per_meas * req.sweeps)
         self.active.remove(j)
+        j.home.jobs.remove(j)
         self.in_use -= j.dev_bytes
         j.chain = None
         j.tensors.clear()
@@ -541,21 +616,29 @@ class Server:
 
     # ---- driving ---------------------------------------------------------
     def step(self) -> bool:
-        """Admit, launch one tick, harvest the older tick; False when idle."""
-        self._admit()
-        plan, predicted = self._plan()
-        if plan:
-            self.inflight.append(self._launch(plan, predicted))
-        if self.inflight and (len(self.inflight) >= 2 or not plan):
-            self._harvest(self.inflight.popleft())
-        return bool(self.queue or self.active or self.inflight)
+        """Admit, harvest finished ticks, keep two ticks in flight per lane.
+
+        Returns False when there is nothing left to do.
+        """
+        progress = self._admit()
+        for lane in list(self._lanes()):
+            while lane.inflight and lane.inflight[0].done.query():
+                self._harvest(lane.inflight[0])
+                progress = True
+        for lane in list(self._lanes()):
+            while len(lane.inflight) < 2 and self._launch(lane):
+                progress = True
+        busy = any(lane.inflight for lane in self._lanes())
+        if not progress and busy:
+            time.sleep(2e-4)  # nothing to do until a tick ends
+        return bool(self.queue or self.active or busy)
 
     def run(self, requests=None) -> list[Result]:
         """Submit ``requests`` (in arrival order) and serve until all are done."""
         for r in requests or ():
             self.submit(r)
         while self.step():
-            if not self.active and not self.inflight and self.queue:
+            if not self.active and self.queue:
                 wait = self.queue[0].arrival - self.now()
                 if wait > 0:
                     time.sleep(wait)

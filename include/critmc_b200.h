@@ -281,6 +281,13 @@ int64_t critmc_items_buffer_bytes(int32_t n_items);
 int32_t critmc_run_items(const critmc_item* items, int32_t n_items, void* buffer,
                          int64_t buffer_bytes, void* staging, int32_t smem_limit, void* stream);
 
+/* Instantiated CUDA graphs are cached across calls with identical parameters
+ * (the same chains advanced slice after slice): capacity in entries (default
+ * 64, 0 disables caching and frees every entry) and current size.  No
+ * counterpart in critmc.                                                     */
+int32_t critmc_graph_cache_set_capacity(int32_t entries);
+int32_t critmc_graph_cache_size(void);
+
 /* critmc_ising_msc_run for callers that cannot allocate device memory.
  * No counterpart in the reference (critmc has no device memory at all).
  * Some callers cannot call cudaMalloc where they run the sampler: a plugin

@@ -67,6 +67,9 @@ SIGNATURES: dict[str, tuple] = {
     ),
     "critmc_on_grid_scratch_bytes": (_I64, [_I32, _I32, _I32, _I32]),
     "critmc_graph_cache_set_capacity": (_I32, [_I32]),
+    "critmc_ea_campaign_buffer_bytes": (_I64, [_I32, _I64]),
+    "critmc_ea_campaign_run": (
+        _I32, [_P, _I32, _I32, _I32, _P, _P, _I32, _U32, _I32, _I32, _I32, _P, _I64, _P, _P]),
     "critmc_graph_cache_size": (_I32, []),
     "critmc_on_run_grid": (
         _I32,

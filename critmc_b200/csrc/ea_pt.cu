@@ -12,8 +12,10 @@
 //
 // Replaces critmc src/critmc/kernels/glass.py:81-163 (`pt_run`), :42-53
 // (`metropolis_sweep`), :34-38 (`energy`), :57-77 (`_measure`).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "geom.cuh"
 #include "host_common.h"
@@ -29,10 +31,18 @@ constexpr int EA_NOBS = 7;  // e, q_l, |q|, q^2, q^4, |q(kmin)|^2, count (critmc
 constexpr int EA_PSAMPLES = 512;
 constexpr int EA_FIXCAP = 64;
 
-struct EaParams {
+// Temperature set and step counts shared by every sample of a call.
+struct EaCommon {
+  const uint32_t* swap_thr;
+  int m, n_steps, n_bins, sweeps_per_step, swap_width;
+  uint32_t t0;
+  uint32_t planes[3][32];  // lane masks of the threshold bits, classes v = 0..z/2-1
+};
+
+// One lattice size: its samples' device arrays and geometry.
+struct EaSet {
   uint32_t* words;
   const uint8_t* jneg;
-  const uint32_t* swap_thr;
   uint8_t* conf_at;
   uint8_t* labels;
   double* acc;
@@ -40,20 +50,25 @@ struct EaParams {
   long long* swap_try;
   long long* label_hist;
   long long* trips;
+  const uint32_t* keys;  // device [n_samples][2][2] (campaign), or null (keys in parameters)
   ByteGeom g;
-  int m, n_samples, sample0, n_steps, n_bins, sweeps_per_step, swap_width;
-  uint32_t t0;
-  uint32_t planes[3][32];  // lane masks of the threshold bits, classes v = 0..z/2-1
-  double cosx[EA_MAX_L], sinx[EA_MAX_L];  // cos/sin(2 pi x / L) per axis extent (same L per axis)
+  int n_samples;
   int ext[3];
+  double cosx[EA_MAX_L], sinx[EA_MAX_L];  // cos/sin(2 pi x / L) per axis extent (same L per axis)
+};
+
+struct EaParams {
+  EaCommon C;
+  EaSet S;
+  int sample0;
   uint32_t keys[EA_PSAMPLES][2][2];
 };
 
 // threshold bit plane for the undecided lanes (counts 0 .. z/2-1)
 template <int Z>
-__device__ __forceinline__ uint32_t ea_tbits(const EaParams& P, const Count3& c, int q) {
-  const uint32_t lo = mux(c.b0, P.planes[1][q], P.planes[0][q]);
-  if constexpr (Z == 6) return mux(c.b1, P.planes[2][q], lo);
+__device__ __forceinline__ uint32_t ea_tbits(const EaCommon& C, const Count3& c, int q) {
+  const uint32_t lo = mux(c.b0, C.planes[1][q], C.planes[0][q]);
+  if constexpr (Z == 6) return mux(c.b1, C.planes[2][q], lo);
   return lo;
 }
 
@@ -62,9 +77,8 @@ struct EaFix {
 };
 
 template <int Z>
-__device__ __forceinline__ void ea_site(const EaParams& P, const uint32_t* lat, const uint8_t* jn,
+__device__ __forceinline__ void ea_site(const ByteGeom& g, const uint32_t* lat, const uint8_t* jn,
                                         int set, int c, uint32_t s, uint32_t& w_s, Count3& cnt) {
-  const ByteGeom& g = P.g;
   int r, i;
   byte_row_index(g, s, r, i);
   uint32_t nb[Z];
@@ -81,7 +95,7 @@ __device__ __forceinline__ void ea_site(const EaParams& P, const uint32_t* lat, 
 }
 
 template <int Z>
-__device__ __forceinline__ void ea_planes(const EaParams& P, const Count3& cnt, uint32_t k0,
+__device__ __forceinline__ void ea_planes(const EaCommon& C, const Count3& cnt, uint32_t k0,
                                           uint32_t k1, uint32_t slot, uint32_t sweep, uint32_t col,
                                           int g_begin, int g_end, uint32_t& D, uint32_t& U) {
   for (int grp = g_begin; grp < g_end && U; ++grp) {
@@ -89,23 +103,29 @@ __device__ __forceinline__ void ea_planes(const EaParams& P, const Count3& cnt, 
         slot, sweep, CRITMC_TAG_PLANES | ((uint32_t)grp << 8) | (col << 16), 0u, k0, k1);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const uint32_t t = ea_tbits<Z>(P, cnt, 4 * grp + q);
+      const uint32_t t = ea_tbits<Z>(C, cnt, 4 * grp + q);
       D |= U & t & ~r.v[q];
       U &= ~(r.v[q] ^ t);
     }
   }
 }
 
+// Dynamic shared memory of one sample's block.
+inline size_t ea_smem_bytes(const ByteGeom& g, int dim, int lx) {
+  return (size_t)(2 * g.slots) * (2 * 4 + 4 + 1) + (size_t)dim * lx * 32 * 4;
+}
+
+// All PT steps of one sample by one thread block.  key[set] = Philox key of replica set.
 template <int Z>
-__global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant__ EaParams P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, const uint32_t (&key)[2][2],
+                              unsigned char* smem_raw) {
   constexpr int DIM = Z / 2;
-  const ByteGeom& g = P.g;
+  const ByteGeom& g = S.g;
   const uint32_t n_sites = 2 * g.slots;
   uint32_t* lat = reinterpret_cast<uint32_t*>(smem_raw);  // [2 sets][2 colours][slots]
   uint32_t* qw = lat + 2 * n_sites;                      // overlap words [2][slots]
   int* splane = reinterpret_cast<int*>(qw + n_sites);    // [DIM][L][32] overlap per plane and lane
-  uint8_t* jn = reinterpret_cast<uint8_t*>(splane + DIM * P.ext[0] * 32);  // [2][slots]
+  uint8_t* jn = reinterpret_cast<uint8_t*>(splane + DIM * S.ext[0] * 32);  // [2][slots]
   __shared__ EaFix fix[EA_WARPS][EA_FIXCAP];
   __shared__ int ecnt[2][32];  // unsatisfied bonds per set and temperature
   __shared__ int qlcnt[32];    // agreeing bonds of the overlap field
@@ -114,18 +134,16 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
   __shared__ double acc_s[32][EA_NOBS];
   __shared__ unsigned long long sw_acc[32], sw_try[32], lhist[32][2], trip[2];
 
-  const int lsample = blockIdx.x;
-  const int sample = P.sample0 + lsample;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int m = P.m;
-  uint32_t* gw = P.words + (size_t)sample * 2 * n_sites;
+  const int m = C.m;
+  uint32_t* gw = S.words + (size_t)sample * 2 * n_sites;
   for (uint32_t j = tid; j < 2 * n_sites; j += EA_THREADS) lat[j] = gw[j];
-  for (uint32_t j = tid; j < n_sites; j += EA_THREADS) jn[j] = P.jneg[(size_t)sample * n_sites + j];
+  for (uint32_t j = tid; j < n_sites; j += EA_THREADS) jn[j] = S.jneg[(size_t)sample * n_sites + j];
   if (tid < 64) {
     const int r = tid >> 5, k = tid & 31;
     if (k < m) {
-      conf[r][k] = P.conf_at[((size_t)sample * 2 + r) * m + k];
-      lab[r][k] = P.labels[((size_t)sample * 2 + r) * m + k];
+      conf[r][k] = S.conf_at[((size_t)sample * 2 + r) * m + k];
+      lab[r][k] = S.labels[((size_t)sample * 2 + r) * m + k];
     }
   }
   if (tid < 32) {
@@ -139,21 +157,21 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
   const uint32_t lt_mask = (1u << lane) - 1u;
   int bin = 0;
   long long next_edge = 1;
-  for (int t = 0; t < P.n_steps; ++t) {
+  for (int t = 0; t < C.n_steps; ++t) {
     if (t >= next_edge) {
       // flush the finished bin (critmc glass.py:114-122)
       if (tid < m)
         for (int o = 0; o < EA_NOBS; ++o) {
-          P.acc[(((size_t)sample * P.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
+          S.acc[(((size_t)sample * C.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
           acc_s[tid][o] = 0.0;
         }
       ++bin;
       next_edge = (1LL << (bin + 1)) - 1;
     }
-    const uint32_t step = P.t0 + (uint32_t)t;
+    const uint32_t step = C.t0 + (uint32_t)t;
     // ---- sweeps of every temperature of both sets --------------------------
-    for (int sw = 0; sw < P.sweeps_per_step; ++sw) {
-      const uint32_t sweep = step * (uint32_t)P.sweeps_per_step + (uint32_t)sw;
+    for (int sw = 0; sw < C.sweeps_per_step; ++sw) {
+      const uint32_t sweep = step * (uint32_t)C.sweeps_per_step + (uint32_t)sw;
       for (int c = 0; c < 2; ++c) {
         int nf = 0;
         const uint32_t work = 2 * g.slots;  // both sets, one colour
@@ -166,13 +184,13 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
             const uint32_t s = j - set * g.slots;
             uint32_t w_s;
             Count3 cnt;
-            ea_site<Z>(P, lat, jn, set, c, s, w_s, cnt);
+            ea_site<Z>(g, lat, jn, set, c, s, w_s, cnt);
             // flips with dE <= 0 (>= z/2 unsatisfied bonds) are always accepted
             const uint32_t alw = (Z == 6) ? (cnt.b2 | (cnt.b1 & cnt.b0)) : (cnt.b1 | cnt.b2);
             D = alw;
             U = ~alw;
-            const uint32_t k0 = P.keys[lsample][set][0], k1 = P.keys[lsample][set][1];
-            ea_planes<Z>(P, cnt, k0, k1, s, sweep, (uint32_t)c, 0, 2, D, U);
+            const uint32_t k0 = key[set][0], k1 = key[set][1];
+            ea_planes<Z>(C, cnt, k0, k1, s, sweep, (uint32_t)c, 0, 2, D, U);
             idx = (uint32_t)set * n_sites + (uint32_t)c * g.slots + s;
             if (U == 0) lat[idx] = w_s ^ D;
           }
@@ -187,9 +205,9 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
                 const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
                 uint32_t w_s;
                 Count3 cnt;
-                ea_site<Z>(P, lat, jn, set, c, s, w_s, cnt);
+                ea_site<Z>(g, lat, jn, set, c, s, w_s, cnt);
                 uint32_t D2 = f.D, U2 = f.U;
-                ea_planes<Z>(P, cnt, P.keys[lsample][set][0], P.keys[lsample][set][1], s, sweep,
+                ea_planes<Z>(C, cnt, key[set][0], key[set][1], s, sweep,
                              (uint32_t)c, 2, 8, D2, U2);
                 lat[f.idx] = w_s ^ D2;
               }
@@ -207,9 +225,9 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
           const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
           uint32_t w_s;
           Count3 cnt;
-          ea_site<Z>(P, lat, jn, set, c, s, w_s, cnt);
+          ea_site<Z>(g, lat, jn, set, c, s, w_s, cnt);
           uint32_t D2 = f.D, U2 = f.U;
-          ea_planes<Z>(P, cnt, P.keys[lsample][set][0], P.keys[lsample][set][1], s, sweep,
+          ea_planes<Z>(C, cnt, key[set][0], key[set][1], s, sweep,
                        (uint32_t)c, 2, 8, D2, U2);
           lat[f.idx] = w_s ^ D2;
         }
@@ -224,9 +242,9 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
       for (uint32_t s = warp; s < g.slots; s += EA_WARPS) {  // colour-0 sites see every bond once
         uint32_t w_s;
         Count3 cnt;
-        ea_site<Z>(P, lat, jn, 0, 0, s, w_s, cnt);
+        ea_site<Z>(g, lat, jn, 0, 0, s, w_s, cnt);
         ca += ((cnt.b0 >> lane) & 1) + 2 * ((cnt.b1 >> lane) & 1) + 4 * ((cnt.b2 >> lane) & 1);
-        ea_site<Z>(P, lat, jn, 1, 0, s, w_s, cnt);
+        ea_site<Z>(g, lat, jn, 1, 0, s, w_s, cnt);
         cb += ((cnt.b0 >> lane) & 1) + 2 * ((cnt.b1 >> lane) & 1) + 4 * ((cnt.b2 >> lane) & 1);
       }
       atomicAdd(&ecnt[0][lane], ca);
@@ -242,16 +260,16 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
         e[k] = -(n_bonds - 2LL * ecnt[r][k]);
         sigma[r][k] = k;
       }
-      const uint32_t k0 = P.keys[lsample][r][0], k1 = P.keys[lsample][r][1];
+      const uint32_t k0 = key[r][0], k1 = key[r][1];
       for (int k = 0; k < m - 1; ++k) {
         // betas ascend hot -> cold, so x = (b_k - b_k+1)(E_k - E_k+1) >= 0 iff E_k <= E_k+1
         const long long de = e[k] - e[k + 1];
         bool ok = de <= 0;
         if (!ok) {
           long long j = de / 4;
-          if (j > P.swap_width - 1) j = P.swap_width - 1;
+          if (j > C.swap_width - 1) j = C.swap_width - 1;
           const uint32_t u = critmc_philox4x32((uint32_t)k, step, CRITMC_TAG_SWAP | ((uint32_t)r << 16), 0u, k0, k1).v[0];
-          ok = u < P.swap_thr[(size_t)k * P.swap_width + j];
+          ok = u < C.swap_thr[(size_t)k * C.swap_width + j];
         }
         atomicAdd(&sw_try[k], 1ULL);
         if (ok) {
@@ -310,9 +328,9 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
     // per-plane overlap counts: warp w handles planes (d, x) = w, w + WARPS, ...
     for (int pl = warp; pl < DIM * EA_MAX_L; pl += EA_WARPS) {
       const int d = pl / EA_MAX_L, x0 = pl % EA_MAX_L;
-      if (x0 >= P.ext[d]) continue;
+      if (x0 >= S.ext[d]) continue;
       int cnt = 0;
-      const int e1 = P.ext[d == 0 ? 1 : 0], e2 = DIM == 3 ? P.ext[d == 2 ? 1 : 2] : 1;
+      const int e1 = S.ext[d == 0 ? 1 : 0], e2 = DIM == 3 ? S.ext[d == 2 ? 1 : 2] : 1;
       for (int u = 0; u < e1; ++u)
         for (int v = 0; v < e2; ++v) {
           int xyz[3] = {0, 0, 0};
@@ -323,7 +341,7 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
           const uint32_t slot = (uint32_t)((xyz[1] + g.ly * xyz[2]) * g.hx + xyz[0] / 2);
           cnt += (qw[(size_t)col * g.slots + slot] >> lane) & 1;
         }
-      splane[(d * P.ext[0] + x0) * 32 + lane] = cnt;
+      splane[(d * S.ext[0] + x0) * 32 + lane] = cnt;
     }
     __syncthreads();
     if (tid < m) {
@@ -331,17 +349,17 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
       const double n = (double)n_sites;
       const double nb = n * DIM;
       int qs = 0;
-      for (int x = 0; x < P.ext[0]; ++x) qs += splane[x * 32 + k];
+      for (int x = 0; x < S.ext[0]; ++x) qs += splane[x * 32 + k];
       const double q = (2.0 * qs - n) / n;
       const double ql = (2.0 * qlcnt[k] - nb) / nb;
       double qk2 = 0.0;
       for (int d = 0; d < DIM; ++d) {
-        const double per = n / P.ext[d];
+        const double per = n / S.ext[d];
         double re = 0.0, im = 0.0;
-        for (int x = 0; x < P.ext[d]; ++x) {
-          const double sx = 2.0 * splane[(d * P.ext[0] + x) * 32 + k] - per;
-          re += P.cosx[x] * sx;
-          im += P.sinx[x] * sx;
+        for (int x = 0; x < S.ext[d]; ++x) {
+          const double sx = 2.0 * splane[(d * S.ext[0] + x) * 32 + k] - per;
+          re += S.cosx[x] * sx;
+          im += S.sinx[x] * sx;
         }
         qk2 += (re * re + im * im) / (n * n);
       }
@@ -360,24 +378,64 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
   // ---- write back ------------------------------------------------------------
   if (tid < m)
     for (int o = 0; o < EA_NOBS; ++o)
-      P.acc[(((size_t)sample * P.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
+      S.acc[(((size_t)sample * C.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
   for (uint32_t j = tid; j < 2 * n_sites; j += EA_THREADS) gw[j] = lat[j];
   if (tid < 64) {
     const int r = tid >> 5, k = tid & 31;
     if (k < m) {
-      P.conf_at[((size_t)sample * 2 + r) * m + k] = (uint8_t)conf[r][k];
-      P.labels[((size_t)sample * 2 + r) * m + k] = (uint8_t)lab[r][k];
+      S.conf_at[((size_t)sample * 2 + r) * m + k] = (uint8_t)conf[r][k];
+      S.labels[((size_t)sample * 2 + r) * m + k] = (uint8_t)lab[r][k];
     }
   }
   if (tid < m - 1) {
-    P.swap_acc[(size_t)sample * (m - 1) + tid] += (long long)sw_acc[tid];
-    P.swap_try[(size_t)sample * (m - 1) + tid] += (long long)sw_try[tid];
+    S.swap_acc[(size_t)sample * (m - 1) + tid] += (long long)sw_acc[tid];
+    S.swap_try[(size_t)sample * (m - 1) + tid] += (long long)sw_try[tid];
   }
   if (tid < m) {
-    P.label_hist[((size_t)sample * m + tid) * 2 + 0] += (long long)lhist[tid][0];
-    P.label_hist[((size_t)sample * m + tid) * 2 + 1] += (long long)lhist[tid][1];
+    S.label_hist[((size_t)sample * m + tid) * 2 + 0] += (long long)lhist[tid][0];
+    S.label_hist[((size_t)sample * m + tid) * 2 + 1] += (long long)lhist[tid][1];
   }
-  if (tid < 2) P.trips[(size_t)sample * 2 + tid] += (long long)trip[tid];
+  if (tid < 2) S.trips[(size_t)sample * 2 + tid] += (long long)trip[tid];
+}
+
+
+template <int Z>
+__global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant__ EaParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lsample = blockIdx.x;
+  const uint32_t key[2][2] = {{P.keys[lsample][0][0], P.keys[lsample][0][1]},
+                              {P.keys[lsample][1][0], P.keys[lsample][1][1]}};
+  ea_sample_run<Z>(P.C, P.S, P.sample0 + lsample, key, smem_raw);
+}
+
+// A campaign: samples of several lattice sizes in one persistent launch.  Work
+// item w is (set, sample) = work[w] (set << 24 | sample), largest lattices
+// first; blocks take items from *queue until the list is done.
+struct EaCampaignParams {
+  EaCommon C;
+  const EaSet* sets;
+  const uint32_t* work;
+  unsigned* queue;
+  int n_work;
+};
+
+template <int Z>
+__global__ void __launch_bounds__(EA_THREADS, 3) ea_campaign_kernel(const __grid_constant__ EaCampaignParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int cur;
+  for (;;) {
+    if (threadIdx.x == 0) cur = (int)atomicAdd(P.queue, 1u);
+    __syncthreads();
+    const int w = cur;
+    __syncthreads();
+    if (w >= P.n_work) break;
+    const EaSet& S = P.sets[P.work[w] >> 24];
+    const int sample = (int)(P.work[w] & 0xFFFFFFu);
+    const uint32_t* k = S.keys + (size_t)sample * 4;
+    const uint32_t key[2][2] = {{k[0], k[1]}, {k[2], k[3]}};
+    ea_sample_run<Z>(P.C, S, sample, key, smem_raw);
+    __syncthreads();
+  }
 }
 
 static thread_local EaParams g_ea;
@@ -445,6 +503,81 @@ extern "C" int32_t critmc_ea_coupling_bits(int32_t dim, int32_t lx, int32_t ly, 
   return CRITMC_OK;
 }
 
+namespace critmc {
+
+// Validate the temperature set and step counts; fill the per-lane threshold planes.
+static int ea_common(EaCommon& C, int dim, int m, const double* betas, const uint32_t* swap_thr,
+                     int swap_width, uint32_t t0, int n_steps, int n_bins, int sweeps_per_step) {
+  if (!betas || !swap_thr) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (dim < 2 || dim > 3) return fail(CRITMC_ERR_UNSUPPORTED, "EA samples need dim 2 or 3");
+  if (m < 2 || m > 32) return fail(CRITMC_ERR_INVALID, "need 2 <= m <= 32 temperatures");
+  if (n_steps < 0 || n_bins < 1 || n_bins > 31 || (long long)n_steps > (1LL << n_bins) - 1)
+    return fail(CRITMC_ERR_INVALID, "need 0 <= n_steps <= 2^n_bins - 1 and 1 <= n_bins <= 31");
+  if (sweeps_per_step < 1) return fail(CRITMC_ERR_INVALID, "sweeps_per_step must be >= 1");
+  if (swap_width < 2) return fail(CRITMC_ERR_INVALID, "swap_width must be >= 2");
+  if (((long long)t0 + n_steps) * sweeps_per_step > 0xFFFFFFFFLL)
+    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+  for (int k = 0; k + 1 < m; ++k)
+    if (!(betas[k] < betas[k + 1])) return fail(CRITMC_ERR_INVALID, "betas must increase (hot -> cold)");
+  const int z = 2 * dim;
+  // per-lane Metropolis thresholds exp(-beta_k (2z - 4v)), v = 0..z/2-1 unsatisfied bonds
+  std::memset(C.planes, 0, sizeof(C.planes));
+  for (int v = 0; v < z / 2; ++v)
+    for (int k = 0; k < m; ++k) {
+      if (!std::isfinite(betas[k]) || betas[k] <= 0.0) return fail(CRITMC_ERR_INVALID, "betas must be positive");
+      const double p = std::exp(-betas[k] * (2.0 * z - 4.0 * v));
+      const double tt = std::nearbyint(std::ldexp(p, 32));
+      const uint32_t thr = tt >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)tt;
+      for (int q = 0; q < 32; ++q)
+        if ((thr >> (31 - q)) & 1u) C.planes[v][q] |= 1u << k;
+    }
+  C.swap_thr = swap_thr;
+  C.m = m;
+  C.n_steps = n_steps;
+  C.n_bins = n_bins;
+  C.sweeps_per_step = sweeps_per_step;
+  C.swap_width = swap_width;
+  C.t0 = t0;
+  return CRITMC_OK;
+}
+
+// Validate one lattice size and fill its set (device pointers as given).
+static int ea_set(EaSet& S, int dim, int lx, int ly, int lz, int n_samples, uint32_t* words,
+                  const uint8_t* jneg, uint8_t* conf_at, uint8_t* labels, double* acc, int64_t* swap_acc,
+                  int64_t* swap_try, int64_t* label_hist, int64_t* trips) {
+  int st = byte_geom(dim, lx, ly, lz, S.g);
+  if (st) return st;
+  if (dim < 2) return fail(CRITMC_ERR_UNSUPPORTED, "EA samples need dim 2 or 3");
+  if (2 * S.g.slots > (uint32_t)EA_MAX_SITES) return fail(CRITMC_ERR_UNSUPPORTED, "at most 4096 sites per sample");
+  if (lx > EA_MAX_L || S.g.ly > EA_MAX_L || S.g.lz > EA_MAX_L) return fail(CRITMC_ERR_UNSUPPORTED, "extent too large");
+  if (lx != S.g.ly || (dim == 3 && lx != S.g.lz))
+    return fail(CRITMC_ERR_UNSUPPORTED, "EA samples use equal extents (one k_min table)");
+  if (!words || !jneg || !conf_at || !labels || !acc || !swap_acc || !swap_try || !label_hist || !trips)
+    return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (n_samples < 1 || n_samples > (1 << 24)) return fail(CRITMC_ERR_INVALID, "need 1 <= n_samples <= 2^24");
+  for (int x = 0; x < lx; ++x) {
+    S.cosx[x] = std::cos(2.0 * M_PI * x / lx);
+    S.sinx[x] = std::sin(2.0 * M_PI * x / lx);
+  }
+  S.ext[0] = lx;
+  S.ext[1] = S.g.ly;
+  S.ext[2] = S.g.lz;
+  S.words = words;
+  S.jneg = jneg;
+  S.conf_at = conf_at;
+  S.labels = labels;
+  S.acc = acc;
+  S.swap_acc = (long long*)swap_acc;
+  S.swap_try = (long long*)swap_try;
+  S.label_hist = (long long*)label_hist;
+  S.trips = (long long*)trips;
+  S.n_samples = n_samples;
+  S.keys = nullptr;
+  return CRITMC_OK;
+}
+
+}  // namespace critmc
+
 extern "C" int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_t dim, int32_t lx,
                                     int32_t ly, int32_t lz, int32_t m, int32_t n_samples,
                                     const uint32_t* keys, const double* betas,
@@ -455,65 +588,14 @@ extern "C" int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_
                                     void* stream) {
   clear_error();
   EaParams& P = g_ea;
-  int st = byte_geom(dim, lx, ly, lz, P.g);
+  if (!keys) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  int st = ea_set(P.S, dim, lx, ly, lz, n_samples, words, jneg, conf_at, labels, acc, swap_acc, swap_try,
+                  label_hist, trips);
   if (st) return st;
-  if (dim < 2) return fail(CRITMC_ERR_UNSUPPORTED, "EA samples need dim 2 or 3");
-  if (2 * P.g.slots > (uint32_t)EA_MAX_SITES) return fail(CRITMC_ERR_UNSUPPORTED, "at most 4096 sites per sample");
-  if (lx > EA_MAX_L || P.g.ly > EA_MAX_L || P.g.lz > EA_MAX_L) return fail(CRITMC_ERR_UNSUPPORTED, "extent too large");
-  if (lx != P.g.ly || (dim == 3 && lx != P.g.lz))
-    return fail(CRITMC_ERR_UNSUPPORTED, "EA samples use equal extents (one k_min table)");
-  if (!words || !jneg || !keys || !betas || !swap_thr || !conf_at || !labels || !acc || !swap_acc ||
-      !swap_try || !label_hist || !trips)
-    return fail(CRITMC_ERR_INVALID, "null pointer argument");
-  if (m < 2 || m > 32) return fail(CRITMC_ERR_INVALID, "need 2 <= m <= 32 temperatures");
-  if (n_samples < 1) return fail(CRITMC_ERR_INVALID, "need n_samples >= 1");
-  if (n_steps < 0 || n_bins < 1 || n_bins > 31 || (long long)n_steps > (1LL << n_bins) - 1)
-    return fail(CRITMC_ERR_INVALID, "need 0 <= n_steps <= 2^n_bins - 1 and 1 <= n_bins <= 31");
-  if (sweeps_per_step < 1) return fail(CRITMC_ERR_INVALID, "sweeps_per_step must be >= 1");
-  if (swap_width < 2) return fail(CRITMC_ERR_INVALID, "swap_width must be >= 2");
-  if (((long long)t0 + n_steps) * sweeps_per_step > 0xFFFFFFFFLL)
-    return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
-  for (int k = 0; k + 1 < m; ++k)
-    if (!(betas[k] < betas[k + 1])) return fail(CRITMC_ERR_INVALID, "betas must increase (hot -> cold)");
+  if ((st = ea_common(P.C, dim, m, betas, swap_thr, swap_width, t0, n_steps, n_bins, sweeps_per_step)))
+    return st;
   if (n_steps == 0) return CRITMC_OK;
-  const int z = 2 * dim;
-  // per-lane Metropolis thresholds exp(-beta_k (2z - 4v)), v = 0..z/2-1 unsatisfied bonds
-  std::memset(P.planes, 0, sizeof(P.planes));
-  for (int v = 0; v < z / 2; ++v)
-    for (int k = 0; k < m; ++k) {
-      if (!std::isfinite(betas[k]) || betas[k] <= 0.0) return fail(CRITMC_ERR_INVALID, "betas must be positive");
-      const double p = std::exp(-betas[k] * (2.0 * z - 4.0 * v));
-      const double tt = std::nearbyint(std::ldexp(p, 32));
-      const uint32_t thr = tt >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)tt;
-      for (int q = 0; q < 32; ++q)
-        if ((thr >> (31 - q)) & 1u) P.planes[v][q] |= 1u << k;
-    }
-  for (int x = 0; x < lx; ++x) {
-    P.cosx[x] = std::cos(2.0 * M_PI * x / lx);
-    P.sinx[x] = std::sin(2.0 * M_PI * x / lx);
-  }
-  P.ext[0] = lx;
-  P.ext[1] = P.g.ly;
-  P.ext[2] = P.g.lz;
-  P.words = words;
-  P.jneg = jneg;
-  P.swap_thr = swap_thr;
-  P.conf_at = conf_at;
-  P.labels = labels;
-  P.acc = acc;
-  P.swap_acc = (long long*)swap_acc;
-  P.swap_try = (long long*)swap_try;
-  P.label_hist = (long long*)label_hist;
-  P.trips = (long long*)trips;
-  P.m = m;
-  P.n_samples = n_samples;
-  P.n_steps = n_steps;
-  P.n_bins = n_bins;
-  P.sweeps_per_step = sweeps_per_step;
-  P.swap_width = swap_width;
-  P.t0 = t0;
-  const uint32_t n_sites = 2 * P.g.slots;
-  const size_t smem = (size_t)n_sites * (2 * 4 + 4 + 1) + (size_t)dim * lx * 32 * 4;
+  const size_t smem = ea_smem_bytes(P.S.g, dim, lx);
   cudaStream_t s = (cudaStream_t)stream;
   for (int c0 = 0; c0 < n_samples; c0 += EA_PSAMPLES) {
     const int nc = std::min(EA_PSAMPLES, n_samples - c0);
@@ -528,4 +610,74 @@ extern "C" int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_
     if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
   }
   return CRITMC_OK;
+}
+
+extern "C" int64_t critmc_ea_campaign_buffer_bytes(int32_t n_sizes, int64_t total_samples) {
+  if (n_sizes < 1 || total_samples < 1) return -1;
+  return 256 + (int64_t)n_sizes * (int64_t)sizeof(EaSet) + 4 * total_samples;
+}
+
+extern "C" int32_t critmc_ea_campaign_run(const critmc_ea_size* sizes, int32_t n_sizes, int32_t dim, int32_t m,
+                                          const double* betas, const uint32_t* swap_thr, int32_t swap_width,
+                                          uint32_t t0, int32_t n_steps, int32_t n_bins, int32_t sweeps_per_step,
+                                          void* buffer, int64_t buffer_bytes, void* staging, void* stream) {
+  clear_error();
+  if (!sizes || n_sizes < 1 || n_sizes > 255) return fail(CRITMC_ERR_INVALID, "need 1..255 lattice sizes");
+  if (!buffer) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  EaCampaignParams P;
+  int st = ea_common(P.C, dim, m, betas, swap_thr, swap_width, t0, n_steps, n_bins, sweeps_per_step);
+  if (st) return st;
+  std::vector<EaSet> sets(n_sizes);
+  long long total = 0;
+  size_t smem = 0;
+  for (int i = 0; i < n_sizes; ++i) {
+    const critmc_ea_size& z = sizes[i];
+    if (!z.keys) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+    if ((st = ea_set(sets[i], dim, z.lx, z.ly, z.lz, z.n_samples, z.words, z.jneg, z.conf_at, z.labels, z.acc,
+                     z.swap_acc, z.swap_try, z.label_hist, z.trips)))
+      return st;
+    sets[i].keys = z.keys;
+    total += z.n_samples;
+    smem = std::max(smem, ea_smem_bytes(sets[i].g, dim, z.lx));
+  }
+  if (buffer_bytes < critmc_ea_campaign_buffer_bytes(n_sizes, total))
+    return fail(CRITMC_ERR_INVALID, "campaign buffer too small");
+  if (n_steps == 0) return CRITMC_OK;
+  // host image of the buffer: [queue | sets | work], work sorted largest lattice first
+  const size_t sets_off = 256, work_off = 256 + (size_t)n_sizes * sizeof(EaSet);
+  const size_t bytes = work_off + 4 * (size_t)total;
+  std::vector<unsigned char> own;
+  unsigned char* img = static_cast<unsigned char*>(staging);
+  if (!img) {
+    own.resize(bytes);
+    img = own.data();
+  }
+  std::memset(img, 0, sets_off);
+  std::memcpy(img + sets_off, sets.data(), (size_t)n_sizes * sizeof(EaSet));
+  std::vector<int> order(n_sizes);
+  for (int i = 0; i < n_sizes; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sets[a].g.slots > sets[b].g.slots; });
+  uint32_t* work = reinterpret_cast<uint32_t*>(img + work_off);
+  size_t w = 0;
+  for (int i : order)
+    for (int smp = 0; smp < sets[i].n_samples; ++smp) work[w++] = ((uint32_t)i << 24) | (uint32_t)smp;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* dev = static_cast<unsigned char*>(buffer);
+  if (cudaMemcpyAsync(dev, img, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return cuda_fail("copy campaign");
+  P.queue = reinterpret_cast<unsigned*>(dev);
+  P.sets = reinterpret_cast<const EaSet*>(dev + sets_off);
+  P.work = reinterpret_cast<const uint32_t*>(dev + work_off);
+  P.n_work = (int)total;
+  auto launch = [&](auto kern) -> int {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return cuda_fail("shared memory attribute");
+    int per_sm = 0, dev_id = 0, sms = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, EA_THREADS, smem);
+    cudaGetDevice(&dev_id);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
+    const long long grid = std::max(1LL, std::min<long long>(total, (long long)std::max(1, per_sm) * sms));
+    kern<<<(unsigned)grid, EA_THREADS, smem, s>>>(P);
+    return cudaGetLastError() == cudaSuccess ? CRITMC_OK : cuda_fail("launch");
+  };
+  return dim == 2 ? launch(ea_campaign_kernel<4>) : launch(ea_campaign_kernel<6>);
 }

@@ -4,7 +4,9 @@ API of critmc ``src/critmc/glass.py``: ``EdwardsAnderson`` (one disorder
 realisation), ``geometric_temperatures``, ``ParallelTempering(model,
 temperatures, seed=..., sweeps_per_step=...).run(n_bins) -> TemperingRun``.
 ``SpinGlassCampaign`` runs many samples of one lattice in one launch (one
-thread block per sample, both replica sets resident in shared memory).
+thread block per sample, both replica sets resident in shared memory);
+``MultiSizeCampaign`` runs the samples of several lattice sizes in one
+persistent launch.
 
 Only bimodal (+-1) couplings map onto the replica multi-spin-coded kernel;
 Gaussian disorder is refused.  For the same seed, the couplings and the
@@ -14,6 +16,7 @@ two replica sets are drawn from the same Generator afterwards.
 
 from __future__ import annotations
 
+import ctypes
 import time
 from dataclasses import dataclass, field
 
@@ -25,7 +28,7 @@ from .device import ptr, require_cuda, stream_handle, to_host
 from .lattice import Lattice
 from .rng import make_rng, philox_key
 
-__all__ = ["EdwardsAnderson", "TemperingRun", "ParallelTempering", "SpinGlassCampaign",
+__all__ = ["EdwardsAnderson", "TemperingRun", "ParallelTempering", "SpinGlassCampaign", "MultiSizeCampaign",
            "geometric_temperatures", "OBS_E", "OBS_QL", "OBS_Q", "OBS_Q2", "OBS_Q4", "OBS_QK2",
            "OBS_COUNT", "N_OBS"]
 
@@ -183,42 +186,121 @@ class SpinGlassCampaign:
 
     def run(self, n_bins: int, n_steps: int | None = None) -> list[TemperingRun]:
         """Run ``2^n_bins - 1`` PT steps (or ``n_steps``), log-binned as critmc."""
-        S, m = self.n_samples, len(self.temperatures)
         n_steps = (1 << n_bins) - 1 if n_steps is None else int(n_steps)
-        dev = self.device
-        acc = torch.zeros((S, n_bins, m, N_OBS), dtype=torch.float64, device=dev)
-        swap_acc = torch.zeros((S, m - 1), dtype=torch.int64, device=dev)
-        swap_try = torch.zeros((S, m - 1), dtype=torch.int64, device=dev)
-        label_hist = torch.zeros((S, m, 2), dtype=torch.int64, device=dev)
-        trips = torch.zeros((S, 2), dtype=torch.int64, device=dev)
+        out = self._outputs(n_bins)
         shape = self.lattice.shape
         dims = tuple(shape) + (1,) * (3 - len(shape))
         t0 = time.perf_counter()
-        _lib.call("critmc_ea_pt_run", ptr(self.words), ptr(self.jneg), len(shape), *dims, m, S,
-                  self.keys.ctypes.data, self.betas.ctypes.data, ptr(self.swap_thr), SWAP_WIDTH,
-                  ptr(self.conf_at), ptr(self.labels), self.step, n_steps, n_bins,
-                  self.sweeps_per_step, ptr(acc), ptr(swap_acc), ptr(swap_try), ptr(label_hist),
-                  ptr(trips), stream_handle(dev))
-        torch.cuda.synchronize(dev)
-        wall = time.perf_counter() - t0
+        _lib.call("critmc_ea_pt_run", ptr(self.words), ptr(self.jneg), len(shape), *dims,
+                  len(self.temperatures), self.n_samples, self.keys.ctypes.data, self.betas.ctypes.data,
+                  ptr(self.swap_thr), SWAP_WIDTH, ptr(self.conf_at), ptr(self.labels), self.step, n_steps,
+                  n_bins, self.sweeps_per_step, *(ptr(out[k]) for k in _OUT_KEYS), stream_handle(self.device))
+        torch.cuda.synchronize(self.device)
         self.step += n_steps
-        acc_h, sa, st = to_host(acc), to_host(swap_acc), to_host(swap_try)
-        lh, tr = to_host(label_hist), to_host(trips)
-        runs = []
+        return self._collect(out, n_bins, time.perf_counter() - t0)
+
+    def _outputs(self, n_bins: int) -> dict[str, torch.Tensor]:
+        S, m, dev = self.n_samples, len(self.temperatures), self.device
+        return {"acc": torch.zeros((S, n_bins, m, N_OBS), dtype=torch.float64, device=dev),
+                "swap_acc": torch.zeros((S, m - 1), dtype=torch.int64, device=dev),
+                "swap_try": torch.zeros((S, m - 1), dtype=torch.int64, device=dev),
+                "label_hist": torch.zeros((S, m, 2), dtype=torch.int64, device=dev),
+                "trips": torch.zeros((S, 2), dtype=torch.int64, device=dev)}
+
+    def _collect(self, out: dict, n_bins: int, wall: float) -> list[TemperingRun]:
+        acc_h, sa, st = to_host(out["acc"]), to_host(out["swap_acc"]), to_host(out["swap_try"])
+        lh, tr = to_host(out["label_hist"]), to_host(out["trips"])
         with np.errstate(invalid="ignore", divide="ignore"):
             rate = sa / st
-        for i in range(S):
-            runs.append(TemperingRun(self.temperatures.copy(), self.lattice.n_sites, self.lattice.z,
-                                     acc_h[i], rate[i], lh[i], tr[i], wall / S,
-                                     {"n_bins": n_bins, "sweeps_per_step": self.sweeps_per_step,
-                                      "backend": "cuda"}))
-        return runs
+        return [TemperingRun(self.temperatures.copy(), self.lattice.n_sites, self.lattice.z, acc_h[i], rate[i],
+                             lh[i], tr[i], wall / self.n_samples,
+                             {"n_bins": n_bins, "sweeps_per_step": self.sweeps_per_step, "backend": "cuda"})
+                for i in range(self.n_samples)]
 
     def spins(self) -> np.ndarray:
         """(samples, 2, m, N) spins per temperature index (critmc site order)."""
         w = to_host(self.words, np.uint32)
         return np.stack([_unpack_words(w[i], len(self.temperatures), self.lattice.shape)
                          for i in range(self.n_samples)])
+
+
+_OUT_KEYS = ("acc", "swap_acc", "swap_try", "label_hist", "trips")
+
+
+class _EaSize(ctypes.Structure):
+    """Mirror of ``critmc_ea_size`` in include/critmc_b200.h."""
+
+    _fields_ = [("words", ctypes.c_void_p), ("jneg", ctypes.c_void_p), ("keys", ctypes.c_void_p),
+                ("conf_at", ctypes.c_void_p), ("labels", ctypes.c_void_p), ("acc", ctypes.c_void_p),
+                ("swap_acc", ctypes.c_void_p), ("swap_try", ctypes.c_void_p), ("label_hist", ctypes.c_void_p),
+                ("trips", ctypes.c_void_p), ("lx", ctypes.c_int32), ("ly", ctypes.c_int32),
+                ("lz", ctypes.c_int32), ("n_samples", ctypes.c_int32)]
+
+
+class MultiSizeCampaign:
+    """Samples of several lattice sizes advanced by ONE persistent launch.
+
+    ``campaigns``: one ``SpinGlassCampaign`` per size, all with the same
+    temperatures, dimension and sweeps per step.  Thread blocks take (size,
+    sample) items from a queue, largest lattices first, so the uneven sizes
+    share the GPU without one launch per size; each sample's result equals
+    its own campaign's ``run``.
+    """
+
+    def __init__(self, campaigns: list["SpinGlassCampaign"]):
+        if not campaigns:
+            raise ValueError("no campaigns")
+        c0 = campaigns[0]
+        for c in campaigns[1:]:
+            if (not np.array_equal(c.temperatures, c0.temperatures) or c.lattice.dim != c0.lattice.dim
+                    or c.sweeps_per_step != c0.sweeps_per_step or c.device != c0.device):
+                raise ValueError("campaigns must share temperatures, dimension, sweeps per step and device")
+            if c.step != c0.step:
+                raise ValueError("campaigns must be at the same PT step")
+        self.campaigns = campaigns
+        self.device = c0.device
+        self._dkeys = [torch.from_numpy(c.keys.reshape(-1).view(np.int32).copy()).to(self.device)
+                       for c in campaigns]
+        total = sum(c.n_samples for c in campaigns)
+        self._bytes = _lib.lib().critmc_ea_campaign_buffer_bytes(len(campaigns), total)
+        self._buffer = torch.empty(self._bytes, dtype=torch.uint8, device=self.device)
+        self._staging = torch.empty(self._bytes, dtype=torch.uint8, pin_memory=True)
+
+    @property
+    def n_updates_per_step(self) -> int:
+        """Attempted spin updates of one PT step (every temperature of both replica sets)."""
+        return sum(c.n_samples * 2 * len(c.temperatures) * c.lattice.n_sites * c.sweeps_per_step
+                   for c in self.campaigns)
+
+    def launch(self, n_bins: int, n_steps: int | None = None, stream=None) -> list[dict]:
+        """Enqueue ``n_steps`` PT steps of every sample (no synchronisation); returns the outputs."""
+        n_steps = (1 << n_bins) - 1 if n_steps is None else int(n_steps)
+        c0 = self.campaigns[0]
+        outs = [c._outputs(n_bins) for c in self.campaigns]
+        sizes = (_EaSize * len(self.campaigns))()
+        for z, c, o, k in zip(sizes, self.campaigns, outs, self._dkeys):
+            dims = tuple(c.lattice.shape) + (1,) * (3 - c.lattice.dim)
+            z.words, z.jneg, z.keys = ptr(c.words), ptr(c.jneg), ptr(k)
+            z.conf_at, z.labels = ptr(c.conf_at), ptr(c.labels)
+            z.acc, z.swap_acc, z.swap_try = ptr(o["acc"]), ptr(o["swap_acc"]), ptr(o["swap_try"])
+            z.label_hist, z.trips = ptr(o["label_hist"]), ptr(o["trips"])
+            z.lx, z.ly, z.lz = dims
+            z.n_samples = c.n_samples
+        _lib.call("critmc_ea_campaign_run", ctypes.cast(sizes, ctypes.c_void_p), len(self.campaigns),
+                  c0.lattice.dim, len(c0.temperatures), c0.betas.ctypes.data, ptr(c0.swap_thr), SWAP_WIDTH,
+                  c0.step, n_steps, n_bins, c0.sweeps_per_step, ptr(self._buffer), self._bytes,
+                  self._staging.data_ptr(), stream if stream is not None else stream_handle(self.device))
+        for c in self.campaigns:
+            c.step += n_steps
+        return outs
+
+    def run(self, n_bins: int, n_steps: int | None = None) -> list[list[TemperingRun]]:
+        """Run every size; returns one list of ``TemperingRun`` per campaign."""
+        t0 = time.perf_counter()
+        outs = self.launch(n_bins, n_steps)
+        torch.cuda.synchronize(self.device)
+        wall = time.perf_counter() - t0
+        return [c._collect(o, n_bins, wall) for c, o in zip(self.campaigns, outs)]
 
 
 class ParallelTempering:

@@ -223,6 +223,34 @@ int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_t dim, int3
                          int32_t n_bins, int32_t sweeps_per_step, double* acc, int64_t* swap_acc,
                          int64_t* swap_try, int64_t* label_hist, int64_t* trips, void* stream);
 
+/* A campaign of several lattice sizes (same dim and temperatures) in ONE
+ * persistent launch: thread blocks take (size, sample) items from a queue,
+ * largest lattices first, and run critmc_ea_pt_run's steps on each; results
+ * equal critmc_ea_pt_run per size.  sizes: HOST array; their keys are DEVICE
+ * arrays [n_samples][2][2].  buffer: device memory of
+ * critmc_ea_campaign_buffer_bytes(n_sizes, total samples) bytes; staging:
+ * NULL or pinned host memory of the same size (the call fills it and copies
+ * from it asynchronously).  No counterpart in critmc (one process per
+ * sample, src/critmc/runner.py:154-223).                                     */
+typedef struct {
+  uint32_t* words;
+  const uint8_t* jneg;
+  const uint32_t* keys;
+  uint8_t* conf_at;
+  uint8_t* labels;
+  double* acc;
+  int64_t* swap_acc;
+  int64_t* swap_try;
+  int64_t* label_hist;
+  int64_t* trips;
+  int32_t lx, ly, lz, n_samples;
+} critmc_ea_size;
+int64_t critmc_ea_campaign_buffer_bytes(int32_t n_sizes, int64_t total_samples);
+int32_t critmc_ea_campaign_run(const critmc_ea_size* sizes, int32_t n_sizes, int32_t dim, int32_t m,
+                               const double* betas, const uint32_t* swap_thr, int32_t swap_width,
+                               uint32_t t0, int32_t n_steps, int32_t n_bins, int32_t sweeps_per_step,
+                               void* buffer, int64_t buffer_bytes, void* staging, void* stream);
+
 /* ---- heterogeneous work items (continuous batching, serving) --------------
  * One item advances one chain by n_meas schedule applications: any model and
  * lattice size, its own beta, key and sweep counter.  critmc_run_items runs

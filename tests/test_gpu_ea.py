@@ -79,3 +79,34 @@ def test_same_seed_same_couplings_and_spins_as_critmc_convention(cuda):
     np.testing.assert_array_equal(ea.couplings, make_rng(77).choice([-1.0, 1.0], size=lat.n_bonds))
     with pytest.raises(ValueError):
         EdwardsAnderson(lat, disorder="gaussian", seed=1)
+
+
+def _campaigns(sizes, temps, n_samples, cuda, sps=1):
+    out = []
+    for L in sizes:
+        lat = cubic(L)
+        samples = [EdwardsAnderson(lat, disorder="bimodal", seed=1000 * L + i) for i in range(n_samples)]
+        out.append(SpinGlassCampaign(samples, temps, seeds=[7000 * L + i for i in range(n_samples)],
+                                     sweeps_per_step=sps, device=cuda))
+    return out
+
+
+def test_multi_size_campaign_equals_per_size_runs(cuda):
+    """Uneven sizes in one persistent launch give each size's own results, over two calls."""
+    from critmc_b200.glass import MultiSizeCampaign
+
+    temps = geometric_temperatures(0.5, 2.0, 32)
+    sizes = (4, 6, 8, 10, 12, 16)
+    alone = _campaigns(sizes, temps, 5, cuda)
+    mixed = MultiSizeCampaign(_campaigns(sizes, temps, 5, cuda))
+    for n_bins in (5, 3):
+        want = [c.run(n_bins) for c in alone]
+        got = mixed.run(n_bins)
+        for runs_a, runs_b in zip(want, got):
+            for a, b in zip(runs_a, runs_b):
+                np.testing.assert_array_equal(a.acc, b.acc)
+                np.testing.assert_array_equal(a.swap_rate, b.swap_rate)
+                np.testing.assert_array_equal(a.label_hist, b.label_hist)
+                np.testing.assert_array_equal(a.trips, b.trips)
+    for ca, cb in zip(alone, mixed.campaigns):
+        np.testing.assert_array_equal(ca.spins(), cb.spins())

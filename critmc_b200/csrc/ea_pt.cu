@@ -64,6 +64,57 @@ struct EaParams {
   uint32_t keys[EA_PSAMPLES][2][2];
 };
 
+// Bit-sliced (vertical) counters: v[p] holds bit p of one count per lane.
+// Add a 0..7 count given as bit planes c.
+template <int NP>
+__device__ __forceinline__ void vadd3(uint32_t (&v)[NP], const Count3& c) {
+  uint32_t carry = 0;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const uint32_t x = p == 0 ? c.b0 : (p == 1 ? c.b1 : (p == 2 ? c.b2 : 0u));
+    const uint32_t a = v[p];
+    v[p] = a ^ x ^ carry;
+    carry = (a & x) | (carry & (a ^ x));
+  }
+}
+
+// Add one bit per lane.
+template <int NP>
+__device__ __forceinline__ void vadd1(uint32_t (&v)[NP], uint32_t x) {
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const uint32_t a = v[p];
+    v[p] = a ^ x;
+    x &= a;
+  }
+}
+
+// Sum of the warp's vertical counters for count lane `lane` (every lane of the
+// warp takes part; each gets the total of its own lane index).
+// Transpose the warp's 32x32 bit matrix: bit i of the result in lane k is bit
+// k of lane i's word (recursive swap of off-diagonal blocks).
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+  const uint32_t lo[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    const int j = 16 >> t;
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~lo[t]) | ((y & ~lo[t]) >> j)) : ((x & lo[t]) | ((y & lo[t]) << j));
+  }
+  return x;
+}
+
+// Sum of the warp's vertical counters for count lane `lane` (every lane of the
+// warp takes part; each gets the total of its own lane index): after the
+// transpose, lane k holds bit k of every lane's plane.
+template <int NP>
+__device__ __forceinline__ int vreduce(const uint32_t (&v)[NP], int lane) {
+  int mine = 0;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) mine += __popc(transpose32(v[p], lane)) << p;
+  return mine;
+}
+
 // threshold bit plane for the undecided lanes (counts 0 .. z/2-1)
 template <int Z>
 __device__ __forceinline__ uint32_t ea_tbits(const EaCommon& C, const Count3& c, int q) {
@@ -130,6 +181,8 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   __shared__ int ecnt[2][32];  // unsatisfied bonds per set and temperature
   __shared__ int qlcnt[32];    // agreeing bonds of the overlap field
   __shared__ int sigma[2][32];
+  __shared__ int es[2][32];         // energies per set and temperature slot during the swaps
+  __shared__ uint32_t swu[2][32];   // swap uniforms of the step
   __shared__ int conf[2][32], lab[2][32];
   __shared__ double acc_s[32][EA_NOBS];
   __shared__ unsigned long long sw_acc[32], sw_try[32], lhist[32][2], trip[2];
@@ -238,74 +291,85 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     if (tid < 64) ecnt[tid >> 5][tid & 31] = 0;
     __syncthreads();
     {
-      int ca = 0, cb = 0;
-      for (uint32_t s = warp; s < g.slots; s += EA_WARPS) {  // colour-0 sites see every bond once
+      // colour-0 sites see every bond once; at most 8 sites per thread x z <= 6 bonds < 64
+      uint32_t va[6] = {0, 0, 0, 0, 0, 0}, vb[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t s = tid; s < g.slots; s += EA_THREADS) {
         uint32_t w_s;
         Count3 cnt;
         ea_site<Z>(g, lat, jn, 0, 0, s, w_s, cnt);
-        ca += ((cnt.b0 >> lane) & 1) + 2 * ((cnt.b1 >> lane) & 1) + 4 * ((cnt.b2 >> lane) & 1);
+        vadd3(va, cnt);
         ea_site<Z>(g, lat, jn, 1, 0, s, w_s, cnt);
-        cb += ((cnt.b0 >> lane) & 1) + 2 * ((cnt.b1 >> lane) & 1) + 4 * ((cnt.b2 >> lane) & 1);
+        vadd3(vb, cnt);
       }
-      atomicAdd(&ecnt[0][lane], ca);
-      atomicAdd(&ecnt[1][lane], cb);
+      atomicAdd(&ecnt[0][lane], vreduce(va, lane));
+      atomicAdd(&ecnt[1][lane], vreduce(vb, lane));
     }
     __syncthreads();
-    // ---- replica exchange, one thread per set (critmc glass.py:128-152) -----
-    if (tid == 0 || tid == 32) {
-      const int r = tid >> 5;
-      const long long n_bonds = (long long)n_sites * DIM;
-      long long e[32];
-      for (int k = 0; k < m; ++k) {
-        e[k] = -(n_bonds - 2LL * ecnt[r][k]);
-        sigma[r][k] = k;
+    // ---- replica exchange, one warp per set (critmc glass.py:128-152): its lanes
+    // draw the swap uniforms, lane 0 walks k = 0..m-2 in order ---------------
+    if (warp < 2) {
+      const int r = warp;
+      const int n_bonds = (int)n_sites * DIM;
+      if (lane < m) {
+        es[r][lane] = -(n_bonds - 2 * ecnt[r][lane]);
+        sigma[r][lane] = lane;
       }
-      const uint32_t k0 = key[r][0], k1 = key[r][1];
-      for (int k = 0; k < m - 1; ++k) {
-        // betas ascend hot -> cold, so x = (b_k - b_k+1)(E_k - E_k+1) >= 0 iff E_k <= E_k+1
-        const long long de = e[k] - e[k + 1];
-        bool ok = de <= 0;
-        if (!ok) {
-          long long j = de / 4;
-          if (j > C.swap_width - 1) j = C.swap_width - 1;
-          const uint32_t u = critmc_philox4x32((uint32_t)k, step, CRITMC_TAG_SWAP | ((uint32_t)r << 16), 0u, k0, k1).v[0];
-          ok = u < C.swap_thr[(size_t)k * C.swap_width + j];
+      if (lane < m - 1)
+        swu[r][lane] = critmc_philox4x32((uint32_t)lane, step, CRITMC_TAG_SWAP | ((uint32_t)r << 16), 0u,
+                                         key[r][0], key[r][1]).v[0];
+      __syncwarp();
+      if (lane == 0) {
+        for (int k = 0; k < m - 1; ++k) {
+          // betas ascend hot -> cold, so x = (b_k - b_k+1)(E_k - E_k+1) >= 0 iff E_k <= E_k+1
+          const int de = es[r][k] - es[r][k + 1];
+          bool ok = de <= 0;
+          if (!ok) {
+            int j = de / 4;
+            if (j > C.swap_width - 1) j = C.swap_width - 1;
+            ok = swu[r][k] < C.swap_thr[(size_t)k * C.swap_width + j];
+          }
+          atomicAdd(&sw_try[k], 1ULL);
+          if (ok) {
+            atomicAdd(&sw_acc[k], 1ULL);
+            const int te = es[r][k];
+            es[r][k] = es[r][k + 1];
+            es[r][k + 1] = te;
+            const int tc = conf[r][k];
+            conf[r][k] = conf[r][k + 1];
+            conf[r][k + 1] = tc;
+            const int ts = sigma[r][k];
+            sigma[r][k] = sigma[r][k + 1];
+            sigma[r][k + 1] = ts;
+          }
         }
-        atomicAdd(&sw_try[k], 1ULL);
-        if (ok) {
-          atomicAdd(&sw_acc[k], 1ULL);
-          const long long te = e[k];
-          e[k] = e[k + 1];
-          e[k + 1] = te;
-          const int tc = conf[r][k];
-          conf[r][k] = conf[r][k + 1];
-          conf[r][k + 1] = tc;
-          const int ts = sigma[r][k];
-          sigma[r][k] = sigma[r][k + 1];
-          sigma[r][k + 1] = ts;
-        }
+        const int hot = conf[r][0], cold = conf[r][m - 1];
+        // labels are indexed by configuration: lab[r][c] for configuration c
+        if (lab[r][hot] == 2) atomicAdd(&trip[r], 1ULL);
+        lab[r][hot] = 1;
+        if (lab[r][cold] == 1) atomicAdd(&trip[r], 1ULL);
+        lab[r][cold] = 2;
       }
-      for (int k = 0; k < m; ++k) ecnt[r][k] = (int)((e[k] + n_bonds) / 2);  // permuted counts
-      const int hot = conf[r][0], cold = conf[r][m - 1];
-      // labels are indexed by configuration: lab[r][c] for configuration c
-      if (lab[r][hot] == 2) atomicAdd(&trip[r], 1ULL);
-      lab[r][hot] = 1;
-      if (lab[r][cold] == 1) atomicAdd(&trip[r], 1ULL);
-      lab[r][cold] = 2;
-      for (int k = 0; k < m; ++k) {
-        const int l = lab[r][conf[r][k]];
-        if (l == 1) atomicAdd(&lhist[k][0], 1ULL);
-        else if (l == 2) atomicAdd(&lhist[k][1], 1ULL);
+      __syncwarp();
+      if (lane < m) {
+        ecnt[r][lane] = (es[r][lane] + n_bonds) / 2;  // permuted counts
+        const int l = lab[r][conf[r][lane]];
+        if (l == 1) atomicAdd(&lhist[lane][0], 1ULL);
+        else if (l == 2) atomicAdd(&lhist[lane][1], 1ULL);
       }
     }
     __syncthreads();
     // ---- move configurations between lanes: new bit k = old bit sigma[k] ----
-    for (uint32_t j = warp; j < 2 * n_sites; j += EA_WARPS) {
-      const int r = j >= n_sites;
-      const uint32_t w = lat[j];
-      const int src = sigma[r][lane];
-      const uint32_t nw = __ballot_sync(0xffffffffu, lane < m && ((w >> src) & 1u));
-      if (lane == 0) lat[j] = nw;
+    // (32 words per warp: transpose, take row sigma[k] into row k, transpose back)
+    for (int r = 0; r < 2; ++r) {
+      const int src = lane < m ? sigma[r][lane] : lane;
+      for (uint32_t base = (uint32_t)warp * 32; base < n_sites; base += EA_WARPS * 32) {
+        const uint32_t i = base + (uint32_t)lane;
+        uint32_t x = i < n_sites ? lat[(size_t)r * n_sites + i] : 0u;
+        x = transpose32(x, lane);
+        const uint32_t y = __shfl_sync(0xffffffffu, x, src);
+        x = transpose32(lane < m ? y : 0u, lane);
+        if (i < n_sites) lat[(size_t)r * n_sites + i] = x;
+      }
     }
     __syncthreads();
     // ---- measurement (critmc glass.py:57-77, :153-163) -----------------------
@@ -313,35 +377,36 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     if (tid < 32) qlcnt[tid] = 0;
     __syncthreads();
     {
-      int agree = 0;
-      for (uint32_t s = warp; s < g.slots; s += EA_WARPS) {
+      uint32_t vq[6] = {0, 0, 0, 0, 0, 0};  // agreeing bonds, at most 8 sites x z <= 6 per thread
+      for (uint32_t s = tid; s < g.slots; s += EA_THREADS) {
         int r, i;
         byte_row_index(g, s, r, i);
         uint32_t nb[Z];
         byte_neighbours<Z>(g, 0, r, i, nb);
         const uint32_t qs = qw[s];
+        uint32_t x[Z];
 #pragma unroll
-        for (int q = 0; q < Z; ++q) agree += (~(qs ^ qw[g.slots + nb[q]]) >> lane) & 1;
+        for (int q = 0; q < Z; ++q) x[q] = ~(qs ^ qw[g.slots + nb[q]]);
+        vadd3(vq, count_bits<Z>(x));
       }
-      atomicAdd(&qlcnt[lane], agree);
+      atomicAdd(&qlcnt[lane], vreduce(vq, lane));
     }
-    // per-plane overlap counts: warp w handles planes (d, x) = w, w + WARPS, ...
-    for (int pl = warp; pl < DIM * EA_MAX_L; pl += EA_WARPS) {
-      const int d = pl / EA_MAX_L, x0 = pl % EA_MAX_L;
-      if (x0 >= S.ext[d]) continue;
-      int cnt = 0;
+    // per-plane overlap counts: warp w handles planes (d, x) = w, w + WARPS, ...;
+    // its lanes split the plane's sites (at most 256 / 32 = 8 each)
+    for (int pl = warp; pl < DIM * S.ext[0]; pl += EA_WARPS) {
+      const int d = pl / S.ext[0], x0 = pl % S.ext[0];
       const int e1 = S.ext[d == 0 ? 1 : 0], e2 = DIM == 3 ? S.ext[d == 2 ? 1 : 2] : 1;
-      for (int u = 0; u < e1; ++u)
-        for (int v = 0; v < e2; ++v) {
-          int xyz[3] = {0, 0, 0};
-          xyz[d] = x0;
-          xyz[d == 0 ? 1 : 0] = u;
-          if (DIM == 3) xyz[d == 2 ? 1 : 2] = v;
-          const int col = (xyz[0] + xyz[1] + xyz[2]) & 1;
-          const uint32_t slot = (uint32_t)((xyz[1] + g.ly * xyz[2]) * g.hx + xyz[0] / 2);
-          cnt += (qw[(size_t)col * g.slots + slot] >> lane) & 1;
-        }
-      splane[(d * S.ext[0] + x0) * 32 + lane] = cnt;
+      uint32_t vp[4] = {0, 0, 0, 0};
+      for (int idx = lane; idx < e1 * e2; idx += 32) {
+        int xyz[3] = {0, 0, 0};
+        xyz[d] = x0;
+        xyz[d == 0 ? 1 : 0] = idx % e1;
+        if (DIM == 3) xyz[d == 2 ? 1 : 2] = idx / e1;
+        const int col = (xyz[0] + xyz[1] + xyz[2]) & 1;
+        const uint32_t slot = (uint32_t)((xyz[1] + g.ly * xyz[2]) * g.hx + xyz[0] / 2);
+        vadd1(vp, qw[(size_t)col * g.slots + slot]);
+      }
+      splane[(d * S.ext[0] + x0) * 32 + lane] = vreduce(vp, lane);
     }
     __syncthreads();
     if (tid < m) {

@@ -114,6 +114,66 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def ea_bench(dev, n_bins: int = 16, peak: float = 6650.0) -> dict:
+    """3D EA +-J campaign: L in {6, 8, 10, 12, 16}, 512 samples each, 2 replica sets x
+    32 temperatures geometric in [0.5, 2.0], one Metropolis sweep + one swap pass per
+    step, 2^n_bins - 1 steps, all sizes in ONE persistent launch."""
+    import torch
+
+    from critmc_b200 import cubic
+    from critmc_b200.glass import EdwardsAnderson, MultiSizeCampaign, SpinGlassCampaign, geometric_temperatures
+
+    temps = geometric_temperatures(0.5, 2.0, 32)
+    camps = []
+    for L in (6, 8, 10, 12, 16):
+        samples = [EdwardsAnderson(cubic(L), disorder="bimodal", seed=L * 100000 + i) for i in range(512)]
+        camps.append(SpinGlassCampaign(samples, temps, seeds=[L * 200000 + i for i in range(512)], device=dev))
+    mc = MultiSizeCampaign(camps)
+    mc.run(2, 3)  # warm-up (first launch, shared-memory attribute)
+    n_steps = (1 << n_bins) - 1
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    mc.launch(n_bins, n_steps)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    s = e0.elapsed_time(e1) * 1e-3
+    ups = mc.n_updates_per_step * n_steps / s / 1e9
+    return {"workload": "EA +-J 3D, L 6..16 x 512 samples x 2 x 32 temperatures, one launch",
+            "steps": n_steps, "seconds": s, "updates_per_ns": ups,
+            "hbm_gbs_at_0.625B": ups * 0.625, "hbm_frac": ups * 0.625 / peak}
+
+
+def on_bench(dev, steps: int = 40, peak: float = 6650.0) -> dict:
+    """O(n) batched: XY and Heisenberg on L in {64, 128, 256}, 128 chains each (16
+    temperatures in [0.7, 1.1] x 8 chains), each step 1 heat bath + 4 over-relaxation
+    sweeps (5N attempted updates); ``steps`` steps per size timed (the full run is
+    20,000)."""
+    import torch
+
+    from critmc_b200 import ON, hypercubic
+    from critmc_b200.on_models import ONEnsemble
+
+    temps = np.linspace(0.7, 1.1, 16)
+    sched = np.array([[2, 1], [5, 4]])
+    out = {}
+    for n, name, bpu in ((2, "xy", 16), (3, "heisenberg", 24)):
+        for L in (64, 128, 256):
+            ens = ONEnsemble(ON(hypercubic((L, L)), n), temps, 8, seed=L, device=dev)
+            ens.run(2, sched)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            ens.run(steps, sched)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            s = e0.elapsed_time(e1) * 1e-3
+            ups = ens.n_chains * ens.n_sites * 5 * steps / s / 1e9
+            out[f"{name}_L{L}"] = {"updates_per_ns": ups, "hbm_frac": ups * bpu / peak}
+            del ens
+    return out
+
+
 def cpu_sample(threads: int, sweeps: int = 1, L: int = L_HEAD) -> dict:
     """The C oracle (a plain-C port of critmc's Ising sweep with the same Philox
     stream) on `threads` host threads, one L x L chain per thread."""
@@ -349,10 +409,13 @@ def main() -> None:
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
         serving = serve_bench(dev, args.serve_requests, args.serve_rate)
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
+        extras["on_batched"] = on_bench(dev, peak=peaks()[0])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(min(32, os.cpu_count() or 1))
+        cpu = cpu_sample(min(32, os.cpu_count() or 1), sweeps=10)
 
     if rank == 0:
         line = {

@@ -277,7 +277,7 @@ static int byte_launch(ByteParams& P, const uint32_t* keys, cudaStream_t s) {
     P.chain0 = c0;
     std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
     auto launch = [&](auto kern) {
-      if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (smem > 0) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  // static + dynamic may pass 48 KiB
       kern<<<nc, threads, smem, s>>>(P);
     };
     switch (P.g.dim) {
@@ -285,7 +285,7 @@ static int byte_launch(ByteParams& P, const uint32_t* keys, cudaStream_t s) {
       case 2: launch(byte_run_kernel<MODEL, 4>); break;
       default: launch(byte_run_kernel<MODEL, 6>); break;
     }
-    if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+    if (int e_ = cuda_check("launch")) return e_;
   }
   return CRITMC_OK;
 }
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_i
 }
 
 int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
-  if (smem > 48 * 1024 &&
+  if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(byte_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
   int per_sm = 0;
@@ -477,7 +477,7 @@ int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t s
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
   byte_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 

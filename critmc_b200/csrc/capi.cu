@@ -22,6 +22,13 @@ int cuda_fail(const char* what) {
   return CRITMC_ERR_CUDA;
 }
 
+int cuda_check(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return CRITMC_OK;
+  std::snprintf(g_error, sizeof(g_error), "%s: %s", what, cudaGetErrorString(e));
+  return CRITMC_ERR_CUDA;
+}
+
 namespace {
 
 struct GraphEntry {

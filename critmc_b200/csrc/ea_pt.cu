@@ -672,7 +672,7 @@ extern "C" int32_t critmc_ea_pt_run(uint32_t* words, const uint8_t* jneg, int32_
     };
     if (dim == 2) launch(ea_pt_kernel<4>);
     else launch(ea_pt_kernel<6>);
-    if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+    if (int e_ = cuda_check("launch")) return e_;
   }
   return CRITMC_OK;
 }
@@ -742,7 +742,7 @@ extern "C" int32_t critmc_ea_campaign_run(const critmc_ea_size* sizes, int32_t n
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
     const long long grid = std::max(1LL, std::min<long long>(total, (long long)std::max(1, per_sm) * sms));
     kern<<<(unsigned)grid, EA_THREADS, smem, s>>>(P);
-    return cudaGetLastError() == cudaSuccess ? CRITMC_OK : cuda_fail("launch");
+    return cuda_check("launch");
   };
   return dim == 2 ? launch(ea_campaign_kernel<4>) : launch(ea_campaign_kernel<6>);
 }

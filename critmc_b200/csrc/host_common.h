@@ -20,6 +20,8 @@ inline int fail(int code, const char* msg) {
 
 // record the pending CUDA error (clearing it) and return CRITMC_ERR_CUDA
 int cuda_fail(const char* what);
+// CRITMC_OK if no CUDA error is pending, else record and clear it (CRITMC_ERR_CUDA)
+int cuda_check(const char* what);
 
 // A stream the library may capture into a CUDA graph: the caller's stream, or,
 // when the caller passed the legacy default stream, a per-thread private

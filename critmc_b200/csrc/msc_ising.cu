@@ -511,7 +511,7 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
   msc_finalize_kernel<<<n_chains, 256, 0, s>>>((const long long*)acc, (long long*)running,
                                                 (long long*)e_out, (long long*)m_out,
                                                 (long long*)aux_out, n_chains, n_meas);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return cs.finish();
 }
 
@@ -531,7 +531,7 @@ extern "C" int32_t critmc_ising_msc_measure(const uint32_t* spins, int32_t dim, 
   else msc_measure_kernel<6><<<grid, 256, 0, s>>>(spins, g, (unsigned long long*)out);
   const long long n_sites = (long long)lx * ly * (dim == 3 ? lz : 1);
   msc_measure_final<<<(n_chains + 127) / 128, 128, 0, s>>>((unsigned long long*)out, n_chains, n_sites, 2 * dim);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 
@@ -548,7 +548,7 @@ extern "C" int32_t critmc_ising_msc_init(uint32_t* spins, int32_t dim, int32_t l
   cudaStream_t s = (cudaStream_t)stream;
   const dim3 grid(std::min<uint32_t>(2048, (2 * g.words + 255) / 256), n_chains);
   msc_init_kernel<<<grid, 256, 0, s>>>(spins, g, keys, start);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 
@@ -683,7 +683,7 @@ extern "C" int32_t critmc_ising_msc_run_noalloc(uint32_t* spins, int32_t dim, in
   msc_finalize_kernel<<<n_chains, 256, 0, s>>>((const long long*)acc, (long long*)running,
                                                 (long long*)e_out, (long long*)m_out,
                                                 (long long*)aux_out, n_chains, n_meas);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 
@@ -847,7 +847,7 @@ __global__ void __launch_bounds__(ITEM_THREADS) msc_items_kernel(const critmc_it
 }
 
 int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
-  if (smem > 48 * 1024 &&
+  if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(msc_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
   int per_sm = 0;
@@ -857,7 +857,7 @@ int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t sm
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
   msc_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 

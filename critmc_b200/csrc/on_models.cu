@@ -601,7 +601,7 @@ static int on_grid_launches(OnGridParams& P, const int* codes, const int* reps, 
   const int fb = (int)std::min<size_t>(1184, (total + 255) / 256);
   on_grid_finalize<N, Z><<<std::max(1, fb), 256, 0, s>>>(acc, n_chains, n_meas, e_out, m_out, sc_out, ss_out,
                                                          aux_out);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 
@@ -668,7 +668,7 @@ extern "C" int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t 
     P.chain0 = c0;
     std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
     auto launch = [&](auto kern) {
-      if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (smem > 0) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  // static + dynamic may pass 48 KiB
       kern<<<nc, threads, smem, s>>>(P);
     };
     const int key = n * 10 + dim;
@@ -680,7 +680,7 @@ extern "C" int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t 
       case 32: launch(on_run_kernel<3, 4>); break;
       default: launch(on_run_kernel<3, 6>); break;
     }
-    if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+    if (int e_ = cuda_check("launch")) return e_;
   }
   return CRITMC_OK;
 }
@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(ON_THREADS) on_items_kernel(const critmc_item*
 template <int N, int Z>
 static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
   auto kern = on_items_kernel<N, Z>;
-  if (smem > 48 * 1024 &&
+  if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
   int per_sm = 0;
@@ -820,7 +820,7 @@ static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, 
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
   kern<<<grid, ON_THREADS, smem, s>>>(items, n, queue, smem);
-  if (cudaGetLastError() != cudaSuccess) return cuda_fail("launch");
+  if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 

@@ -71,3 +71,69 @@ class ONChain:
         self.sweep += int(sched[:, 1].sum()) * n_meas
         return {"E": to_host(e)[0], "M": to_host(m)[0], "stiff_c": to_host(sc)[0],
                 "stiff_s": to_host(ss)[0], "aux": to_host(aux)[0]}
+
+
+class ONEnsemble:
+    """Many O(n) chains of one lattice advanced by one ``critmc_on_run`` call.
+
+    ``temperatures`` x ``chains_per_temperature`` chains (chains of one
+    temperature form a group), uniform random unit-vector starts; chain ``c``
+    of temperature index ``t`` draws its start and Philox key from
+    ``make_rng(seed, "on", n, L, t, c)``, so its trajectory does not depend on
+    what it is batched with.  Replaces critmc's process pool over independent
+    chains (src/critmc/runner.py:154-223) for the sampling step.
+    """
+
+    def __init__(self, model, temperatures, chains_per_temperature: int, *, seed: int = 0, step: float = 1.0,
+                 device=None):
+        from .rng import make_rng, philox_key
+
+        self.device = require_cuda(device)
+        self.model = model
+        self.n = model.n
+        self.shape = tuple(model.lattice.shape)
+        self.dims = self.shape + (1,) * (3 - len(self.shape))
+        self.betas = np.ascontiguousarray(1.0 / np.asarray(temperatures, dtype=np.float64))
+        if not 1 <= len(self.betas) <= 16:
+            raise ValueError("between 1 and 16 temperatures per ensemble")
+        self.chains_per_temperature = int(chains_per_temperature)
+        self.n_chains = len(self.betas) * self.chains_per_temperature
+        keys, comps = [], []
+        L = self.shape[0]
+        for t in range(len(self.betas)):
+            for c in range(self.chains_per_temperature):
+                rng = make_rng(seed, "on", self.n, L, t, c)
+                s = model.initial_state("random", rng).astype(np.float32)
+                keys.append(philox_key(rng))
+                comps.append(np.stack([cb_pack(s[:, k], self.shape) for k in range(self.n)]))
+        self.keys = np.ascontiguousarray(np.stack(keys), dtype=np.uint32)
+        self.spins = torch.from_numpy(np.ascontiguousarray(np.stack(comps))).to(self.device)
+        self.steps = np.full(len(self.betas), float(step))
+        self.sweep = 0
+
+    @property
+    def n_sites(self) -> int:
+        return int(np.prod(self.shape))
+
+    def run(self, n_meas: int, schedule, stream=None) -> dict[str, torch.Tensor]:
+        """Apply ``schedule`` ((code, reps) rows) ``n_meas`` times to every chain; device outputs."""
+        dev, n, dim = self.device, self.n, len(self.shape)
+        sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+        nc = self.n_chains
+        out = {"E": torch.empty((nc, n_meas), dtype=torch.float64, device=dev),
+               "M": torch.empty((nc, n_meas, n), dtype=torch.float64, device=dev),
+               "stiff_c": torch.empty((nc, n_meas, dim), dtype=torch.float64, device=dev),
+               "stiff_s": torch.empty((nc, n_meas, dim), dtype=torch.float64, device=dev),
+               "aux": torch.empty((nc, n_meas, N_AUX), dtype=torch.int64, device=dev)}
+        lx, ly, lz = self.dims
+        _lib.call("critmc_on_run", ptr(self.spins), dim, lx, ly, lz, n, nc, self.keys.ctypes.data,
+                  self.betas.ctypes.data, self.steps.ctypes.data, len(self.betas), self.sweep,
+                  sched.ctypes.data, len(sched), n_meas, *(ptr(out[k]) for k in ("E", "M", "stiff_c", "stiff_s")),
+                  ptr(out["aux"]), stream if stream is not None else stream_handle(dev))
+        self.sweep += int(sched[:, 1].sum()) * n_meas
+        return out
+
+    def chain(self, i: int) -> np.ndarray:
+        """Configuration of chain ``i`` in critmc's site order, shape (N, n)."""
+        comps = to_host(self.spins[i])
+        return np.stack([cb_unpack(comps[k], self.shape) for k in range(self.n)], axis=1).astype(np.float64)

@@ -25,6 +25,7 @@ CASES = [
     ((8, 6, 4), 3, [[2, 1], [5, 1]], 0.7),
     ((32,), 2, [[2, 1], [0, 1], [5, 2]], 1.1),
     ((128, 130), 2, [[2, 1]], 1.0),  # larger than shared memory: updated in HBM
+    ((64, 64), 3, [[0, 1]], 0.9),  # 48 KiB lattice: with the block's static arrays above the default limit
 ]
 
 
@@ -98,3 +99,24 @@ def test_metropolis_step_is_tuned(cuda):
     assert 0.001 <= info["step"] <= 10
     acc = sim.run(500).meta["acceptance"]
     assert 0.3 < acc < 0.7
+
+
+def test_on_ensemble_chain_equals_single_chain(cuda):
+    """A chain of the batched ensemble gives the series of the same chain run alone."""
+    from critmc_b200.on_models import ONEnsemble
+    from critmc_b200.rng import make_rng, philox_key
+
+    model = ON(hypercubic((32, 32)), 2)
+    temps = np.linspace(0.7, 1.1, 4)
+    ens = ONEnsemble(model, temps, 3, seed=9, device=cuda)
+    sched = np.array([[2, 1], [5, 4]])
+    out = ens.run(6, sched)
+    for t, c in ((0, 0), (2, 1), (3, 2)):
+        rng = make_rng(9, "on", 2, 32, t, c)
+        s0 = model.initial_state("random", rng).astype(np.float32)
+        ch = ONChain(model, s0, philox_key(rng), cuda, lane="block")
+        raw = ch.advance({"step": 1.0}, 1.0 / temps[t], sched, 6)
+        i = t * 3 + c
+        np.testing.assert_array_equal(out["E"][i].cpu().numpy(), raw["E"])
+        np.testing.assert_array_equal(out["M"][i].cpu().numpy(), raw["M"])
+        np.testing.assert_array_equal(ens.chain(i), ch.fetch())

@@ -261,7 +261,7 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0) -> dict:
         lat.append(res.latency)
         upd[0] += res.updates
 
-    srv = Server(dev, keep_series=False, on_result=lambda r: None)
+    srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto")
     # warm-up: one short request per (model, size) of the mix builds the
     # lattice cache, the library streams and the kernels' first launches
     shapes = sorted({(r.model, r.L) for r in reqs})
@@ -344,7 +344,9 @@ def main() -> None:
         print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate)}), flush=True)
         return
 
-    ens = IsingEnsemble(L_HEAD, BETAS, CHAINS_PER_BETA, seed=1000 + rank, device=dev)
+    # launch shape (rows per thread, inline planes) from the autotuner; results do not depend on it
+    ens = IsingEnsemble(L_HEAD, BETAS, CHAINS_PER_BETA, seed=1000 + rank, device=dev, tune=True)
+    tuning = ens.tuning
     n_upd = ens.n_chains * ens.n_sites  # per step and rank
     for _ in range(args.warmup):
         ens.run(1, "metropolis", host=False)
@@ -429,6 +431,7 @@ def main() -> None:
                        "l2": "inputs larger than L2 (384 MiB of spins per GPU)"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "gpu_launches": args.steps * (1 + launches_per_step + 1),
+            "tuning": tuning,
             "clocks": clk.summary(), "extras": extras, "serving": serving,
         }
         print(json.dumps(line), flush=True)

@@ -396,6 +396,9 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
     if (reps < 1) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be positive");
     sweeps_per_meas += reps;
   }
+  const int run_code = (mode >> 8) & 0xF;  // tuning: rows walked per thread, 2^(code-1); 0 = automatic
+  if ((mode & ~0xFFF) || run_code > 6) return fail(CRITMC_ERR_INVALID, "mode: bits 8..11 must be 0..6, no higher bits");
+  mode &= 0xFF;
   if (mode == 0) mode = 3;
   if (mode != 1 && mode != 3) return fail(CRITMC_ERR_UNSUPPORTED, "mode must be 0, 1 or 3");
   if (n_meas == 0) return CRITMC_OK;
@@ -430,6 +433,7 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
   const long long col_threads = (long long)n_chains * g.wc * g.rows;
   int run = 8;
   while (run > 1 && col_threads / run < 148LL * 1536) run /= 2;
+  if (run_code) run = 1 << (run_code - 1);
 
   static thread_local MscParams P[2];
   for (int slot = 0; slot < 2; ++slot) {

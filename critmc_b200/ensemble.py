@@ -40,7 +40,7 @@ class IsingEnsemble:
 
     def __init__(self, lattice: Lattice | int, betas, chains_per_beta: int, *, h: float = 0.0,
                  seed: int = 0, start: str = "random", device=None, mode: int = 0,
-                 k_inline: int = 8):
+                 k_inline: int = 8, tune: bool = False):
         self.lattice = square(lattice) if isinstance(lattice, int) else lattice
         shape = tuple(self.lattice.shape)
         if not (_msc_ok(shape) and self.lattice.bipartite):
@@ -73,6 +73,14 @@ class IsingEnsemble:
         self.tables = np.ascontiguousarray(np.stack([self.model.tables(b)[0] for b in self.betas]))
         self.sweep = 0
         self._scratch = None
+        self.tuning = None
+        if tune:
+            # launch shape from the autotuner (cached per GPU, shape, batch): results do not change
+            from .autotune import msc_mode, tune_msc
+
+            self.tuning = tune_msc(shape, self.n_chains, beta=self.betas[0], h=h, device=self.device)
+            self.mode = msc_mode(self.tuning["run"], self.tuning["mode"])
+            self.k_inline = self.tuning["k_inline"]
 
     @property
     def n_sites(self) -> int:

@@ -279,7 +279,7 @@ class Server:
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
                  tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
-                 keep_state: bool = False, grid_streams: int = 32, on_result=None):
+                 keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None):
         self.device = require_cuda(device)
         free, _ = torch.cuda.mem_get_info(self.device)
         cap = max(0, free - reserve - 2 * arena_bytes)
@@ -307,6 +307,12 @@ class Server:
         self.arena = _Arena(int(arena_bytes), self.device)
         self.grid_scratch: dict[int, torch.Tensor] = {}
         self.costs = dict(COSTS)
+        if costs == "auto":  # the autotuner's measured cost model (cached per GPU)
+            from .autotune import calibrate_serving
+
+            self.costs.update(calibrate_serving(self.device))
+        elif costs is not None:
+            self.costs.update(costs)
         self.ticks = 0
         self.gpu_seconds = 0.0
         self.updates_done = 0

@@ -86,7 +86,9 @@ int32_t critmc_ising_class_table(int32_t algo, int32_t z, double beta, double h,
  * hold critmc_ising_msc_scratch_bytes(n_chains, n_meas) bytes of device
  * memory.  schedule is a HOST array of n_rows (code, reps) pairs; sweep k of
  * the call uses sweep index sweep0 + k of every chain.
- * mode: 0 auto, 1 one launch per half-sweep, 3 = 1 replayed as CUDA graphs.
+ * mode: 0 auto, 1 one launch per half-sweep, 3 = 1 replayed as CUDA graphs;
+ * plus, in bits 8..11, v = 1..6 for 2^(v-1) rows walked per thread (0 =
+ * automatic).  Both are tuning knobs (critmc_b200.autotune picks them).
  * k_inline: 4 or 8 acceptance planes resolved inline (tuning only; the
  * results do not depend on it).                                            */
 int64_t critmc_ising_msc_scratch_bytes(int32_t n_chains, int32_t n_meas);

@@ -174,6 +174,48 @@ def on_bench(dev, steps: int = 40, peak: float = 6650.0) -> dict:
     return out
 
 
+def small_case(dev, case: str) -> dict:
+    """A small, short case of one secondary kernel: one warm-up launch, then one timed launch.
+
+    ea-small: the EA campaign kernel on L in {6, 8, 10, 12, 16} x 64 samples x 2 x 32
+    temperatures, 31 steps.  on-small: the O(n) block kernel on 128 XY chains of
+    128 x 128 (16 temperatures x 8), 2 steps of 1 heat bath + 4 over-relaxation.
+    """
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if case == "ea-small":
+        from critmc_b200 import cubic
+        from critmc_b200.glass import EdwardsAnderson, MultiSizeCampaign, SpinGlassCampaign, geometric_temperatures
+
+        temps = geometric_temperatures(0.5, 2.0, 32)
+        camps = [SpinGlassCampaign([EdwardsAnderson(cubic(L), disorder="bimodal", seed=L * 1000 + i)
+                                    for i in range(64)], temps, seeds=[L * 2000 + i for i in range(64)],
+                                   device=dev) for L in (6, 8, 10, 12, 16)]
+        mc = MultiSizeCampaign(camps)
+        mc.launch(5, 31)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        mc.launch(5, 31)
+        e1.record()
+        units = mc.n_updates_per_step * 31
+    else:
+        from critmc_b200 import ON, hypercubic
+        from critmc_b200.on_models import ONEnsemble
+
+        ens = ONEnsemble(ON(hypercubic((128, 128)), 2), np.linspace(0.7, 1.1, 16), 8, seed=3, device=dev)
+        sched = np.array([[2, 1], [5, 4]])
+        ens.run(2, sched)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        ens.run(2, sched)
+        e1.record()
+        units = ens.n_chains * ens.n_sites * 5 * 2
+    torch.cuda.synchronize(dev)
+    s = e0.elapsed_time(e1) * 1e-3
+    return {"case": case, "seconds": s, "updates_per_ns": units / s / 1e9}
+
+
 def cpu_sample(threads: int, sweeps: int = 1, L: int = L_HEAD) -> dict:
     """The C oracle (a plain-C port of critmc's Ising sweep with the same Philox
     stream) on `threads` host threads, one L x L chain per thread."""
@@ -295,6 +337,8 @@ def main() -> None:
                     help="requests of the serving run (0 skips it; 1 GPU only)")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
+    ap.add_argument("--case", choices=["ea-small", "on-small"],
+                    help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -339,6 +383,10 @@ def main() -> None:
         e1.record(s)
         barrier()
         return max_over_ranks(e0.elapsed_time(e1))
+
+    if args.case:
+        print(json.dumps(small_case(dev, args.case)), flush=True)
+        return
 
     if args.serve_only:
         print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate)}), flush=True)

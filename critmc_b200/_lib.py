@@ -67,6 +67,19 @@ SIGNATURES: dict[str, tuple] = {
     ),
     "critmc_on_grid_scratch_bytes": (_I64, [_I32, _I32, _I32, _I32]),
     "critmc_graph_cache_set_capacity": (_I32, [_I32]),
+    "critmc_chain_create": (_I32, [_I32, _P, _I32, _D, _U32, _U32, ctypes.c_uint64, _I32, _P, _P]),
+    "critmc_chain_destroy": (_I32, [_P]),
+    "critmc_chain_info": (_I32, [_P, _P, _P, _P]),
+    "critmc_chain_set_step": (_I32, [_P, _D]),
+    "critmc_advance": (_I32, [_P, _D, _P, _I32, _I32, _P, _P, _P, _P, _P]),
+    "critmc_get_state": (_I32, [_P, _P, _P, _P]),
+    "critmc_set_state": (_I32, [_P, _P, _P]),
+    "critmc_batch_create": (_I32, [_P]),
+    "critmc_batch_destroy": (_I32, [_P]),
+    "critmc_batch_submit": (_I32, [_P, _P, _D, _P, _I32, _I32, _P, _P, _P, _P, _P]),
+    "critmc_batch_poll": (_I32, [_P, _P, _P, _I32, _P]),
+    "critmc_batch_cancel": (_I32, [_P, ctypes.c_int64]),
+    "critmc_batch_pending": (_I32, [_P]),
     "critmc_ea_campaign_buffer_bytes": (_I64, [_I32, _I64]),
     "critmc_ea_campaign_run": (
         _I32, [_P, _I32, _I32, _I32, _P, _P, _I32, _U32, _I32, _I32, _I32, _P, _I64, _P, _P]),

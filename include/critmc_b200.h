@@ -311,6 +311,66 @@ int64_t critmc_items_buffer_bytes(int32_t n_items);
 int32_t critmc_run_items(const critmc_item* items, int32_t n_items, void* buffer,
                          int64_t buffer_bytes, void* staging, int32_t smem_limit, void* stream);
 
+/* ---- chains owned by the library (handles) ----------------------------------
+ * The library allocates and keeps a chain's lattice, running sums, Philox key
+ * and sweep counter; the caller passes states in critmc's site order (first
+ * coordinate fastest) and gets per-measurement series.  Replaces critmc's
+ * Model.advance with the state held by Simulation (src/critmc/models.py:58-68,
+ * sim.py:174, :188-191).
+ * model_kind: CRITMC_MODEL_*.  dims: extents {lx, ly, lz}, 0 for absent
+ * axes (1D: {L, 0, 0}); every extent even.  q_or_n: Potts q, O(n) n (2, 3);
+ * h: Ising field.  The chain's Philox key is words 0, 1 of
+ * Philox(chain_id, 0, 0x205, chain_id >> 32) under the key (seed_lo, seed_hi).
+ * start: CRITMC_START_RANDOM (from the chain's key), _ORDERED (all +1 / state
+ * 0 / (1, 0, ..)), or _STATE from init_state (HOST: int8 [N] Ising +-1 or
+ * Potts 0..q-1, double [N][n] O(n)).  Multi-spin-coded Ising (2D/3D, lx/64 a
+ * power of two) and 1-byte lattices are chosen by shape.                     */
+typedef struct critmc_chain critmc_chain;
+#define CRITMC_MODEL_ISING 0
+#define CRITMC_MODEL_POTTS 1
+#define CRITMC_MODEL_ON 2
+#define CRITMC_START_RANDOM 0
+#define CRITMC_START_ORDERED 1
+#define CRITMC_START_STATE 2
+int32_t critmc_chain_create(int32_t model_kind, const int32_t dims[3], int32_t q_or_n, double h,
+                            uint32_t seed_lo, uint32_t seed_hi, uint64_t chain_id, int32_t start,
+                            const void* init_state, critmc_chain** handle);
+int32_t critmc_chain_destroy(critmc_chain* chain);
+/* layout: 0 multi-spin-coded, 1 byte, 2 float; sweep: the chain's counter */
+int32_t critmc_chain_info(const critmc_chain* chain, int32_t* layout, uint32_t* sweep, uint32_t key[2]);
+/* O(n) Metropolis step size (critmc's running["step"], sim.py:226-229) */
+int32_t critmc_chain_set_step(critmc_chain* chain, double step);
+/* n_meas applications of schedule (HOST (code, reps) rows) at inverse
+ * temperature beta, on `stream`.  Outputs (device-accessible):
+ * Ising e_out = E_b, m_out = M [n_meas] int64; Potts e_out = E, m_out =
+ * counts [n_meas][q]; O(n) f64_out = E [n_meas] | M [n_meas][n] | stiffness
+ * cos [n_meas][dim] | sin [n_meas][dim]; aux_out [n_meas][4] for all.
+ * Results equal the per-model entry points for the same key and sweep.     */
+int32_t critmc_advance(critmc_chain* chain, double beta, const int64_t* schedule, int32_t n_rows,
+                       int32_t n_meas, int64_t* e_out, int64_t* m_out, int64_t* aux_out,
+                       double* f64_out, void* stream);
+/* State in critmc's site order into / from HOST memory (synchronous);
+ * running_out (HOST, may be null): Ising (E_b, M), Potts (E, counts[q]).  */
+int32_t critmc_get_state(critmc_chain* chain, void* host_out, int64_t* running_out, void* stream);
+int32_t critmc_set_state(critmc_chain* chain, const void* host_in, void* stream);
+
+/* Batch queue over handles: submissions of many chains run together as work
+ * items (critmc_run_items), one submission per chain per round, in
+ * submission order per chain.  poll runs rounds until nothing is pending or
+ * max_done tickets are finished, then waits for `stream`; cancel drops a
+ * pending submission.  No counterpart in critmc (process pool,
+ * src/critmc/runner.py:154-223).                                            */
+typedef struct critmc_batch critmc_batch;
+int32_t critmc_batch_create(critmc_batch** batch);
+int32_t critmc_batch_destroy(critmc_batch* batch);
+int32_t critmc_batch_submit(critmc_batch* batch, critmc_chain* chain, double beta,
+                            const int64_t* schedule, int32_t n_rows, int32_t n_meas, int64_t* e_out,
+                            int64_t* m_out, int64_t* aux_out, double* f64_out, int64_t* ticket);
+int32_t critmc_batch_poll(critmc_batch* batch, void* stream, int64_t* done, int32_t max_done,
+                          int32_t* n_done);
+int32_t critmc_batch_cancel(critmc_batch* batch, int64_t ticket);
+int32_t critmc_batch_pending(const critmc_batch* batch);
+
 /* Instantiated CUDA graphs are cached across calls with identical parameters
  * (the same chains advanced slice after slice): capacity in entries (default
  * 64, 0 disables caching and frees every entry) and current size.  No

@@ -286,17 +286,21 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def serve_bench(dev, n_requests: int, rate: float, seed: int = 0) -> dict:
+def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0, world: int = 1) -> dict | None:
     """Continuous-batching server on a seeded Poisson stream of mixed requests.
 
     Workload: ``n_requests`` requests at ``rate``/s, each uniform over 2D Ising
     L in {16..1024} (beta ~ U[0.38, 0.50]), q=10 Potts L in {16..128}
     (beta ~ U[1.35, 1.50]) and XY L in {32, 64, 128} (T ~ U[0.8, 1.0]), sweeps
     log-uniform in [1e3, 1e5].  Latency = arrival -> result on the host.
+    With several ranks each serves its shard of the same stream (replicas);
+    rank 0 returns the whole job's numbers, the others None.
     """
+    from critmc_b200 import replicas
     from critmc_b200.serve import Request, Server, mixed_workload
 
-    reqs = mixed_workload(n_requests, rate, seed)
+    all_reqs = mixed_workload(n_requests, rate, seed)
+    reqs = replicas.shard(all_reqs, rank, world)
     lat, upd = [], [0]
 
     def on_result(res):
@@ -311,12 +315,21 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0) -> dict:
              for i, (m, L) in enumerate(shapes)])
     srv.on_result = on_result
     srv.ticks, srv.gpu_seconds, srv.updates_done, srv.max_queued, srv.peak_in_use = 0, 0.0, 0, 0, 0
+    replicas.barrier(dev)
     srv.t0 = time.perf_counter()
     srv.run(reqs)
-    wall = srv.now()
-    lat_a = np.array(lat)
     st = srv.stats()
-    return {"requests": len(lat), "rate_per_s": rate, "wall_s": wall,
+    parts = replicas.gather_to_root({"lat": lat, "upd": upd[0], "wall": srv.now(), "gpu": st["gpu_seconds"],
+                                     "ticks": st["ticks"], "hbm": st["peak_hbm_bytes"], "queued": st["max_queued"]})
+    if parts is None:
+        return None
+    wall = max(p["wall"] for p in parts)
+    lat = [x for p in parts for x in p["lat"]]
+    upd = [sum(p["upd"] for p in parts)]
+    st = {"gpu_seconds": sum(p["gpu"] for p in parts), "ticks": sum(p["ticks"] for p in parts),
+          "peak_hbm_bytes": max(p["hbm"] for p in parts), "max_queued": max(p["queued"] for p in parts)}
+    lat_a = np.array(lat)
+    return {"requests": len(lat), "rate_per_s": rate, "wall_s": wall, "gpus": world,
             "p50_latency_s": float(np.percentile(lat_a, 50)), "p99_latency_s": float(np.percentile(lat_a, 99)),
             "mean_latency_s": float(lat_a.mean()), "max_latency_s": float(lat_a.max()),
             "updates_per_ns": upd[0] / wall / 1e9, "gpu_busy_frac": st["gpu_seconds"] / wall,
@@ -457,8 +470,8 @@ def main() -> None:
             "L1024": extras["batched_L1024"] / extras["plain_one_chain_L1024"]}
 
     serving = None
-    if rank == 0 and world == 1 and args.serve_requests > 0:
-        serving = serve_bench(dev, args.serve_requests, args.serve_rate)
+    if args.serve_requests > 0:  # every rank serves its shard; rank 0 gets the job's numbers
+        serving = serve_bench(dev, args.serve_requests, args.serve_rate, rank=rank, world=world)
     if rank == 0 and world == 1 and not args.no_extras:
         extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
         extras["on_batched"] = on_bench(dev, peak=peaks()[0])

@@ -286,7 +286,8 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0, world: int = 1) -> dict | None:
+def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0, world: int = 1,
+                max_grid_lanes: int = 8) -> dict | None:
     """Continuous-batching server on a seeded Poisson stream of mixed requests.
 
     Workload: ``n_requests`` requests at ``rate``/s, each uniform over 2D Ising
@@ -307,7 +308,7 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0,
         lat.append(res.latency)
         upd[0] += res.updates
 
-    srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto")
+    srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto", max_grid_lanes=max_grid_lanes)
     # warm-up: one short request per (model, size) of the mix builds the
     # lattice cache, the library streams and the kernels' first launches
     shapes = sorted({(r.model, r.L) for r in reqs})
@@ -350,6 +351,7 @@ def main() -> None:
                     help="requests of the serving run (0 skips it; 1 GPU only)")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
+    ap.add_argument("--serve-grid-lanes", type=int, default=8, help="requests on multi-block lanes at once")
     ap.add_argument("--case", choices=["ea-small", "on-small"],
                     help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()
@@ -402,7 +404,8 @@ def main() -> None:
         return
 
     if args.serve_only:
-        print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate)}), flush=True)
+        print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate,
+                                                 max_grid_lanes=args.serve_grid_lanes)}), flush=True)
         return
 
     # launch shape (rows per thread, inline planes) from the autotuner; results do not depend on it
@@ -471,14 +474,15 @@ def main() -> None:
 
     serving = None
     if args.serve_requests > 0:  # every rank serves its shard; rank 0 gets the job's numbers
-        serving = serve_bench(dev, args.serve_requests, args.serve_rate, rank=rank, world=world)
+        serving = serve_bench(dev, args.serve_requests, args.serve_rate, rank=rank, world=world,
+                              max_grid_lanes=args.serve_grid_lanes)
     if rank == 0 and world == 1 and not args.no_extras:
         extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
         extras["on_batched"] = on_bench(dev, peak=peaks()[0])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(min(32, os.cpu_count() or 1), sweeps=10)
+        cpu = cpu_sample(min(32, os.cpu_count() or 1), sweeps=30)
 
     if rank == 0:
         line = {

@@ -48,10 +48,68 @@ N_AUX = 4
 # moves of critmc that are not data-parallel sweeps and stay on its CPU path
 _NOT_ON_GPU = {
     "metropolis-random": "random-site Metropolis is a sequential walk, not a checkerboard sweep",
-    "wolff": "cluster updates are not part of the checkerboard sampling path",
-    "sw": "cluster updates are not part of the checkerboard sampling path",
-    "swendsen-wang": "cluster updates are not part of the checkerboard sampling path",
+    "wolff": "O(n) cluster updates (embedded-Ising reflections) are not on the GPU path",
+    "sw": "O(n) cluster updates (embedded-Ising reflections) are not on the GPU path",
+    "swendsen-wang": "O(n) cluster updates (embedded-Ising reflections) are not on the GPU path",
 }
+CLUSTER_CODES = (WOLFF, SWENDSEN_WANG)
+
+
+def advance_with_clusters(model, chain, running, beta, schedule, n_meas, bits: bool, q: int):
+    """``Model.advance`` for schedules with Wolff / Swendsen-Wang rows (Ising, Potts).
+
+    Rows run in order once per measurement: sweep rows through the chain's own
+    entry point, cluster rows through ``critmc_cluster_update`` on the chain's
+    device lattice; the sweep counter advances by one per repetition of every
+    row, as for sweeps.  aux columns as critmc (kernels/common.py:35-39).
+    """
+    sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+    dev = chain.device
+    potts = q > 0
+    dims = chain.dims
+    if not hasattr(chain, "_cl_scratch"):
+        chain._cl_scratch = empty_bytes(_lib.lib().critmc_cluster_scratch_bytes(1, model.n_sites), dev)
+    spins = chain.words if bits else chain.spins
+    out_e = np.empty(n_meas, dtype=np.int64)
+    out_m = np.empty((n_meas, q) if potts else n_meas, dtype=np.int64)
+    aux = np.zeros((n_meas, N_AUX), dtype=np.int64)
+    stats = torch.zeros((1, 3), dtype=torch.int64, device=dev)
+    for meas in range(n_meas):
+        stats.zero_()
+        for code, reps in sched:
+            if code in CLUSTER_CODES:
+                if potts:
+                    run_t = torch.tensor([running["energy"]], dtype=torch.int64, device=dev)
+                    cnt_t = torch.from_numpy(np.asarray(running["counts"], dtype=np.int64)).to(dev)
+                else:
+                    run_t = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
+                    cnt_t = None
+                for _ in range(int(reps)):
+                    _lib.call("critmc_cluster_update", int(bits), ptr(spins), len(chain.shape), *dims, q, 1,
+                              chain.key.ctypes.data, float(beta), int(code), chain.sweep, ptr(run_t), ptr(cnt_t),
+                              ptr(stats), ptr(chain._cl_scratch), stream_handle(dev))
+                    chain.sweep += 1
+                r = to_host(run_t).ravel()
+                if potts:
+                    running["energy"] = int(r[0])
+                    running["counts"] = to_host(cnt_t).copy()
+                else:
+                    running["e_b"], running["m"] = int(r[0]), int(r[1])
+            else:
+                part = model._advance_sweeps(chain, running, beta, np.array([[code, reps]]), 1)
+                aux[meas, AUX_ACCEPTED] += int(part["aux"][0][AUX_ACCEPTED])
+        st = to_host(stats).ravel()
+        aux[meas, AUX_WOLFF_SIZE] = st[0]
+        aux[meas, AUX_SW_C2], aux[meas, AUX_SW_NCLUSTERS] = st[1], st[2]
+        if potts:
+            out_e[meas] = running["energy"]
+            out_m[meas] = running["counts"]
+        else:
+            out_e[meas], out_m[meas] = running["e_b"], running["m"]
+    if potts:
+        return {"E": out_e, "counts": out_m, "aux": aux}
+    h = model.h
+    return {"E": out_e - h * out_m if h != 0.0 else out_e, "Eb": out_e, "M": out_m, "aux": aux}
 
 
 def _checkerboard_shape(lattice: Lattice) -> tuple[int, ...]:
@@ -181,7 +239,7 @@ class Ising(Model):
     """Ising model with uniform field ``h`` (critmc models.py:95-162)."""
 
     kind = "ising"
-    updates = ("metropolis", "heatbath")
+    updates = ("metropolis", "heatbath", "wolff", "sw", "swendsen-wang")
 
     def __init__(self, lattice: Lattice, h: float = 0.0):
         super().__init__(lattice)
@@ -237,6 +295,12 @@ class Ising(Model):
         return IsingByteChain(self, np.asarray(state, dtype=np.int8), key, device)
 
     def advance(self, chain, running, beta, schedule, n_meas):
+        if np.isin(np.asarray(schedule).reshape(-1, 2)[:, 0], CLUSTER_CODES).any():
+            return advance_with_clusters(self, chain, running, beta, schedule, n_meas,
+                                         isinstance(chain, _IsingMscChain), 0)
+        return self._advance_sweeps(chain, running, beta, schedule, n_meas)
+
+    def _advance_sweeps(self, chain, running, beta, schedule, n_meas):
         if not isinstance(chain, _IsingMscChain):
             return chain.advance(running, beta, schedule, n_meas)
         dev = chain.device
@@ -268,7 +332,7 @@ class Potts(Model):
     """q-state Potts model (critmc models.py:165-222)."""
 
     kind = "potts"
-    updates = ("metropolis", "heatbath")
+    updates = ("metropolis", "heatbath", "wolff", "sw", "swendsen-wang")
 
     def __init__(self, lattice: Lattice, q: int):
         super().__init__(lattice)
@@ -307,6 +371,11 @@ class Potts(Model):
         return PottsChain(self, np.asarray(state, dtype=np.int8), philox_key(rng), device)
 
     def advance(self, chain, running, beta, schedule, n_meas):
+        if np.isin(np.asarray(schedule).reshape(-1, 2)[:, 0], CLUSTER_CODES).any():
+            return advance_with_clusters(self, chain, running, beta, schedule, n_meas, False, self.q)
+        return chain.advance(running, beta, schedule, n_meas)
+
+    def _advance_sweeps(self, chain, running, beta, schedule, n_meas):
         return chain.advance(running, beta, schedule, n_meas)
 
     def spec(self):

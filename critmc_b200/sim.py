@@ -27,6 +27,7 @@ import numpy as np
 from .io import load_npz, save_npz
 from .models import (
     AUX_ACCEPTED,
+    AUX_WOLFF_SIZE,
     HEATBATH,
     METROPOLIS,
     METROPOLIS_RANDOM,
@@ -140,6 +141,10 @@ class Simulation:
         self.schedule = np.array(
             [[UPDATE_CODES[name], 1 if k is None else k] for name, k in rows], dtype=np.int64
         )
+        # "wolff" without a count: tuned to about N / <|C|> clusters per measurement (sim.py:166, :208-222)
+        self._auto_wolff = [r for r, (name, k) in enumerate(rows) if name == "wolff" and k is None]
+        self._mean_cluster = float("nan")
+        self._wolff_history: list[int] = []
         host_state = model.initial_state(start, self.rng) if state is None else np.array(state, copy=True)
         self.start = "given" if state is not None else start
         self.running = model.begin(host_state)
@@ -160,12 +165,14 @@ class Simulation:
         return self.model.advance(self.chain, self.running, self.beta, self.schedule, n_meas)
 
     def thermalize(self, n_meas: int, *, tune: bool = True, n_chunks: int = 10) -> dict[str, Any]:
-        """Discard ``n_meas`` measurements; tune the O(n) Metropolis step (critmc sim.py:193-231)."""
+        """Discard ``n_meas`` measurements; tune the Wolff count and the O(n) Metropolis step
+        (critmc sim.py:193-231)."""
         if n_meas < 0:
             raise ValueError("n_meas must not be negative")
         n_chunks = max(1, min(n_chunks, n_meas)) if n_meas else 1
         sizes = np.diff(np.linspace(0, n_meas, n_chunks + 1).astype(int))
         n_metro = self._count(METROPOLIS, METROPOLIS_RANDOM)
+        n_wolff = self._count(WOLFF)
         for chunk in sizes:
             if chunk == 0:
                 continue
@@ -173,6 +180,18 @@ class Simulation:
             if not tune:
                 continue
             aux = raw["aux"]
+            if n_wolff:
+                late = aux[len(aux) // 2:, AUX_WOLFF_SIZE]  # the better-equilibrated half
+                mean_c = late.sum() / (n_wolff * len(late))
+                self._mean_cluster = float(mean_c)
+                if self._auto_wolff and mean_c > 0:
+                    target = max(1, int(round(self.model.n_sites / mean_c)))
+                    for row in self._auto_wolff:
+                        current = int(self.schedule[row, 1])
+                        # at most a factor 4 per chunk: a hot start has tiny clusters
+                        self.schedule[row, 1] = int(np.clip(target, max(1, current // 4), 4 * current))
+                    self._wolff_history.append(int(self.schedule[self._auto_wolff[0], 1]))
+                    n_wolff = self._count(WOLFF)
             if "step" in self.running and n_metro:
                 rate = aux[:, AUX_ACCEPTED].sum() / (n_metro * self.model.n_sites * len(aux))
                 factor = float(np.clip(rate / 0.5, 0.5, 2.0))
@@ -182,6 +201,11 @@ class Simulation:
 
     def tuning(self) -> dict[str, Any]:
         info: dict[str, Any] = {"schedule": self.schedule.tolist()}
+        if self._count(WOLFF):
+            info["wolff_per_meas"] = self._count(WOLFF)
+            info["mean_cluster"] = self._mean_cluster
+            if self._wolff_history:
+                info["wolff_history"] = list(self._wolff_history)
         if "step" in self.running:
             info["step"] = self.running["step"]
         return info
@@ -208,7 +232,10 @@ class Simulation:
         self.n_meas += n_meas
         aux = raw["aux"]
         n = self.model.n_sites
-        sweeps = self._count(METROPOLIS, METROPOLIS_RANDOM, HEATBATH, OVERRELAX, SWENDSEN_WANG)
+        n_wolff = self._count(WOLFF)
+        mean_cluster = float(aux[:, AUX_WOLFF_SIZE].sum() / (n_wolff * n_meas)) if n_wolff else float("nan")
+        sweeps = self._count(METROPOLIS, METROPOLIS_RANDOM, HEATBATH, OVERRELAX, SWENDSEN_WANG) + (
+            n_wolff * mean_cluster / n if n_wolff else 0.0)
         n_single = self._count(METROPOLIS, METROPOLIS_RANDOM)
         meta = {
             **self.model.meta(),
@@ -220,7 +247,7 @@ class Simulation:
             "n_therm": self.n_therm,
             "n_meas": n_meas,
             "sweeps_per_meas": float(sweeps),
-            "mean_cluster": float("nan"),
+            "mean_cluster": mean_cluster,
             "acceptance": (
                 float(aux[:, AUX_ACCEPTED].sum() / (n_single * n * n_meas)) if n_single else None
             ),
@@ -232,4 +259,3 @@ class Simulation:
         return TimeSeries(raw, meta)
 
 
-_ = WOLFF  # the code exists in the schedule vocabulary; the GPU models refuse it

@@ -311,6 +311,29 @@ int64_t critmc_items_buffer_bytes(int32_t n_items);
 int32_t critmc_run_items(const critmc_item* items, int32_t n_items, void* buffer,
                          int64_t buffer_bytes, void* staging, int32_t smem_limit, void* stream);
 
+/* ---- cluster updates (Swendsen-Wang, Wolff) ----------------------------------
+ * One cluster update of n_chains Ising or Potts chains.  bits: 1 for the
+ * multi-spin-coded Ising words, 0 for int8 spins (Ising +-1, Potts 0..q-1).
+ * q: 0 for Ising, else the Potts q.  keys: HOST [n_chains][2].  algo:
+ * CRITMC_WOLFF or CRITMC_SWENDSEN_WANG.  Sites are numbered by their
+ * colour-major layout index u; bond (colour-0 site s, direction q) is active
+ * when both ends agree and word q%4 of Philox(s, sweep, 0x07 | (q/4)<<8, 0)
+ * < round(p 2^32), p = 1 - e^{-2 beta} (Ising), 1 - e^{-beta} (Potts).  The
+ * root of a cluster is its smallest u.  SW: root r draws word 0 of
+ * Philox(r, sweep, 0x08, 0) (Ising: flip if >= 2^31; Potts: state
+ * (w q) >> 32).  Wolff: seed (w0 N) >> 32 from Philox(0, sweep, 0x09, 0),
+ * Potts new state (old + 1 + ((w1 (q-1)) >> 32)) mod q.
+ * Device in/out: running (Ising [n][2] E_b, M; Potts energy [n]), counts
+ * (Potts [n][q]), stats [n][3] (+= Wolff cluster size; SW sum |C|^2 and
+ * cluster count of this decomposition).  scratch:
+ * critmc_cluster_scratch_bytes(n_chains, sites per chain) bytes.
+ * Replaces critmc kernels/ising.py:111-171, kernels/potts.py:107-168.       */
+int64_t critmc_cluster_scratch_bytes(int32_t n_chains, int64_t n_sites);
+int32_t critmc_cluster_update(int32_t bits, void* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                              int32_t q, int32_t n_chains, const uint32_t* keys, double beta,
+                              int32_t algo, uint32_t sweep, int64_t* running, int64_t* counts,
+                              int64_t* stats, void* scratch, void* stream);
+
 /* ---- chains owned by the library (handles) ----------------------------------
  * The library allocates and keeps a chain's lattice, running sums, Philox key
  * and sweep counter; the caller passes states in critmc's site order (first

@@ -65,9 +65,34 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_potts_run.restype = _I
     L.oracle_on_run.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _D, _U32, _P, _I, _I, _P, _P, _P, _P, _P]
     L.oracle_on_run.restype = _I
+    L.oracle_cluster_update.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _I, _U32, _P, _P, _P, _P]
+    L.oracle_cluster_update.restype = _I
     L.oracle_ea_pt_run.argtypes = [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _P, _P, _U32, _I, _I, _I,
                                    _P, _P, _P, _P, _P]
     L.oracle_ea_pt_run.restype = _I
+
+
+def cluster_update(lay: np.ndarray, shape, q: int, key, beta: float, algo: int, sweep: int,
+                   stats: np.ndarray | None = None):
+    """One Wolff (algo 3) or SW (4) update of int8 values in the colour-major layout (in place).
+
+    Returns (dE, dM, counts_delta, stats): Ising dE of E_b, Potts dE of E and the
+    change of the state counts.
+    """
+    lay8 = np.ascontiguousarray(lay, dtype=np.int8)
+    flat = lay8.reshape(-1)
+    lx, ly, lz = _dims(shape)
+    k = np.ascontiguousarray(key, dtype=np.uint32).reshape(2)
+    de = ctypes.c_int64(0)
+    dm = ctypes.c_int64(0)
+    cd = np.zeros(max(q, 1), dtype=np.int64)
+    st = np.zeros(3, dtype=np.int64) if stats is None else stats
+    rc = lib().oracle_cluster_update(_ptr(flat), len(shape), lx, ly, lz, q, _ptr(k), float(beta), algo, sweep,
+                                     ctypes.byref(de), ctypes.byref(dm), _ptr(cd), _ptr(st))
+    if rc:
+        raise MemoryError("oracle_cluster_update")
+    lay[...] = flat.reshape(lay.shape)
+    return de.value, dm.value, cd[:q] if q else None, st
 
 
 def _ptr(a: np.ndarray) -> int:

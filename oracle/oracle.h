@@ -23,6 +23,9 @@ int oracle_on_run(float* s, int dim, int lx, int ly, int lz, int n, const uint32
                   double beta, double step, uint32_t sweep0, const int64_t* schedule, int n_rows,
                   int n_meas, double* e_out, double* m_out, double* sc_out, double* ss_out,
                   int64_t* aux_out);
+int oracle_cluster_update(int8_t* lay, int dim, int lx, int ly, int lz, int q, const uint32_t key[2],
+                          double beta, int algo, uint32_t sweep, int64_t* d_energy, int64_t* d_mag,
+                          int64_t* counts_delta, int64_t stats[3]);
 int oracle_ea_pt_run(int8_t* spins, const double* J, int dim, int lx, int ly, int lz, int m,
                      const uint32_t* keys, const double* betas, const uint32_t* swap_thr, int width,
                      int* perm, int* labels, uint32_t t0, int n_steps, int n_bins,

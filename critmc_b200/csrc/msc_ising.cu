@@ -80,7 +80,7 @@ __device__ __forceinline__ void msc_fixup(const MscRule<Z, RULE>& rule, const Ms
 // One colour of one sweep.  grid: x = column/run tiles, y = chain of the launch.
 // Thread t walks `run` consecutive rows of column k = t mod wc.
 template <int Z, int RULE, int KG>
-__global__ void __launch_bounds__(MSC_THREADS)
+__global__ void __launch_bounds__(MSC_THREADS, 4)
     msc_halfsweep_kernel(const __grid_constant__ MscParams P) {
   __shared__ MscFix fix[MSC_WARPS][MSC_FIXCAP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

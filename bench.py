@@ -308,7 +308,9 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0,
         lat.append(res.latency)
         upd[0] += res.updates
 
-    srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto", max_grid_lanes=max_grid_lanes)
+    # series reduced to sums (stats_lag=0: no host-side error-bar sums inside the timed run)
+    srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto", max_grid_lanes=max_grid_lanes,
+                 stats_lag=0)
     # warm-up: one short request per (model, size) of the mix builds the
     # lattice cache, the library streams and the kernels' first launches
     shapes = sorted({(r.model, r.L) for r in reqs})

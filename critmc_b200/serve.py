@@ -42,6 +42,7 @@ from .lattice import hypercubic
 from .models import ON, UPDATE_CODES, Ising, Model, Potts, _IsingMscChain, _msc_ok
 from .rng import make_rng, philox_key
 from .sim import parse_updates
+from .streaming import HostStreamStats
 
 __all__ = ["Request", "Result", "Server", "open_chain", "mixed_workload", "DEFAULT_UPDATES"]
 
@@ -105,6 +106,7 @@ class Result:
     admitted: float
     finished: float
     updates: int
+    stats: dict | None = None  # summary servers: Gamma-method mean, error, tau_int per scalar series
 
     @property
     def latency(self) -> float:
@@ -201,6 +203,7 @@ class _Job:
     harvested: int = 0
     group: str = ""
     home: object = None  # the lane that advances it
+    stream: dict = field(default_factory=dict)  # summary mode: streaming statistics per scalar field
 
     @property
     def meas_bytes(self) -> int:
@@ -279,7 +282,8 @@ class Server:
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
                  tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
-                 keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None):
+                 keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None,
+                 stats_lag: int = 64):
         self.device = require_cuda(device)
         free, _ = torch.cuda.mem_get_info(self.device)
         cap = max(0, free - reserve - 2 * arena_bytes)
@@ -291,6 +295,7 @@ class Server:
         # kernels throughput, so at most this many requests use them at once
         self.max_grid_lanes = max_grid_lanes
         self.keep_series, self.keep_state = keep_series, keep_state
+        self.stats_lag = int(stats_lag)
         self.on_result = on_result
         self.in_use = 0
         self.peak_in_use = 0
@@ -458,6 +463,9 @@ class Server:
                           for name, dt, w in fields}
         else:
             job.series = {name: np.zeros(w, dtype=dt) for name, dt, w in fields}
+            # error bars without keeping the series: streaming Gamma-method sums per scalar field
+            if self.stats_lag > 0:
+                job.stream = {name: HostStreamStats(self.stats_lag) for name, _, w in fields if w == 1}
         return job
 
     # ---- ticks -----------------------------------------------------------
@@ -587,6 +595,8 @@ class Server:
                     j.series[name][h0:h0 + n] = v.reshape(n, w) if w > 1 else v
                 else:
                     j.series[name] += v.reshape(n, w).sum(axis=0)
+                    if name in j.stream:
+                        j.stream[name].update(v)
             j.harvested += n
             self.updates_done += n * j.sweeps_per_meas * j.req.n_sites
             if j.harvested == j.req.sweeps:
@@ -609,7 +619,8 @@ class Server:
             series["E"] = series["Eb"] - j.model.h * series["M"] if j.model.h != 0.0 else series["Eb"]
         state = j.chain.fetch() if self.keep_state else None
         res = Result(req, series, state, float(req.arrival), j.admitted, now,
-                     req.n_sites * j.sweeps_per_meas * req.sweeps)
+                     req.n_sites * j.sweeps_per_meas * req.sweeps,
+                     {name: hs.result() for name, hs in j.stream.items()} if j.stream else None)
         self.active.remove(j)
         j.home.jobs.remove(j)
         self.in_use -= j.dev_bytes

@@ -334,6 +334,18 @@ int32_t critmc_cluster_update(int32_t bits, void* spins, int32_t dim, int32_t lx
                               int32_t algo, uint32_t sweep, int64_t* running, int64_t* counts,
                               int64_t* stats, void* scratch, void* stream);
 
+/* ---- streaming Gamma-method sums ---------------------------------------------
+ * Append n values per chain (values: DEVICE [n_chains][ld], int64 or double)
+ * to the per-chain state (DEVICE, critmc_stream_state_bytes(n_chains,
+ * max_lag) bytes, zeroed before the first update): count, shift (first value),
+ * sum and sum of squares of value - shift, lag sums S_t (t = 1..max_lag), first
+ * and last max_lag values.  Gamma(t) for t <= max_lag follows exactly, as
+ * critmc's gamma_method gets it from the full series
+ * (src/critmc/stats/autocorr.py:381).                                         */
+int64_t critmc_stream_state_bytes(int32_t n_chains, int32_t max_lag);
+int32_t critmc_stream_update(const void* values, int32_t is_double, int32_t n_chains, int32_t n, int64_t ld,
+                             double* state, int32_t max_lag, void* stream);
+
 /* ---- chains owned by the library (handles) ----------------------------------
  * The library allocates and keeps a chain's lattice, running sums, Philox key
  * and sweep counter; the caller passes states in critmc's site order (first

@@ -70,6 +70,20 @@ def test_admission_waits_for_hbm(cuda):
         _check(res, cuda)
 
 
+def test_summary_mode_error_bars(cuda):
+    from exact_helpers import gamma_error
+
+    req = Request("ising", 64, 0.44, 3000, seed=50, rid=0, arrival=0.0)
+    srv = Server(cuda, tick_ms=0.3, keep_series=False, stats_lag=128)
+    (res,) = srv.run([req])
+    raw, _ = _alone(req, cuda)
+    st = res.stats["Eb"]
+    mean, err, tau = gamma_error(raw["Eb"].astype(np.float64))
+    assert st["n"] == 3000 and st["mean"] == pytest.approx(mean, rel=1e-12)
+    if not st["truncated"]:
+        assert st["error"] == pytest.approx(err, rel=1e-7)
+
+
 def test_summary_mode_sums_match(cuda):
     reqs = [Request("ising", 32, 0.44, 300, seed=40, rid=0, arrival=0.0),
             Request("potts", 16, 1.4, 250, seed=41, rid=1, arrival=0.0)]

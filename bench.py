@@ -174,17 +174,84 @@ def on_bench(dev, steps: int = 40, peak: float = 6650.0) -> dict:
     return out
 
 
+def fh_bench(dev) -> dict:
+    """Wang-Landau moves on the q = 10 Potts 8 x 8 torus, energy window [-1.95, -0.6]
+    per site (critmc's flat-histogram double-peak case): 4736 walkers (32 per SM)
+    x 200,000 moves in one launch, and one walker x 1,000,000 moves, each with
+    constant ln f and in 1/t mode; the C oracle runs one walker on one host core
+    (2,000,000 moves) for comparison."""
+    import torch
+
+    import oracle
+    from critmc_b200 import Potts, square
+    from critmc_b200.flathist import WangLandau
+
+    model = Potts(square(8), 10)
+    out = {}
+    for nw, moves in ((4736, 200_000), (1, 1_000_000)):
+        for one_t in (0, 1):
+            wl = WangLandau(model, e_window=(-1.95, -0.6), seed=5, n_walkers=nw, device=dev)
+            W = wl.walkers
+            lng = torch.zeros((nw, wl.levels.size), dtype=torch.float64, device=dev)
+            lnf = torch.full((nw,), 1e-3, dtype=torch.float64, device=dev)
+            mode = torch.full((nw,), one_t, dtype=torch.int32, device=dev)
+            args = dict(ln_f=lnf, n_levels=lnf * 80, one_over_t=mode)
+            W.run(0, lng, 1000, t_base=W.trials.clone(), **args)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            base = W.trials.clone()
+            torch.cuda.synchronize(dev)
+            e0.record()
+            W.run(0, lng, moves, t_base=base, **args)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            s = e0.elapsed_time(e1) * 1e-3
+            out[f"walkers{nw}_{'one_over_t' if one_t else 'const'}_moves_per_ns"] = nw * moves / s / 1e9
+    wl = WangLandau(model, e_window=(-1.95, -0.6), seed=6, device=dev)
+    W = wl.walkers
+    st = W.spins[0].cpu().numpy().copy()
+    order = np.bincount(st.astype(np.int64), minlength=10).astype(np.int64)
+    lng_h = np.zeros(wl.levels.size)
+    hist_h = np.zeros(wl.levels.size, dtype=np.int64)
+    key = W.keys[0].cpu().numpy().view(np.uint32)
+    t0 = time.perf_counter()
+    oracle.fh_run(0, st, (8, 8), 10, key, int(W.idx[0]), order, lng_h, hist_h, wl.window, 0, 1e-3, 0.0, False, 0,
+                  2_000_000)
+    cpu = 2_000_000 / (time.perf_counter() - t0) / 1e9
+    out["cpu_oracle_one_walker_one_core_moves_per_ns"] = cpu
+    out["batch_over_cpu_core"] = out["walkers4736_const_moves_per_ns"] / cpu
+    return out
+
+
 def small_case(dev, case: str) -> dict:
     """A small, short case of one secondary kernel: one warm-up launch, then one timed launch.
 
     ea-small: the EA campaign kernel on L in {6, 8, 10, 12, 16} x 64 samples x 2 x 32
     temperatures, 31 steps.  on-small: the O(n) block kernel on 128 XY chains of
     128 x 128 (16 temperatures x 8), 2 steps of 1 heat bath + 4 over-relaxation.
+    fh-single / fh-batch: Wang-Landau moves (ln f = 1e-3) of one walker (500,000
+    moves) or of 4736 walkers (32 per SM, 200,000 moves each) on the q = 10 Potts
+    8 x 8 torus, energy window [-1.95, -0.6] per site.
     """
     import torch
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if case == "ea-small":
+    if case in ("fh-single", "fh-batch"):
+        from critmc_b200 import Potts, square
+        from critmc_b200.flathist import WangLandau
+
+        nw, moves = (1, 500_000) if case == "fh-single" else (4736, 200_000)
+        wl = WangLandau(Potts(square(8), 10), e_window=(-1.95, -0.6), seed=5, n_walkers=nw, device=dev)
+        W = wl.walkers
+        lng = torch.zeros((nw, wl.levels.size), dtype=torch.float64, device=dev)
+        lnf = torch.full((nw,), 1e-3, dtype=torch.float64, device=dev)
+        off = torch.zeros(nw, dtype=torch.int32, device=dev)
+        W.run(0, lng, 1000, ln_f=lnf, n_levels=lnf, one_over_t=off, t_base=W.trials.clone())
+        torch.cuda.synchronize(dev)
+        e0.record()
+        W.run(0, lng, moves, ln_f=lnf, n_levels=lnf, one_over_t=off, t_base=W.trials.clone())
+        e1.record()
+        units = nw * moves
+    elif case == "ea-small":
         from critmc_b200 import cubic
         from critmc_b200.glass import EdwardsAnderson, MultiSizeCampaign, SpinGlassCampaign, geometric_temperatures
 
@@ -354,7 +421,7 @@ def main() -> None:
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
     ap.add_argument("--serve-grid-lanes", type=int, default=8, help="requests on multi-block lanes at once")
-    ap.add_argument("--case", choices=["ea-small", "on-small"],
+    ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch"],
                     help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -481,6 +548,7 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_extras:
         extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
         extras["on_batched"] = on_bench(dev, peak=peaks()[0])
+        extras["flat_histogram"] = fh_bench(dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

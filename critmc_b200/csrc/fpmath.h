@@ -86,6 +86,108 @@ CM_HD float cm_expf(float x) {
   return cm_scale2(p, (int)k);
 }
 
+/* x * 2^k for |k| <= 2100 (double), with exact power-of-two factors */
+CM_HD double cm_scale2d(double x, int k) {
+  while (k > 1000) {
+    x = x * 0x1p1000;
+    k -= 1000;
+  }
+  while (k < -1000) {
+    x = x * 0x1p-1000;
+    k += 1000;
+  }
+  uint64_t b = (uint64_t)(k + 1023) << 52;
+  double f;
+#if defined(__CUDA_ARCH__)
+  f = __longlong_as_double((long long)b);
+#else
+  memcpy(&f, &b, 8);
+#endif
+  return x * f;
+}
+
+/* e^x in double precision: k = round(x / ln 2), r = x - k ln 2 with ln 2 split
+ * into 0x1.62e42fp-1 (25 bits, so k * hi is exact) + 0x1.df473de6af279p-26,
+ * then the Taylor series of e^r to r^13 for |r| <= 0.347 (truncation below
+ * 1e-17 relative), scaled by 2^k. */
+CM_HD double cm_exp(double x) {
+  if (x != x) return x;
+  if (x > 709.79) return INFINITY;
+  if (x < -745.2) return 0.0;
+  const double k = rint(x * 1.4426950408889634);
+  double r = x - k * 0x1.62e42fp-1;
+  r = r - k * 0x1.df473de6af279p-26;
+  double p = 1.0 / 6227020800.0; /* 1/13! */
+  p = p * r + 1.0 / 479001600.0;
+  p = p * r + 1.0 / 39916800.0;
+  p = p * r + 1.0 / 3628800.0;
+  p = p * r + 1.0 / 362880.0;
+  p = p * r + 1.0 / 40320.0;
+  p = p * r + 1.0 / 5040.0;
+  p = p * r + 1.0 / 720.0;
+  p = p * r + 1.0 / 120.0;
+  p = p * r + 1.0 / 24.0;
+  p = p * r + 1.0 / 6.0;
+  p = p * r + 0.5;
+  p = p * r + 1.0;
+  p = p * r + 1.0;
+  return cm_scale2d(p, (int)k);
+}
+
+/* natural logarithm (double): x = 2^e m with m in [sqrt(1/2), sqrt(2)),
+ * log m = 2 atanh(s), s = (m - 1) / (m + 1), |s| <= 0.1716, series to s^23 */
+CM_HD double cm_log(double x) {
+  if (!(x > 0.0)) return x == 0.0 ? -INFINITY : NAN;
+  if (x == INFINITY) return x;
+  uint64_t b;
+  int adj = 0;
+#if defined(__CUDA_ARCH__)
+  b = (uint64_t)__double_as_longlong(x);
+#else
+  memcpy(&b, &x, 8);
+#endif
+  if (((b >> 52) & 0x7FF) == 0) { /* subnormal */
+    x = x * 0x1p54;
+    adj = 54;
+#if defined(__CUDA_ARCH__)
+    b = (uint64_t)__double_as_longlong(x);
+#else
+    memcpy(&b, &x, 8);
+#endif
+  }
+  int e = (int)((b >> 52) & 0x7FF) - 1023 - adj;
+  uint64_t mb = (b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull;
+  double m;
+#if defined(__CUDA_ARCH__)
+  m = __longlong_as_double((long long)mb);
+#else
+  memcpy(&m, &mb, 8);
+#endif
+  if (m > 1.4142135623730951) {
+    m = m * 0.5;
+    e += 1;
+  }
+  const double f = m - 1.0;
+  const double s = f / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 23.0;
+  p = p * z + 1.0 / 21.0;
+  p = p * z + 1.0 / 19.0;
+  p = p * z + 1.0 / 17.0;
+  p = p * z + 1.0 / 15.0;
+  p = p * z + 1.0 / 13.0;
+  p = p * z + 1.0 / 11.0;
+  p = p * z + 1.0 / 9.0;
+  p = p * z + 1.0 / 7.0;
+  p = p * z + 1.0 / 5.0;
+  p = p * z + 1.0 / 3.0;
+  /* log m = 2 s + 2 s z p, written as f - (f - 2 s) + ... to keep f's bits:
+   * 2 s = f - s f, so log m = f - s (f - 2 z p) */
+  const double lm = f - s * (f - 2.0 * z * p);
+  const double ed = (double)e;
+  return ed * 0x1.62e42fp-1 + (ed * 0x1.df473de6af279p-26 + lm);
+}
+
 /* natural logarithm, x > 0 */
 CM_HD float cm_logf(float x) {
   if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;

@@ -346,6 +346,32 @@ int64_t critmc_stream_state_bytes(int32_t n_chains, int32_t max_lag);
 int32_t critmc_stream_update(const void* values, int32_t is_double, int32_t n_chains, int32_t n, int64_t ld,
                              double* state, int32_t max_lag, void* stream);
 
+/* ---- flat-histogram walks (Wang-Landau, multicanonical) ----------------------
+ * n_walkers independent walkers of one zero-field Ising (q = 0) or Potts
+ * (q = 2..127) lattice, one thread each.  Levels: Ising idx = (E_b + B)/4,
+ * Potts idx = E + B (B bonds), `levels` of them.  Move t of a walker uses
+ * Philox(t mod 2^32, t / 2^32, 0x0A, 0) under its key: word 0 the site
+ * ((w0 N) >> 32), word 1 the Potts proposal ((w1 (q-1)) >> 32, skipping the old
+ * state), words 2, 3 the 53-bit uniform u; accepted if ln w(new) >= ln w(old) or
+ * ln u < ln w(new) - ln w(old) (critmc's u < exp(ln w(new) - ln w(old))); a
+ * move leaving [window[0], window[1]] is rejected.  All arrays are DEVICE arrays, per walker: spins [N] (critmc site
+ * order), keys [2], idx (level), order (Ising M; Potts counts [q]), lng
+ * [levels] (mode 0 Wang-Landau: ln g, incremented by ln f each move; mode 1
+ * multicanonical: the weights ln w, read only), hist [levels] (+1 per move),
+ * window [2], trials (move counter, advanced).  Mode 0: ln_f [w] constant,
+ * or, where one_over_t [w] is set, ln f = n_levels [w] / (trials - t_base [w]
+ * + 1); `moves` per walker.  Mode 1: n_meas measurements of `moves` moves each,
+ * idx_out / order_out [w][n_meas] (Ising M, Potts sum_k n_k^2).  Walkers
+ * run in shared memory when all can be resident that way or >= 256 fit an SM,
+ * else in global memory; mode | 0x10 forces global memory, mode | 0x20 shared
+ * memory (same results).  At most 2^24 sites per walker.
+ * Replaces critmc kernels/flathist.py:28-132.                                */
+int32_t critmc_fh_run(int32_t mode, int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t q,
+                      int32_t n_walkers, const uint32_t* keys, int32_t levels, int64_t* idx, int64_t* order,
+                      double* lng, int64_t* hist, const int32_t* window, uint64_t* trials, const double* ln_f,
+                      const double* n_levels, const int32_t* one_over_t, const uint64_t* t_base, int64_t moves,
+                      int32_t n_meas, int64_t* idx_out, int64_t* order_out, void* stream);
+
 /* ---- chains owned by the library (handles) ----------------------------------
  * The library allocates and keeps a chain's lattice, running sums, Philox key
  * and sweep counter; the caller passes states in critmc's site order (first

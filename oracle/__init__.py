@@ -67,6 +67,9 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_on_run.restype = _I
     L.oracle_cluster_update.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _I, _U32, _P, _P, _P, _P]
     L.oracle_cluster_update.restype = _I
+    L.oracle_fh_run.argtypes = [_I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _P, _D, _D, _I,
+                                ctypes.c_uint64, ctypes.c_int64, _I, _P, _P]
+    L.oracle_fh_run.restype = _I
     L.oracle_ea_pt_run.argtypes = [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _P, _P, _U32, _I, _I, _I,
                                    _P, _P, _P, _P, _P]
     L.oracle_ea_pt_run.restype = _I
@@ -93,6 +96,29 @@ def cluster_update(lay: np.ndarray, shape, q: int, key, beta: float, algo: int, 
         raise MemoryError("oracle_cluster_update")
     lay[...] = flat.reshape(lay.shape)
     return de.value, dm.value, cd[:q] if q else None, st
+
+
+def fh_run(mode: int, s: np.ndarray, shape, q: int, key, idx: int, order: np.ndarray, lng: np.ndarray,
+           hist: np.ndarray, window, trials: int, ln_f: float, n_levels: float, one_over_t: bool, t_base: int,
+           moves: int, n_meas: int = 1):
+    """One walker's Wang-Landau (mode 0) or multicanonical (1) moves; arrays updated in place.
+
+    Returns (idx, trials, idx_out, order_out).
+    """
+    lx, ly, lz = _dims(shape)
+    k = np.ascontiguousarray(key, dtype=np.uint32).reshape(2)
+    i = ctypes.c_int64(idx)
+    t = ctypes.c_uint64(trials)
+    io = np.zeros(max(n_meas, 1), dtype=np.int64)
+    oo = np.zeros(max(n_meas, 1), dtype=np.int64)
+    for a, dt in ((s, np.int8), (order, np.int64), (lng, np.float64), (hist, np.int64)):
+        if a.dtype != dt or not a.flags["C_CONTIGUOUS"]:
+            raise TypeError("arrays are updated in place: pass contiguous arrays of the right dtype")
+    lib().oracle_fh_run(mode, _ptr(s), len(shape), lx, ly, lz, q, _ptr(k), ctypes.byref(i), _ptr(order),
+                        _ptr(lng), _ptr(hist), int(window[0]), int(window[1]), ctypes.byref(t), float(ln_f),
+                        float(n_levels), int(one_over_t), ctypes.c_uint64(t_base), int(moves), int(n_meas),
+                        _ptr(io), _ptr(oo))
+    return i.value, t.value, io[:n_meas], oo[:n_meas]
 
 
 def _ptr(a: np.ndarray) -> int:

@@ -122,3 +122,11 @@ def ea_exact(lattice, couplings, temperatures):
         out["q2"].append(np.sum(corr ** 2) / n ** 2)
         out["ql"].append(np.mean(corr[b[:, 0], b[:, 1]] ** 2))
     return {k: np.array(v) for k, v in out.items()}
+
+
+def ising_log_g_square6() -> np.ndarray:
+    """Exact ln g(E) of the 6x6 Ising torus, levels E = -72 + 4 j (-inf where empty)."""
+    import math
+
+    g = [int(v) for v in golden()["ising_dos_square6"]["g"]]
+    return np.array([math.log(v) if v > 0 else -np.inf for v in g])

@@ -13,3 +13,9 @@ void cm_eval(int which, const float* x, const float* y, float* out, int n) {
     }
   }
 }
+void cm_eval_d(const double* x, double* out, int n) {
+  for (int i = 0; i < n; ++i) out[i] = cm_exp(x[i]);
+}
+void cm_eval_log_d(const double* x, double* out, int n) {
+  for (int i = 0; i < n; ++i) out[i] = cm_log(x[i]);
+}

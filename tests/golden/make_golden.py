@@ -18,7 +18,7 @@ from pathlib import Path
 import numpy as np
 
 from critmc import chain, square  # noqa: F401  (critmc must be on PYTHONPATH)
-from critmc.exact import chains, enumeration, kaufman, onsager
+from critmc.exact import chains, dos, enumeration, kaufman, onsager, potts
 from critmc.stats.autocorr import gamma_method
 
 OUT = Path(__file__).resolve().parent / "critmc_exact.json"
@@ -83,6 +83,13 @@ def main() -> None:
     e = enumeration.ea_energies(lat, J)
     out["ea_square4"] = {"couplings": J.tolist(), "energies_first_64": e[:64].tolist(),
                          "energy_sum": float(e.sum()), "energy_min": float(e.min())}
+    # flat-histogram checks: exact g(E) of the 6x6 Ising torus (integers, as strings),
+    # Kaufman energies at L = 6, the 3-state Potts joint DOS on the 4x3 torus and
+    # the 10-state Potts transition point
+    out["ising_dos_square6"] = {"g": [str(v) for v in dos.ising_dos(6).g]}
+    out["kaufman_energy"]["6"] = {f"{b:.10f}": float(kaufman.energy(b, 6)) for b in (0.3, 0.44, 0.55, 0.6)}
+    out["potts3_dos_square4x3"] = joint(enumeration.potts_joint_dos(square(4, 3), 3))
+    out["potts_beta_c"] = {str(q): float(potts.beta_c(q)) for q in (3, 10)}
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

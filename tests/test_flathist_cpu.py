@@ -1,0 +1,123 @@
+"""Flat-histogram sampling on the CPU: level mapping and window walk (host
+logic), and the oracle's Wang-Landau / multicanonical walks pinned against
+exact densities of states (critmc tests/test_flathist.py patterns)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from exact_helpers import JointDOS, ising_log_g_square6, kaufman_energy
+from flathist_replay import replay_multicanonical, replay_wang_landau
+
+from critmc_b200 import Ising, Potts, square
+from critmc_b200.flathist import EnergyLevels, MucaResult, WLResult, _walk_into_window
+
+
+def test_energy_levels_mapping():
+    lv = EnergyLevels.of(Ising(square(4)))
+    assert lv.size == 17
+    assert lv.energies[0] == -32 and lv.energies[-1] == 32
+    assert lv.index(-24) == 2
+    pv = EnergyLevels.of(Potts(square(4), 3))
+    assert pv.size == 33 and pv.index(-32) == 0
+    assert lv.window(-2.0, 0.0) == (0, 8)
+    with pytest.raises(ValueError):
+        lv.window(0.5, 0.5)
+    with pytest.raises(ValueError):
+        EnergyLevels.of(Ising(square(4), h=0.1))
+
+
+@pytest.mark.parametrize("kind", ["ising", "potts"])
+def test_walk_into_window_reaches_the_window(kind):
+    model = Ising(square(8)) if kind == "ising" else Potts(square(6), 4)
+    lv = EnergyLevels.of(model)
+    lo, hi = lv.window(-1.9, -1.6) if kind == "ising" else lv.window(-1.5, -1.2)
+    rng = np.random.default_rng(5)
+    s = model.initial_state("random", rng)
+    idx = _walk_into_window(model, s, lv, lo, hi, rng)
+    assert lo <= idx <= hi and idx == lv.index(model.energy(s))
+
+
+def _walker(model, seed, window):
+    lv = EnergyLevels.of(model)
+    rng = np.random.default_rng(seed)
+    s = model.initial_state("random", rng)
+    idx = _walk_into_window(model, s, lv, *window, rng)
+    key = rng.integers(0, 1 << 32, size=2, dtype=np.uint64).astype(np.uint32)
+    return lv, s.astype(np.int8), idx, key
+
+
+@pytest.mark.parametrize("one_over_t", [False, True])
+def test_oracle_wang_landau_ising_against_exact_dos(one_over_t):
+    model = Ising(square(6))
+    lv = EnergyLevels.of(model)
+    window = (0, lv.size - 1)
+    lv, s, idx, key = _walker(model, 3, window)
+    r = replay_wang_landau((6, 6), 0, s, key, idx, window, lv.size, 36, 1e-6, one_over_t=one_over_t)
+    res = WLResult(lv, r["ln_g"], r["visited"], window, r["trials"], r["ln_f"], 0.0, r["stages"])
+    exact = ising_log_g_square6()
+    v = res.visited
+    assert np.array_equal(v, np.isfinite(exact))
+    err = np.abs(res.normalized()[v] - exact[v])
+    assert err.mean() < (0.02 if one_over_t else 0.08)
+    betas = [0.3, 0.44, 0.6]
+    th = res.canonical(betas)
+    tol = 0.01 if one_over_t else 0.03
+    assert np.allclose(th["u"], [kaufman_energy(b, 6) for b in betas], atol=tol)
+    assert res.stages[0]["ln_f"] == 1.0
+
+
+def test_oracle_wang_landau_potts_window():
+    model = Potts(square(4, 3), 3)
+    jd = JointDOS("potts3_dos_square4x3")
+    exact = dict(zip(jd.energies, np.log(jd.counts.sum(axis=1))))
+    lv = EnergyLevels.of(model)
+    window = lv.window(-2.0, -1.0)
+    lv, s, idx, key = _walker(model, 4, window)
+    r = replay_wang_landau((4, 3), 3, s, key, idx, window, lv.size, 12, 1e-7)
+    res = WLResult(lv, r["ln_g"], r["visited"], window, r["trials"], r["ln_f"], 0.0)
+    got = res.normalized()
+    e = lv.energies
+    diff = got[res.visited] - np.array([exact[x] for x in e[res.visited]])
+    assert np.ptp(diff) < 0.02
+    assert e[res.visited].max() <= -12
+
+
+def test_oracle_multicanonical_reweighting_to_canonical():
+    model = Ising(square(6))
+    lng = ising_log_g_square6()
+    lv = EnergyLevels.of(model)
+    window = (0, lv.size - 1)
+    lv, s, idx, key = _walker(model, 8, window)
+    ln_w = np.where(np.isfinite(lng), -lng, -np.inf)
+    r = replay_multicanonical((6, 6), 0, s, key, idx, window, ln_w, 36, 200_000, n_therm=100)
+    out = MucaResult(lv, lng, r["level_series"], r["order_series"], window, r["hist"])
+    assert (out.hist > 0).sum() == np.isfinite(lng).sum()
+    for b in (0.3, 0.44, 0.55):
+        assert out.canonical(b)["u"][0] == pytest.approx(kaufman_energy(b, 6), abs=0.01)
+    # the order series is the magnetisation of the configuration: check the last one
+    assert r["order_series"][-1] == int(r["state"].astype(np.int64).sum())
+
+
+def test_oracle_multicanonical_potts_order_series_and_m2():
+    model = Potts(square(4, 2), 3)
+    jd = JointDOS("potts3_dos_square4x2")
+    lv = EnergyLevels.of(model)
+    g = jd.counts.sum(axis=1)
+    lng = np.full(lv.size, -np.inf)
+    for e, c in zip(jd.energies, g):
+        if c > 0:
+            lng[lv.index(e)] = np.log(c)
+    window = (0, lv.size - 1)
+    lv, s, idx, key = _walker(model, 2, window)
+    ln_w = np.where(np.isfinite(lng), -lng, -np.inf)
+    r = replay_multicanonical((4, 2), 3, s, key, idx, window, ln_w, 8, 100_000)
+    out = MucaResult(lv, lng, r["level_series"], r["order_series"], window, r["hist"])
+    counts = np.bincount(r["state"].astype(np.int64), minlength=3)
+    assert r["order_series"][-1] == int((counts ** 2).sum())
+    beta, n = 0.8, 8
+    # the fixture's order variable is q sum_k n_k^2
+    exact_m2 = jd.average(beta, lambda e, o: (o / n ** 2 - 1.0) / 2.0)
+    got = out.canonical(beta)
+    assert got["m2"][0] == pytest.approx(exact_m2, abs=0.02)
+    assert got["u"][0] == pytest.approx(jd.average(beta, lambda e, o: e) / n, abs=0.02)

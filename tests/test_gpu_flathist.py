@@ -1,0 +1,282 @@
+"""Flat-histogram walkers on the GPU: the kernel bit-identical to the oracle
+for every model and mode, the Wang-Landau and multicanonical drivers
+bit-identical to the CPU replay of their schedules, and critmc's own
+statistical checks (critmc tests/test_flathist.py)."""
+
+from __future__ import annotations
+
+import zlib
+
+import numpy as np
+import pytest
+import torch
+from exact_helpers import JointDOS, ising_log_g_square6, kaufman_energy
+from flathist_replay import initial_order, replay_multicanonical, replay_wang_landau
+
+import oracle
+from critmc_b200 import Ising, Potts, hypercubic, square
+from critmc_b200 import _lib
+from critmc_b200.device import ptr, stream_handle
+from critmc_b200.flathist import EnergyLevels, Multicanonical, WangLandau, _walk_into_window
+
+pytestmark = pytest.mark.gpu
+
+KERNEL_CASES = [
+    ("ising", (6, 6), 0),
+    ("ising", (4, 4, 4), 0),
+    ("ising", (16,), 0),
+    ("ising", (10, 6), 0),
+    ("potts", (4, 3), 3),
+    ("potts", (8, 8), 10),
+    ("potts", (4, 2, 2), 4),
+]
+
+
+def _model(kind, shape, q):
+    lat = hypercubic(shape)
+    return Ising(lat) if kind == "ising" else Potts(lat, q)
+
+
+@pytest.mark.parametrize("path", ["shared", "global"])
+@pytest.mark.parametrize("mode", ["wl", "wl_1t", "muca"])
+@pytest.mark.parametrize("kind,shape,q", KERNEL_CASES)
+def test_fh_kernel_bit_identical_to_oracle(cuda, kind, shape, q, mode, path):
+    model = _model(kind, shape, q)
+    lv = EnergyLevels.of(model)
+    n = model.n_sites
+    rng = np.random.default_rng(zlib.crc32(repr((kind, shape, mode)).encode()))
+    mid = lv.size // 2
+    windows = [(0, lv.size - 1), (max(0, mid - 4), min(lv.size - 1, mid + 3)), (1, lv.size - 2)]
+    W = len(windows)
+    states, idxs, orders = [], [], []
+    for lo, hi in windows:
+        s = model.initial_state("random", rng)
+        idxs.append(_walk_into_window(model, s, lv, lo, hi, rng))
+        states.append(s.astype(np.int8))
+        orders.append(initial_order(s, q))
+    keys = rng.integers(0, 1 << 32, size=(W, 2), dtype=np.uint64).astype(np.uint32)
+    lng = rng.normal(0.0, 2.0, size=(W, lv.size))
+    if mode == "muca":
+        lng[:, 0] = -np.inf  # a forbidden level
+    hist = rng.integers(0, 5, size=(W, lv.size)).astype(np.int64)
+    ln_f = np.array([0.5, 0.125, 1e-3])
+    n_lev = np.array([float(hi - lo + 1) for lo, hi in windows])
+    one_t = np.full(W, 1 if mode == "wl_1t" else 0, dtype=np.int32)
+    t_base = np.array([0, 3, 7], dtype=np.uint64)
+    trials = t_base.copy()
+    # device copies
+    d = dict(spins=torch.from_numpy(np.stack(states)).to(cuda), keys=torch.from_numpy(keys.view(np.int32)).to(cuda),
+             idx=torch.tensor(idxs, dtype=torch.int64, device=cuda),
+             order=torch.from_numpy(np.concatenate(orders)).to(cuda), lng=torch.from_numpy(lng.copy()).to(cuda),
+             hist=torch.from_numpy(hist.copy()).to(cuda),
+             window=torch.tensor(np.array(windows, dtype=np.int32), device=cuda),
+             trials=torch.from_numpy(trials.view(np.int64).copy()).to(cuda),
+             ln_f=torch.from_numpy(ln_f).to(cuda), n_lev=torch.from_numpy(n_lev).to(cuda),
+             one_t=torch.from_numpy(one_t).to(cuda), t_base=torch.from_numpy(t_base.view(np.int64)).to(cuda))
+    is_muca = mode == "muca"
+    moves, n_meas = (3 * n, 7) if is_muca else (40 * n, 1)
+    lx, ly, lz = tuple(shape) + (1,) * (3 - len(shape))
+    ref = [dict(s=states[w].copy(), order=orders[w].copy(), lng=lng[w].copy(), hist=hist[w].copy(),
+                idx=idxs[w], trials=int(trials[w])) for w in range(W)]
+    for block in range(2):
+        io = torch.zeros((W, n_meas), dtype=torch.int64, device=cuda) if is_muca else None
+        oo = torch.zeros_like(io) if is_muca else None
+        flags = 0x10 if path == "global" else 0x20
+        _lib.call("critmc_fh_run", int(is_muca) | flags, ptr(d["spins"]), len(shape), lx, ly, lz, q, W, ptr(d["keys"]),
+                  lv.size, ptr(d["idx"]), ptr(d["order"]), ptr(d["lng"]), ptr(d["hist"]), ptr(d["window"]),
+                  ptr(d["trials"]), ptr(d["ln_f"]), ptr(d["n_lev"]), ptr(d["one_t"]), ptr(d["t_base"]), moves,
+                  n_meas, ptr(io), ptr(oo), stream_handle(cuda))
+        torch.cuda.synchronize()
+        for w in range(W):
+            r = ref[w]
+            r["idx"], r["trials"], r_io, r_oo = oracle.fh_run(
+                int(is_muca), r["s"], shape, q, keys[w], r["idx"], r["order"], r["lng"], r["hist"], windows[w],
+                r["trials"], ln_f[w], n_lev[w], bool(one_t[w]), int(t_base[w]), moves, n_meas)
+            if is_muca:
+                np.testing.assert_array_equal(io[w].cpu().numpy(), r_io)
+                np.testing.assert_array_equal(oo[w].cpu().numpy(), r_oo)
+        np.testing.assert_array_equal(d["spins"].cpu().numpy(), np.stack([r["s"] for r in ref]))
+        np.testing.assert_array_equal(d["idx"].cpu().numpy(), [r["idx"] for r in ref])
+        np.testing.assert_array_equal(d["trials"].cpu().numpy(), [r["trials"] for r in ref])
+        np.testing.assert_array_equal(d["hist"].cpu().numpy(), np.stack([r["hist"] for r in ref]))
+        got_lng = d["lng"].cpu().numpy()
+        assert np.array_equal(got_lng, np.stack([r["lng"] for r in ref]), equal_nan=True)
+        if q == 0:
+            np.testing.assert_array_equal(d["order"].cpu().numpy(), [r["order"][0] for r in ref])
+        else:
+            np.testing.assert_array_equal(d["order"].cpu().numpy(), np.concatenate([r["order"] for r in ref]))
+    # the configurations stay consistent with their levels and orders
+    for w, r in enumerate(ref):
+        assert lv.index(model.energy(r["s"])) == r["idx"]
+        assert windows[w][0] <= r["idx"] <= windows[w][1]
+
+
+@pytest.mark.parametrize("kind,shape,q", [("ising", (8, 8), 0), ("potts", (6, 5), 5)])
+def test_shared_and_global_paths_agree_over_many_blocks(cuda, kind, shape, q):
+    """70 walkers: three blocks of the shared-memory kernel, the last one partial."""
+    model = _model(kind, shape, q)
+    out = []
+    for memory in ("shared", "global"):
+        wl = WangLandau(model, seed=21, n_walkers=70)
+        W = wl.walkers
+        lng = torch.zeros((70, wl.levels.size), dtype=torch.float64, device=cuda)
+        lnf = torch.full((70,), 0.01, dtype=torch.float64, device=cuda)
+        one_t = torch.tensor([w % 2 for w in range(70)], dtype=torch.int32, device=cuda)
+        for _ in range(3):
+            W.run(0, lng, 5 * model.n_sites, ln_f=lnf, n_levels=lnf * 100, one_over_t=one_t,
+                  t_base=torch.zeros(70, dtype=torch.int64, device=cuda), memory=memory)
+        out.append([x.cpu().numpy() for x in (lng, W.hist, W.spins, W.idx, W.order, W.trials)])
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+def _start(walkers, w):
+    return (walkers.spins[w].cpu().numpy().copy(), int(walkers.idx[w]), walkers.keys[w].cpu().numpy().view(np.uint32))
+
+
+def test_wang_landau_matches_replay(cuda):
+    model = Ising(square(4))
+    wl = WangLandau(model, seed=1)
+    s, idx, key = _start(wl.walkers, 0)
+    res = wl.run(1e-4, checkpoints=[1000, 50_000, 10**9])
+    lv = res.levels
+    r = replay_wang_landau((4, 4), 0, s, key, idx, wl.window, lv.size, 16, 1e-4, checkpoints=[1000, 50_000, 10**9])
+    assert np.array_equal(res.ln_g, r["ln_g"])
+    assert np.array_equal(res.visited, r["visited"])
+    assert res.trials == r["trials"] and res.ln_f == r["ln_f"] and res.stages == r["stages"]
+    assert [c[0] for c in res.checkpoints] == [1000, 50_000, 10**9]
+    for a, b in zip(res.checkpoints, r["checkpoints"]):
+        assert a[1] == b[1] and np.array_equal(a[2], b[2])
+
+
+def test_wang_landau_batch_of_windows_matches_replay(cuda):
+    model = Potts(square(4, 3), 3)
+    wins = [None, (-2.0, -1.0), (-1.5, -0.5), (None, -0.8)]
+    wl = WangLandau(model, e_window=wins, n_walkers=4, seed=2, criterion="visit")
+    starts = [_start(wl.walkers, w) for w in range(4)]
+    results = wl.run(1e-3, one_over_t=True, check_sweeps=50)
+    assert len(results) == 4
+    for w, res in enumerate(results):
+        s, idx, key = starts[w]
+        r = replay_wang_landau((4, 3), 3, s, key, idx, wl.windows[w], res.levels.size, 12, 1e-3, check_sweeps=50,
+                               criterion="visit")
+        assert res.window == wl.windows[w]
+        assert np.array_equal(res.ln_g, r["ln_g"]), w
+        assert res.trials == r["trials"] and res.stages == r["stages"]
+
+
+@pytest.mark.parametrize("n_walkers", [1, 4])
+def test_multicanonical_matches_replay(cuda, n_walkers):
+    model = Ising(square(6))
+    lng = ising_log_g_square6()
+    mu = Multicanonical(model, lng, seed=8, n_walkers=n_walkers)
+    starts = [_start(mu.walkers, w) for w in range(n_walkers)]
+    out = mu.run(3000, sweeps_per_meas=2, n_therm=50)
+    outs = out if n_walkers > 1 else [out]
+    for w, o in enumerate(outs):
+        s, idx, key = starts[w]
+        r = replay_multicanonical((6, 6), 0, s, key, idx, mu.window, mu.ln_w, 72, 3000, n_therm=50)
+        np.testing.assert_array_equal(o.level_series, r["level_series"])
+        np.testing.assert_array_equal(o.order_series, r["order_series"])
+        np.testing.assert_array_equal(o.hist, r["hist"])
+
+
+# ---- critmc's statistical checks (tests/test_flathist.py) ----
+
+
+@pytest.mark.parametrize("one_over_t", [False, True])
+def test_wang_landau_ising_against_exact_dos(cuda, one_over_t):
+    wl = WangLandau(Ising(square(6)), seed=3, criterion="flat")
+    res = wl.run(1e-6, one_over_t=one_over_t)
+    exact = ising_log_g_square6()
+    got = res.normalized()
+    v = res.visited
+    assert np.array_equal(v, np.isfinite(exact))
+    err = np.abs(got[v] - exact[v])
+    assert err.mean() < (0.02 if one_over_t else 0.08)
+    betas = [0.3, 0.44, 0.6]
+    th = res.canonical(betas)
+    tol = 0.01 if one_over_t else 0.03
+    assert np.allclose(th["u"], [kaufman_energy(b, 6) for b in betas], atol=tol)
+
+
+def test_wang_landau_batch_of_seeds_against_exact_dos(cuda):
+    """Independent walkers in one launch: each converges, and their spread is the error bar."""
+    results = WangLandau(Ising(square(6)), seed=11, n_walkers=64).run(1e-5)
+    exact = ising_log_g_square6()
+    v = np.isfinite(exact)
+    errs = np.array([np.abs(r.normalized()[v] - exact[v]).mean() for r in results])
+    assert (errs < 0.08).all() and np.median(errs) < 0.04
+    mean = np.mean([r.normalized()[v] for r in results], axis=0)
+    assert np.abs(mean - exact[v]).mean() < 0.01
+
+
+def test_wang_landau_checkpoints_and_stages(cuda):
+    res = WangLandau(Ising(square(4)), seed=1).run(1e-5, checkpoints=[10_000, 100_000, 1_000_000])
+    assert [c[0] for c in res.checkpoints] == [10_000, 100_000, 1_000_000]
+    assert res.stages and res.stages[0]["ln_f"] == 1.0
+
+
+def test_wang_landau_potts_window(cuda):
+    lat = square(4, 3)
+    jd = JointDOS("potts3_dos_square4x3")
+    exact = dict(zip(jd.energies, np.log(jd.counts.sum(axis=1))))
+    res = WangLandau(Potts(lat, 3), e_window=(-2.0, -1.0), seed=4).run(1e-7)
+    got = res.normalized()
+    lv = res.levels.energies
+    diff = got[res.visited] - np.array([exact[e] for e in lv[res.visited]])
+    assert np.ptp(diff) < 0.02
+    assert lv[res.visited].max() <= -12
+
+
+def test_multicanonical_reweighting_to_canonical(cuda):
+    exact_lng = ising_log_g_square6()
+    out = Multicanonical(Ising(square(6)), exact_lng, seed=8).run(200_000, sweeps_per_meas=1, n_therm=100)
+    assert (out.hist > 0).sum() == np.isfinite(exact_lng).sum()
+    for b in (0.3, 0.44, 0.55):
+        assert out.canonical(b)["u"][0] == pytest.approx(kaufman_energy(b, 6), abs=0.01)
+
+
+def test_multicanonical_potts_double_peak(cuda):
+    from exact_helpers import golden
+
+    model = Potts(square(8), 10)
+    res = WangLandau(model, e_window=(-1.95, -0.6), seed=9).run(1e-5)
+    out = Multicanonical(model, res.ln_g, e_window=(-1.95, -0.6), seed=10).run(100_000)
+    bc = float(golden()["potts_beta_c"]["10"])
+    b = out.equal_height_beta((bc - 0.05, bc + 0.05), split=-1.3)
+    dp = out.double_peak(b, split=-1.3)
+    assert dp["p_ordered"] == pytest.approx(dp["p_disordered"], rel=1e-6)
+    assert dp["e_ordered"] < -1.5 < -1.1 < dp["e_disordered"]
+    assert abs(b - bc) < 0.05
+
+
+def _wl_result_with_a_missed_level(L=6, level=12):
+    res = WangLandau(Ising(square(L)), seed=3).run(1e-5)
+    assert res.visited[level]
+    res.ln_g[level] = 0.0
+    res.visited[level] = False
+    return res, level
+
+
+def test_multicanonical_raw_ln_g_traps_the_walk_on_an_unvisited_level(cuda):
+    res, level = _wl_result_with_a_missed_level()
+    out = Multicanonical(Ising(square(6)), res.ln_g, seed=4).run(5000)
+    assert out.hist[level] > 0.99 * out.hist.sum()
+
+
+def test_multicanonical_forbids_levels_wang_landau_never_visited(cuda):
+    res, level = _wl_result_with_a_missed_level()
+    out = Multicanonical(Ising(square(6)), res, seed=4).run(50_000)
+    assert out.hist[level] == 0
+    sampled = out.hist > 0
+    assert np.array_equal(sampled, res.visited)
+    assert out.hist[sampled].min() > 0.3 * out.hist[sampled].mean()
+
+
+def test_multicanonical_wl_result_matches_its_array_when_all_levels_were_visited(cuda):
+    model = Potts(square(6), 10)
+    res = WangLandau(model, e_window=(-1.95, -0.6), seed=9).run(1e-4)
+    a = Multicanonical(model, res.ln_g, e_window=(-1.95, -0.6), seed=10).run(5000)
+    b = Multicanonical(model, res, e_window=(-1.95, -0.6), seed=10).run(5000)
+    np.testing.assert_array_equal(a.level_series, b.level_series)

@@ -43,7 +43,8 @@ def nvcc() -> str:
 
 
 # translation units whose float arithmetic must match a host replay exactly
-PER_FILE_FLAGS = {"on_models.cu": ["--fmad=false"], "ea_pt.cu": ["--fmad=false"], "flathist.cu": ["--fmad=false"]}
+PER_FILE_FLAGS = {"on_models.cu": ["--fmad=false"], "ea_pt.cu": ["--fmad=false"], "flathist.cu": ["--fmad=false"],
+                  "cluster.cu": ["--fmad=false"]}
 
 
 def _headers() -> list[Path]:

@@ -74,6 +74,7 @@ SIGNATURES: dict[str, tuple] = {
     "critmc_stream_update": (_I32, [_P, _I32, _I32, _I32, _I64, _P, _I32, _P]),
     "critmc_cluster_update": (
         _I32, [_I32, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _D, _I32, _U32, _P, _P, _P, _P, _P]),
+    "critmc_on_cluster_update": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _D, _I32, _U32, _P, _P, _P]),
     "critmc_chain_create": (_I32, [_I32, _P, _I32, _D, _U32, _U32, ctypes.c_uint64, _I32, _P, _P]),
     "critmc_chain_destroy": (_I32, [_P]),
     "critmc_chain_info": (_I32, [_P, _P, _P, _P]),

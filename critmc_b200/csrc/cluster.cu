@@ -17,13 +17,25 @@
 // magnetisation (or Potts counts) are updated exactly from the changed bonds
 // and sites.
 //
+// O(n) chains (FP32 unit spins, colour-major structure of arrays) use the
+// embedded Ising model of a random axis r: Philox(0, sweep, 0x0B, 0) gives r
+// (XY: angle 2 pi u0; Heisenberg: z = 2 u0 - 1 and angle 2 pi u1, uniform on
+// the sphere), p_i = S_i . r, a bond is active when p_i p_j > 0 and the 24-bit
+// uniform of its word is below 1 - exp(-2 beta p_i p_j), and a flipped
+// cluster is reflected, S_i <- S_i - 2 p_i r.  The float arithmetic uses
+// fpmath.h and this file is compiled without contraction, so the CPU replay
+// follows bit for bit.
+//
 // Replaces critmc src/critmc/kernels/ising.py:111-171 (wolff_update,
-// sw_update) and kernels/potts.py:107-168; statistics as critmc's aux columns
-// (kernels/common.py:35-39: summed Wolff size, SW sum |C|^2 and cluster count).
+// sw_update), kernels/potts.py:107-168 and kernels/on.py:265-345; statistics
+// as critmc's aux columns (kernels/common.py:35-39: summed Wolff size, SW
+// sum |C|^2 and cluster count).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
 #include "common.cuh"
+#include "fpmath.h"
 #include "geom.cuh"
 #include "host_common.h"
 
@@ -31,7 +43,7 @@ namespace critmc {
 
 constexpr int CL_THREADS = 256;
 constexpr int CL_PCHAINS = 256;
-constexpr uint32_t TAG_BOND = 0x07u, TAG_CLFLIP = 0x08u, TAG_WOLFF = 0x09u;
+constexpr uint32_t TAG_BOND = 0x07u, TAG_CLFLIP = 0x08u, TAG_WOLFF = 0x09u, TAG_ONAXIS = 0x0Bu;
 
 struct ClParams {
   void* spins;
@@ -45,6 +57,9 @@ struct ClParams {
   uint32_t n;            // sites per chain (2 slots)
   int bits;              // 1: bit layout, 0: int8
   int potts, q, algo, chain0;
+  int on_n;              // O(n) chains: components (2, 3); 0 for Ising / Potts
+  float* proj;           // O(n): [n_chains][N] projections on the axis
+  float nb2;             // O(n): -2 beta
   uint32_t thr, sweep;
   uint32_t keys[CL_PCHAINS][2];
 };
@@ -84,10 +99,44 @@ __device__ __forceinline__ void cl_unite(int* L, int a, int b) {
   }
 }
 
+// the reflection axis of an O(n) chain for this update
+__device__ __forceinline__ void cl_axis(const ClParams& P, int lchain, float* r) {
+  const critmc_u32x4 w = critmc_philox4x32(0u, P.sweep, TAG_ONAXIS, 0u, P.keys[lchain][0], P.keys[lchain][1]);
+  const float two_pi = 6.28318530717958647692f;
+  float sn, cs;
+  if (P.on_n == 2) {
+    cm_sincosf(two_pi * critmc_u01f(w.v[0]), &sn, &cs);
+    r[0] = cs;
+    r[1] = sn;
+    r[2] = 0.0f;
+  } else {
+    const float z = 2.0f * critmc_u01f(w.v[0]) - 1.0f;
+    const float rho = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    cm_sincosf(two_pi * critmc_u01f(w.v[1]), &sn, &cs);
+    r[0] = rho * cs;
+    r[1] = rho * sn;
+    r[2] = z;
+  }
+}
+
+__device__ __forceinline__ const float* cl_on_spins(const ClParams& P, int chain) {
+  return static_cast<const float*>(P.spins) + (size_t)chain * P.on_n * P.n;
+}
+
 __global__ void cl_init_kernel(ClParams P) {
-  const int chain = P.chain0 + blockIdx.y;
+  const int lchain = blockIdx.y, chain = P.chain0 + lchain;
   int* L = P.label + (size_t)chain * P.n;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < P.n; u += gridDim.x * blockDim.x) L[u] = (int)u;
+  float r[3];
+  if (P.on_n) cl_axis(P, lchain, r);
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < P.n; u += gridDim.x * blockDim.x) {
+    L[u] = (int)u;
+    if (P.on_n) {
+      const float* S = cl_on_spins(P, chain);
+      float p = S[u] * r[0] + S[P.n + u] * r[1];
+      if (P.on_n == 3) p = p + S[2 * (size_t)P.n + u] * r[2];
+      P.proj[(size_t)chain * P.n + u] = p;
+    }
+  }
 }
 
 template <int Z>
@@ -100,10 +149,22 @@ __global__ void __launch_bounds__(CL_THREADS) cl_link_kernel(const __grid_consta
     byte_row_index(P.g, s, r, i);
     uint32_t nb[Z];
     byte_neighbours<Z>(P.g, 0, r, i, nb);
-    const int v0 = cl_val(P, chain, s);
     const critmc_u32x4 w0 = critmc_philox4x32(s, P.sweep, TAG_BOND, 0u, k0, k1);
     critmc_u32x4 w1 = w0;
     if constexpr (Z == 6) w1 = critmc_philox4x32(s, P.sweep, TAG_BOND | (1u << 8), 0u, k0, k1);
+    if (P.on_n) {
+      const float* pr = P.proj + (size_t)chain * P.n;
+      const float p0 = pr[s];
+#pragma unroll
+      for (int q = 0; q < Z; ++q) {
+        const uint32_t u1 = P.g.slots + nb[q];
+        const uint32_t word = q < 4 ? w0.v[q] : w1.v[q - 4];
+        const float x = p0 * pr[u1];
+        if (x > 0.0f && critmc_u01f(word) < 1.0f - cm_expf(P.nb2 * x)) cl_unite(L, (int)s, (int)u1);
+      }
+      continue;
+    }
+    const int v0 = cl_val(P, chain, s);
 #pragma unroll
     for (int q = 0; q < Z; ++q) {
       const uint32_t u1 = P.g.slots + nb[q];
@@ -139,12 +200,26 @@ __global__ void __launch_bounds__(CL_THREADS) cl_decide_kernel(const __grid_cons
     const critmc_u32x4 w = critmc_philox4x32(0u, P.sweep, TAG_WOLFF, 0u, k0, k1);
     const uint32_t seed = (uint32_t)(((unsigned long long)w.v[0] * P.n) >> 32);
     root = L[seed];
-    const int old = cl_val(P, chain, seed);
-    wnew = P.potts ? (old + 1 + (int)(((unsigned long long)w.v[1] * (unsigned)(P.q - 1)) >> 32)) % P.q : -old;
+    if (!P.on_n) {
+      const int old = cl_val(P, chain, seed);
+      wnew = P.potts ? (old + 1 + (int)(((unsigned long long)w.v[1] * (unsigned)(P.q - 1)) >> 32)) % P.q : -old;
+    }
   }
   long long flipped = 0;
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < P.n; u += gridDim.x * blockDim.x) {
     const int r = L[u];
+    if (P.on_n) {  // O(n): newv is the reflect flag
+      int f = 0;
+      if (P.algo == CRITMC_WOLFF) {
+        f = r == root;
+        flipped += f;
+      } else {
+        atomicAdd(&S[r], 1);
+        f = (int)(critmc_philox4x32((uint32_t)r, P.sweep, TAG_CLFLIP, 0u, k0, k1).v[0] >> 31);
+      }
+      nv[u] = (int8_t)f;
+      continue;
+    }
     const int old = cl_val(P, chain, u);
     int v = old;
     if (P.algo == CRITMC_WOLFF) {
@@ -269,13 +344,58 @@ __global__ void __launch_bounds__(CL_THREADS) cl_apply_kernel(const __grid_const
   }
 }
 
+// O(n): reflect the spins of the flipped clusters, S <- S - 2 p r
+__global__ void __launch_bounds__(CL_THREADS) cl_on_apply_kernel(const __grid_constant__ ClParams P) {
+  const int lchain = blockIdx.y, chain = P.chain0 + lchain;
+  const int8_t* nv = P.newv + (size_t)chain * P.n;
+  const float* pr = P.proj + (size_t)chain * P.n;
+  float* S = static_cast<float*>(P.spins) + (size_t)chain * P.on_n * P.n;
+  float r[3];
+  cl_axis(P, lchain, r);
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < P.n; u += gridDim.x * blockDim.x) {
+    if (!nv[u]) continue;
+    const float tp = 2.0f * pr[u];
+    for (int c = 0; c < P.on_n; ++c) S[(size_t)c * P.n + u] = S[(size_t)c * P.n + u] - tp * r[c];
+  }
+}
+
+static int cl_launch(ClParams& P, int n_chains, const uint32_t* keys, cudaStream_t s) {
+  const unsigned bx_sites = std::min<unsigned>(4096, (P.n + CL_THREADS - 1) / CL_THREADS);
+  const unsigned bx_slots = std::min<unsigned>(4096, (P.g.slots + CL_THREADS - 1) / CL_THREADS);
+  const unsigned bx_words = std::min<unsigned>(4096, ((P.n >> 5) + CL_THREADS - 1) / CL_THREADS);
+  for (int c0 = 0; c0 < n_chains; c0 += CL_PCHAINS) {
+    const int nc = std::min(CL_PCHAINS, n_chains - c0);
+    P.chain0 = c0;
+    std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
+    if (P.algo == CRITMC_SWENDSEN_WANG) cl_sw_clear_kernel<<<(nc + 127) / 128, 128, 0, s>>>(P.stats, c0, nc);
+    const dim3 gs(bx_sites, nc), gb(bx_slots, nc), gw(std::max(1u, bx_words), nc);
+    cl_init_kernel<<<gs, CL_THREADS, 0, s>>>(P);
+    if (P.g.dim == 1) cl_link_kernel<2><<<gb, CL_THREADS, 0, s>>>(P);
+    else if (P.g.dim == 2) cl_link_kernel<4><<<gb, CL_THREADS, 0, s>>>(P);
+    else cl_link_kernel<6><<<gb, CL_THREADS, 0, s>>>(P);
+    cl_flatten_kernel<<<gs, CL_THREADS, 0, s>>>(P);
+    cl_decide_kernel<<<gs, CL_THREADS, 0, s>>>(P);
+    if (P.algo == CRITMC_SWENDSEN_WANG) cl_sw_stats_kernel<<<gs, CL_THREADS, 0, s>>>(P);
+    if (P.on_n) {
+      cl_on_apply_kernel<<<gs, CL_THREADS, 0, s>>>(P);
+    } else {
+      if (P.g.dim == 1) cl_delta_kernel<2><<<gb, CL_THREADS, 0, s>>>(P);
+      else if (P.g.dim == 2) cl_delta_kernel<4><<<gb, CL_THREADS, 0, s>>>(P);
+      else cl_delta_kernel<6><<<gb, CL_THREADS, 0, s>>>(P);
+      cl_apply_kernel<<<P.bits ? gw : gs, CL_THREADS, 0, s>>>(P);
+    }
+    if (int e = cuda_check("launch")) return e;
+  }
+  return CRITMC_OK;
+}
+
 }  // namespace critmc
 
 using namespace critmc;
 
 extern "C" int64_t critmc_cluster_scratch_bytes(int32_t n_chains, int64_t n_sites) {
   if (n_chains < 1 || n_sites < 2) return -1;
-  return (int64_t)n_chains * n_sites * (4 + 4 + 1) + 256;
+  return (int64_t)n_chains * n_sites * (4 + 4 + 4 + 1) + 256;
 }
 
 extern "C" int32_t critmc_cluster_update(int32_t bits, void* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
@@ -311,29 +431,43 @@ extern "C" int32_t critmc_cluster_update(int32_t bits, void* spins, int32_t dim,
   char* base = static_cast<char*>(scratch);
   P.label = reinterpret_cast<int*>(base);
   P.size = reinterpret_cast<int*>(base + (size_t)n_chains * P.n * 4);
-  P.newv = reinterpret_cast<int8_t*>(base + (size_t)n_chains * P.n * 8);
-  cudaStream_t s = (cudaStream_t)stream;
-  const unsigned bx_sites = std::min<unsigned>(4096, (P.n + CL_THREADS - 1) / CL_THREADS);
-  const unsigned bx_slots = std::min<unsigned>(4096, (P.g.slots + CL_THREADS - 1) / CL_THREADS);
-  const unsigned bx_words = std::min<unsigned>(4096, ((P.n >> 5) + CL_THREADS - 1) / CL_THREADS);
-  for (int c0 = 0; c0 < n_chains; c0 += CL_PCHAINS) {
-    const int nc = std::min(CL_PCHAINS, n_chains - c0);
-    P.chain0 = c0;
-    std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
-    if (algo == CRITMC_SWENDSEN_WANG) cl_sw_clear_kernel<<<(nc + 127) / 128, 128, 0, s>>>(P.stats, c0, nc);
-    const dim3 gs(bx_sites, nc), gb(bx_slots, nc), gw(std::max(1u, bx_words), nc);
-    cl_init_kernel<<<gs, CL_THREADS, 0, s>>>(P);
-    if (P.g.dim == 1) cl_link_kernel<2><<<gb, CL_THREADS, 0, s>>>(P);
-    else if (P.g.dim == 2) cl_link_kernel<4><<<gb, CL_THREADS, 0, s>>>(P);
-    else cl_link_kernel<6><<<gb, CL_THREADS, 0, s>>>(P);
-    cl_flatten_kernel<<<gs, CL_THREADS, 0, s>>>(P);
-    cl_decide_kernel<<<gs, CL_THREADS, 0, s>>>(P);
-    if (algo == CRITMC_SWENDSEN_WANG) cl_sw_stats_kernel<<<gs, CL_THREADS, 0, s>>>(P);
-    if (P.g.dim == 1) cl_delta_kernel<2><<<gb, CL_THREADS, 0, s>>>(P);
-    else if (P.g.dim == 2) cl_delta_kernel<4><<<gb, CL_THREADS, 0, s>>>(P);
-    else cl_delta_kernel<6><<<gb, CL_THREADS, 0, s>>>(P);
-    cl_apply_kernel<<<bits ? gw : gs, CL_THREADS, 0, s>>>(P);
-    if (int e = cuda_check("launch")) return e;
-  }
-  return CRITMC_OK;
+  P.proj = reinterpret_cast<float*>(base + (size_t)n_chains * P.n * 8);
+  P.newv = reinterpret_cast<int8_t*>(base + (size_t)n_chains * P.n * 12);
+  P.on_n = 0;
+  return cl_launch(P, n_chains, keys, (cudaStream_t)stream);
+}
+
+extern "C" int32_t critmc_on_cluster_update(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
+                                            int32_t n, int32_t n_chains, const uint32_t* keys, double beta,
+                                            int32_t algo, uint32_t sweep, int64_t* stats, void* scratch,
+                                            void* stream) {
+  clear_error();
+  static thread_local ClParams P;
+  int st = byte_geom(dim, lx, ly, lz, P.g);
+  if (st) return st;
+  if (!spins || !keys || !stats || !scratch) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (algo != CRITMC_WOLFF && algo != CRITMC_SWENDSEN_WANG) return fail(CRITMC_ERR_INVALID, "algo must be wolff or sw");
+  if (n != 2 && n != 3) return fail(CRITMC_ERR_UNSUPPORTED, "O(n) cluster updates for n = 2, 3");
+  if (n_chains < 1) return fail(CRITMC_ERR_INVALID, "need n_chains >= 1");
+  if (!(beta >= 0.0) || !std::isfinite(beta)) return fail(CRITMC_ERR_INVALID, "beta must be finite and >= 0");
+  P.n = 2 * P.g.slots;
+  if ((long long)P.n * n_chains >= (1LL << 31)) return fail(CRITMC_ERR_UNSUPPORTED, "too many sites");
+  P.spins = spins;
+  P.bits = 0;
+  P.potts = 0;
+  P.q = 2;
+  P.algo = algo;
+  P.sweep = sweep;
+  P.running = nullptr;
+  P.counts = nullptr;
+  P.stats = (long long*)stats;
+  P.thr = 0;
+  P.nb2 = (float)(-2.0 * beta);
+  char* base = static_cast<char*>(scratch);
+  P.label = reinterpret_cast<int*>(base);
+  P.size = reinterpret_cast<int*>(base + (size_t)n_chains * P.n * 4);
+  P.proj = reinterpret_cast<float*>(base + (size_t)n_chains * P.n * 8);
+  P.newv = reinterpret_cast<int8_t*>(base + (size_t)n_chains * P.n * 12);
+  P.on_n = n;
+  return cl_launch(P, n_chains, keys, (cudaStream_t)stream);
 }

@@ -633,7 +633,8 @@ extern "C" int32_t critmc_on_run(float* spins, int32_t dim, int32_t lx, int32_t 
     const int64_t code = schedule[2 * r], reps = schedule[2 * r + 1];
     if (code != CRITMC_METROPOLIS && code != CRITMC_HEATBATH && code != CRITMC_OVERRELAX)
       return fail(CRITMC_ERR_UNSUPPORTED, "O(n) kernels run metropolis, heatbath and overrelax rows");
-    if (reps < 1 || reps > (1 << 20)) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be in [1, 2^20]");
+    // a row of 0 repetitions is allowed: a schedule of only such rows measures
+    if (reps < 0 || reps > (1 << 20)) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be in [0, 2^20]");
     P.codes[r] = (int)code;
     P.reps[r] = (int)reps;
     per_meas += reps;
@@ -721,7 +722,7 @@ extern "C" int32_t critmc_on_run_grid(float* spins, int32_t dim, int32_t lx, int
     const int64_t code = schedule[2 * r], rp = schedule[2 * r + 1];
     if (code != CRITMC_METROPOLIS && code != CRITMC_HEATBATH && code != CRITMC_OVERRELAX)
       return fail(CRITMC_ERR_UNSUPPORTED, "O(n) kernels run metropolis, heatbath and overrelax rows");
-    if (rp < 1 || rp > (1 << 20)) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be in [1, 2^20]");
+    if (rp < 0 || rp > (1 << 20)) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be in [0, 2^20]");
     codes[r] = (int)code;
     reps[r] = (int)rp;
     per_meas += rp;

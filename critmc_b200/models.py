@@ -48,9 +48,6 @@ N_AUX = 4
 # moves of critmc that are not data-parallel sweeps and stay on its CPU path
 _NOT_ON_GPU = {
     "metropolis-random": "random-site Metropolis is a sequential walk, not a checkerboard sweep",
-    "wolff": "O(n) cluster updates (embedded-Ising reflections) are not on the GPU path",
-    "sw": "O(n) cluster updates (embedded-Ising reflections) are not on the GPU path",
-    "swendsen-wang": "O(n) cluster updates (embedded-Ising reflections) are not on the GPU path",
 }
 CLUSTER_CODES = (WOLFF, SWENDSEN_WANG)
 
@@ -386,7 +383,7 @@ class ON(Model):
     """Classical O(n) vector model with unit spins (critmc models.py:225-299)."""
 
     kind = "on"
-    updates = ("metropolis", "heatbath", "overrelax")
+    updates = ("metropolis", "heatbath", "overrelax", "wolff", "sw", "swendsen-wang")
 
     def __init__(self, lattice: Lattice, n: int):
         super().__init__(lattice)

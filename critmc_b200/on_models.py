@@ -18,6 +18,8 @@ from .layout import cb_pack, cb_unpack
 
 N_AUX = 4
 GRID_MIN_SITES = 4096
+OVERRELAX = 5
+CLUSTER_CODES = (3, 4)  # Wolff, Swendsen-Wang
 
 
 class ONChain:
@@ -47,9 +49,64 @@ class ONChain:
         return out.astype(np.float64)
 
     def advance(self, running, beta, schedule, n_meas):
+        sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+        if np.isin(sched[:, 0], CLUSTER_CODES).any():
+            return self._advance_with_clusters(running, beta, sched, n_meas)
+        return self._advance_sweeps(running, beta, sched, n_meas)
+
+    def _advance_with_clusters(self, running, beta, sched, n_meas):
+        """Schedules with Wolff / Swendsen-Wang rows (critmc kernels/on.py:349-418).
+
+        Per measurement the rows run in order: consecutive sweep rows as one
+        ``critmc_on_run`` call (which ends with a renormalisation and a
+        measurement), cluster rows as ``critmc_on_cluster_update`` calls (the
+        counter advances by one per update, as for sweeps); the measurement
+        of the last call is the measurement of the row set, a zero-repetition
+        call providing it after a trailing cluster row.  aux as critmc: accepted
+        moves, summed Wolff size, SW sum |C|^2 and cluster count.
+        """
+        dev = self.device
+        lx, ly, lz = self.dims
+        n_sites = int(np.prod(self.shape))
+        if getattr(self, "_cl_scratch", None) is None:
+            self._cl_scratch = empty_bytes(_lib.lib().critmc_cluster_scratch_bytes(1, n_sites), dev)
+        stats = torch.zeros((1, 3), dtype=torch.int64, device=dev)
+        segments: list[tuple[str, np.ndarray]] = []
+        pending: list[list[int]] = []
+        for code, reps in sched:
+            if code in CLUSTER_CODES:
+                if pending:
+                    segments.append(("sweeps", np.array(pending, dtype=np.int64)))
+                    pending = []
+                segments.append(("cluster", np.array([code, reps], dtype=np.int64)))
+            else:
+                pending.append([int(code), int(reps)])
+        segments.append(("sweeps", np.array(pending or [[OVERRELAX, 0]], dtype=np.int64)))
+        out = {k: [] for k in ("E", "M", "stiff_c", "stiff_s", "aux")}
+        for _ in range(n_meas):
+            stats.zero_()
+            accepted = 0
+            part = None
+            for kind, seg in segments:
+                if kind == "cluster":
+                    for _ in range(int(seg[1])):
+                        _lib.call("critmc_on_cluster_update", ptr(self.spins), len(self.shape), lx, ly, lz, self.n, 1,
+                                  self.key.ctypes.data, float(beta), int(seg[0]), self.sweep, ptr(stats),
+                                  ptr(self._cl_scratch), stream_handle(dev))
+                        self.sweep += 1
+                else:
+                    part = self._advance_sweeps(running, beta, seg, 1)
+                    accepted += int(part["aux"][0][0])
+            st = to_host(stats).ravel()
+            aux = np.array([accepted, st[0], st[1], st[2]], dtype=np.int64)
+            for k in ("E", "M", "stiff_c", "stiff_s"):
+                out[k].append(part[k][0])
+            out["aux"].append(aux)
+        return {k: np.array(v) for k, v in out.items()}
+
+    def _advance_sweeps(self, running, beta, sched, n_meas):
         dev = self.device
         n, dim = self.n, len(self.shape)
-        sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
         betas = np.array([beta], dtype=np.float64)
         steps = np.array([running.get("step", 1.0)], dtype=np.float64)
         e = torch.empty((1, n_meas), dtype=torch.float64, device=dev)

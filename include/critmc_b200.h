@@ -334,6 +334,19 @@ int32_t critmc_cluster_update(int32_t bits, void* spins, int32_t dim, int32_t lx
                               int32_t algo, uint32_t sweep, int64_t* running, int64_t* counts,
                               int64_t* stats, void* scratch, void* stream);
 
+/* One Wolff (algo 3) or Swendsen-Wang (4) update of n_chains O(n) chains
+ * (n = 2, 3) on the embedded Ising model of a random axis r: spins DEVICE
+ * float [n_chains][n][N] in the colour-major layout of critmc_on_run.  r from
+ * Philox(0, sweep, 0x0B, 0) (XY: angle 2 pi u0; n = 3: z = 2 u0 - 1, angle
+ * 2 pi u1), p_i = S_i . r, bond (as in critmc_cluster_update) active when
+ * p_i p_j > 0 and its 24-bit uniform < 1 - exp(-2 beta p_i p_j); flipped
+ * clusters are reflected, S <- S - 2 p r.  Spins are not renormalised (the
+ * next critmc_on_run measurement does it).  stats and scratch as above.
+ * Replaces critmc kernels/on.py:265-345 (wolff_update, sw_update).          */
+int32_t critmc_on_cluster_update(float* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t n,
+                                 int32_t n_chains, const uint32_t* keys, double beta, int32_t algo,
+                                 uint32_t sweep, int64_t* stats, void* scratch, void* stream);
+
 /* ---- streaming Gamma-method sums ---------------------------------------------
  * Append n values per chain (values: DEVICE [n_chains][ld], int64 or double)
  * to the per-chain state (DEVICE, critmc_stream_state_bytes(n_chains,

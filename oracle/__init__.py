@@ -67,6 +67,8 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_on_run.restype = _I
     L.oracle_cluster_update.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _I, _U32, _P, _P, _P, _P]
     L.oracle_cluster_update.restype = _I
+    L.oracle_on_cluster_update.argtypes = [_P, _I, _I, _I, _I, _I, _P, _D, _I, _U32, _P]
+    L.oracle_on_cluster_update.restype = _I
     L.oracle_fh_run.argtypes = [_I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _P, _D, _D, _I,
                                 ctypes.c_uint64, ctypes.c_int64, _I, _P, _P]
     L.oracle_fh_run.restype = _I
@@ -96,6 +98,24 @@ def cluster_update(lay: np.ndarray, shape, q: int, key, beta: float, algo: int, 
         raise MemoryError("oracle_cluster_update")
     lay[...] = flat.reshape(lay.shape)
     return de.value, dm.value, cd[:q] if q else None, st
+
+
+def on_cluster_update(comps: np.ndarray, shape, key, beta: float, algo: int, sweep: int,
+                      stats: np.ndarray | None = None) -> np.ndarray:
+    """One O(n) Wolff (3) / SW (4) update of float32 components [n][N] (colour-major, in place).
+
+    Returns the stats triple (Wolff size added; SW sum |C|^2, cluster count).
+    """
+    lx, ly, lz = _dims(shape)
+    if comps.dtype != np.float32 or not comps.flags["C_CONTIGUOUS"]:
+        raise TypeError("comps is updated in place: pass a C-contiguous float32 array")
+    k = np.ascontiguousarray(key, dtype=np.uint32).reshape(2)
+    st = np.zeros(3, dtype=np.int64) if stats is None else stats
+    rc = lib().oracle_on_cluster_update(_ptr(comps), len(shape), lx, ly, lz, comps.shape[0], _ptr(k), float(beta),
+                                        algo, sweep, _ptr(st))
+    if rc != 0:
+        raise MemoryError("oracle_on_cluster_update")
+    return st
 
 
 def fh_run(mode: int, s: np.ndarray, shape, q: int, key, idx: int, order: np.ndarray, lng: np.ndarray,

@@ -26,6 +26,8 @@ int oracle_on_run(float* s, int dim, int lx, int ly, int lz, int n, const uint32
 int oracle_cluster_update(int8_t* lay, int dim, int lx, int ly, int lz, int q, const uint32_t key[2],
                           double beta, int algo, uint32_t sweep, int64_t* d_energy, int64_t* d_mag,
                           int64_t* counts_delta, int64_t stats[3]);
+int oracle_on_cluster_update(float* s, int dim, int lx, int ly, int lz, int ncomp, const uint32_t key[2],
+                             double beta, int algo, uint32_t sweep, int64_t stats[3]);
 int oracle_fh_run(int mode, int8_t* s, int dim, int lx, int ly, int lz, int q, const uint32_t key[2],
                   int64_t* idx_io, int64_t* order, double* lng, int64_t* hist, int lo, int hi,
                   uint64_t* trials, double ln_f, double n_levels, int one_over_t, uint64_t t_base,

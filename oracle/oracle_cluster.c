@@ -18,6 +18,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "fpmath.h"
 #include "oracle.h"
 
 static int find_root(int* parent, int x) {
@@ -141,5 +142,108 @@ int oracle_cluster_update(int8_t* lay, int dim, int lx, int ly, int lz, int q, c
   free(parent);
   free(size);
   free(nv);
+  return 0;
+}
+
+/* 24-bit uniform in [0, 1) of a Philox word (the device's critmc_u01f) */
+static float u01f(uint32_t a) { return (float)(a >> 8) * (1.0f / 16777216.0f); }
+
+/*
+ * O(n) chains: restates critmc's embedded-Ising cluster updates
+ *   wolff_update, sw_update   src/critmc/kernels/on.py:265-345
+ * with the GPU's streams: axis r from Philox(0, sweep, 0x0B, 0) (XY: angle
+ * 2 pi u0; n = 3: z = 2 u0 - 1, angle 2 pi u1), p_i = S_i . r, bond active
+ * when p_i p_j > 0 and u01f(word) < 1 - exp(-2 beta p_i p_j), flipped clusters
+ * reflected, S <- S - 2 p r.  s: float [ncomp][N], colour-major.  Float
+ * arithmetic in the device's order with fpmath.h (built without contraction).
+ */
+int oracle_on_cluster_update(float* s, int dim, int lx, int ly, int lz, int ncomp, const uint32_t key[2],
+                             double beta, int algo, uint32_t sweep, int64_t stats[3]) {
+  if (dim < 2) ly = 1;
+  if (dim < 3) lz = 1;
+  const int hx = lx / 2, rows = ly * lz, slots = rows * hx, n = 2 * slots, z = 2 * dim;
+  const float nb2 = (float)(-2.0 * beta);
+  float r[3];
+  {
+    uint32_t w[4];
+    const uint32_t ctr[4] = {0u, sweep, 0x0Bu, 0u};
+    oracle_philox(ctr, key, w);
+    const float two_pi = 6.28318530717958647692f;
+    float sn, cs;
+    if (ncomp == 2) {
+      cm_sincosf(two_pi * u01f(w[0]), &sn, &cs);
+      r[0] = cs;
+      r[1] = sn;
+      r[2] = 0.0f;
+    } else {
+      const float zc = 2.0f * u01f(w[0]) - 1.0f;
+      const float rho = sqrtf(fmaxf(0.0f, 1.0f - zc * zc));
+      cm_sincosf(two_pi * u01f(w[1]), &sn, &cs);
+      r[0] = rho * cs;
+      r[1] = rho * sn;
+      r[2] = zc;
+    }
+  }
+  int* parent = (int*)malloc(sizeof(int) * n);
+  int* size = (int*)calloc((size_t)n, sizeof(int));
+  float* proj = (float*)malloc(sizeof(float) * n);
+  int8_t* flip = (int8_t*)calloc((size_t)n, 1);
+  if (!parent || !size || !proj || !flip) return -1;
+  for (int u = 0; u < n; ++u) {
+    parent[u] = u;
+    float p = s[u] * r[0] + s[n + u] * r[1];
+    if (ncomp == 3) p = p + s[2 * n + u] * r[2];
+    proj[u] = p;
+  }
+  int nb[6];
+  for (int q = 0; q < slots; ++q) {
+    nbrs0(dim, lx, ly, lz, q, nb);
+    uint32_t w[8];
+    uint32_t ctr[4] = {(uint32_t)q, sweep, 0x07u, 0u};
+    oracle_philox(ctr, key, w);
+    if (z == 6) {
+      ctr[2] = 0x07u | (1u << 8);
+      oracle_philox(ctr, key, w + 4);
+    }
+    for (int k = 0; k < z; ++k) {
+      const int u1 = slots + nb[k];
+      const float x = proj[q] * proj[u1];
+      if (x > 0.0f && u01f(w[k]) < 1.0f - cm_expf(nb2 * x)) join(parent, q, u1);
+    }
+  }
+  for (int u = 0; u < n; ++u) parent[u] = find_root(parent, u);
+  if (algo == 4) stats[1] = stats[2] = 0;
+  if (algo == 3) {
+    uint32_t w[4];
+    const uint32_t ctr[4] = {0u, sweep, 0x09u, 0u};
+    oracle_philox(ctr, key, w);
+    const int seed = (int)(((uint64_t)w[0] * (uint64_t)n) >> 32);
+    for (int u = 0; u < n; ++u)
+      if (parent[u] == parent[seed]) {
+        flip[u] = 1;
+        ++stats[0];
+      }
+  } else {
+    for (int u = 0; u < n; ++u) ++size[parent[u]];
+    for (int u = 0; u < n; ++u) {
+      if (parent[u] == u) {
+        stats[1] += (int64_t)size[u] * size[u];
+        ++stats[2];
+      }
+      uint32_t w[4];
+      const uint32_t ctr[4] = {(uint32_t)parent[u], sweep, 0x08u, 0u};
+      oracle_philox(ctr, key, w);
+      flip[u] = (int8_t)(w[0] >> 31);
+    }
+  }
+  for (int u = 0; u < n; ++u) {
+    if (!flip[u]) continue;
+    const float tp = 2.0f * proj[u];
+    for (int c = 0; c < ncomp; ++c) s[c * n + u] = s[c * n + u] - tp * r[c];
+  }
+  free(parent);
+  free(size);
+  free(proj);
+  free(flip);
   return 0;
 }

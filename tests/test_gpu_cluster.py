@@ -1,6 +1,7 @@
 """Cluster updates (Swendsen-Wang, Wolff): bit-exact against the CPU replay on
-both layouts, and critmc's exact results through Simulation schedules
-(critmc tests/test_kernels.py:27-92 patterns with cluster moves)."""
+both Ising layouts, Potts and the O(n) models, and critmc's exact results
+through Simulation schedules (critmc tests/test_kernels.py:27-109 patterns with
+cluster moves)."""
 
 from __future__ import annotations
 
@@ -13,7 +14,7 @@ from conftest import assert_consistent
 from exact_helpers import JointDOS
 
 import oracle
-from critmc_b200 import Ising, Potts, Simulation, chain, hypercubic, square
+from critmc_b200 import ON, Ising, Potts, Simulation, chain, hypercubic, square
 from critmc_b200 import _lib
 from critmc_b200.device import empty_bytes, ptr, stream_handle
 from critmc_b200.layout import cb_pack, cb_unpack
@@ -120,3 +121,91 @@ def test_auto_wolff_count_is_tuned(cuda):
     info = sim.thermalize(200)
     assert info["wolff_per_meas"] >= 1 and info["mean_cluster"] > 1
     assert "wolff_history" in info
+
+
+ON_CASES = [
+    ((16, 8), 2, 0.9),
+    ((64, 32), 2, 1.1),
+    ((16,), 2, 1.1),
+    ((8, 8, 4), 3, 0.7),
+    ((6, 4), 3, 1.5),
+]
+
+
+@pytest.mark.parametrize("algo", [WOLFF, SW])
+@pytest.mark.parametrize("shape,n,beta", ON_CASES)
+def test_on_cluster_update_bit_identical_to_replay(cuda, shape, n, beta, algo):
+    """Embedded-Ising reflections (critmc kernels/on.py:265-345) against the CPU replay."""
+    lat = hypercubic(shape)
+    model = ON(lat, n)
+    rng = np.random.default_rng(sum(shape) + 10 * n + algo)
+    s0 = model.initial_state("random", rng)
+    ch = model.to_device(s0, rng, cuda)
+    dims = tuple(shape) + (1,) * (3 - len(shape))
+    comps = np.ascontiguousarray(np.stack([cb_pack(s0[:, k].astype(np.float32), shape) for k in range(n)]))
+    comps = comps.reshape(n, -1)
+    stats = torch.zeros((1, 3), dtype=torch.int64, device=cuda)
+    scratch = empty_bytes(_lib.lib().critmc_cluster_scratch_bytes(1, lat.n_sites), cuda)
+    ref_stats = np.zeros(3, dtype=np.int64)
+    for sweep in range(6):
+        _lib.call("critmc_on_cluster_update", ptr(ch.spins), len(shape), *dims, n, 1, ch.key.ctypes.data, beta, algo,
+                  sweep, ptr(stats), ptr(scratch), stream_handle(cuda))
+        oracle.on_cluster_update(comps, shape, ch.key, beta, algo, sweep, ref_stats)
+        got = ch.spins.cpu().numpy().reshape(n, -1)
+        assert np.array_equal(got.view(np.uint32), comps.view(np.uint32))
+        np.testing.assert_array_equal(stats.cpu().numpy().ravel(), ref_stats)
+    # reflections keep unit length up to rounding
+    assert np.allclose(np.linalg.norm(ch.fetch(), axis=1), 1.0, atol=1e-5)
+    if algo == WOLFF:
+        assert ref_stats[0] > 0
+
+
+def test_on_mixed_cluster_schedule_matches_replay(cuda):
+    """heatbath + overrelax + wolff + sw per measurement: E, M and spins bit for bit."""
+    shape, n, beta = (16, 16), 2, 1.0
+    model = ON(hypercubic(shape), n)
+    rng = np.random.default_rng(77)
+    s0 = model.initial_state("random", rng)
+    ch = model.to_device(s0, rng, cuda)
+    key = ch.key.copy()
+    sched = np.array([[2, 1], [5, 2], [3, 3], [4, 1]])
+    running = model.begin(s0)
+    out = model.advance(ch, running, beta, sched, 5)
+    # replay: sweep rows through oracle.on_run (ending in a measurement), cluster rows through the oracle
+    s = s0.astype(np.float32)
+    sweep = 0
+    ref_e, ref_aux = [], []
+    for _ in range(5):
+        _, _, _, _, aux1 = oracle.on_run(s, shape, n, key, beta, 1.0, sched[:2], 1, sweep0=sweep)
+        sweep += 3
+        comps = np.ascontiguousarray(np.stack([cb_pack(s[:, k], shape) for k in range(n)])).reshape(n, -1)
+        st = np.zeros(3, dtype=np.int64)
+        for code, reps in sched[2:]:
+            for _ in range(reps):
+                oracle.on_cluster_update(comps, shape, key, beta, int(code), sweep, st)
+                sweep += 1
+        s = np.ascontiguousarray(np.stack([cb_unpack(comps[k], shape) for k in range(n)], axis=1))
+        e, _, _, _, aux2 = oracle.on_run(s, shape, n, key, beta, 1.0, [[5, 0]], 1, sweep0=sweep)
+        ref_e.append(e[0])
+        ref_aux.append([aux1[0][0] + aux2[0][0], st[0], st[1], st[2]])
+    np.testing.assert_array_equal(out["E"], ref_e)
+    np.testing.assert_array_equal(out["aux"], np.array(ref_aux))
+    assert np.array_equal(ch.fetch().astype(np.float32), s)
+
+
+@pytest.mark.parametrize("n_comp", [2, 3])
+@pytest.mark.parametrize("updates", ["3*wolff", "heatbath+sw"])
+def test_on_cluster_ring_matches_transfer_operator(cuda, n_comp, updates):
+    """critmc tests/test_kernels.py:95-109 with cluster moves."""
+    from exact_helpers import golden
+
+    ref = golden()["on_ring"][f"n{n_comp}_N8_b1.1"]
+    beta, n_sites = 1.1, 8
+    sim = Simulation(ON(chain(n_sites), n_comp), beta, updates, seed=6)
+    sim.thermalize(1000)
+    ts = sim.run(30_000)
+    assert_consistent(ts["e"], ref["energy"])
+    e = ts["E"]
+    assert beta ** 2 * e.var() / n_sites == pytest.approx(ref["specific_heat"], rel=0.1)
+    s = sim.state
+    assert np.allclose(np.linalg.norm(s, axis=1), 1.0, atol=1e-6)

@@ -88,6 +88,32 @@ def test_oracle_on_ring_matches_transfer_operator(n, sched):
     assert c_mc == pytest.approx(ref["specific_heat"], rel=0.06)
 
 
+@pytest.mark.parametrize("n", [2, 3])
+@pytest.mark.parametrize("algo,reps", [(3, 3), (4, 1)], ids=["3*wolff", "sw"])
+def test_oracle_on_cluster_ring_matches_transfer_operator(n, algo, reps):
+    """Embedded-Ising cluster updates alone (critmc kernels/on.py:265-345) on the
+    8-site O(n) ring against chains.on_ring_*; spins renormalised per measurement."""
+    from critmc_b200.layout import cb_pack, cb_unpack
+
+    ref = golden()["on_ring"][f"n{n}_N8_b1.1"]
+    rng = np.random.default_rng(10 + n)
+    s = rng.standard_normal((8, n))
+    s /= np.linalg.norm(s, axis=1, keepdims=True)
+    comps = np.ascontiguousarray(np.stack([cb_pack(s[:, k], (8,)) for k in range(n)]).astype(np.float32))
+    comps = comps.reshape(n, -1)
+    n_meas, sweep, e = 40_000, 0, []
+    for _ in range(n_meas):
+        for _ in range(reps):
+            oracle.on_cluster_update(comps, (8,), (n, 17), 1.1, algo, sweep)
+            sweep += 1
+        comps /= np.sqrt((comps.astype(np.float64) ** 2).sum(axis=0)).astype(np.float32)
+        v = np.stack([cb_unpack(comps[k], (8,)) for k in range(n)], axis=1).astype(np.float64)
+        e.append(-np.sum(v * np.roll(v, -1, axis=0)))
+    e = np.array(e[1000:])
+    assert_consistent(e / 8.0, ref["energy"])
+    assert 1.1 ** 2 * e.var() / 8 == pytest.approx(ref["specific_heat"], rel=0.08)
+
+
 def test_ea_enumeration_helper_matches_critmc():
     """The test-side EA enumeration reproduces critmc's ea_energies fixture."""
     from critmc_b200 import square

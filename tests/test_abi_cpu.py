@@ -65,6 +65,33 @@ def test_invalid_arguments_fail_before_any_launch():
     assert st == -3
 
 
+def test_flat_histogram_and_on_cluster_arguments_fail_before_any_launch():
+    L = _lib.lib()
+    d = ctypes.c_void_p(16)  # never dereferenced: validation fails first
+    keys = np.zeros(2, np.uint32)
+    # mode 2 does not exist
+    st = L.critmc_fh_run(2, d, 2, 4, 4, 1, 0, 1, d, 9, d, d, d, d, d, d, d, d, d, d, 10, 1, None, None, None)
+    assert st == -1 and "mode" in _lib.last_error()
+    # Potts q out of range, and more than 2^24 sites per walker
+    st = L.critmc_fh_run(0, d, 2, 4, 4, 1, 200, 1, d, 9, d, d, d, d, d, d, d, d, d, d, 10, 1, None, None, None)
+    assert st == -1
+    st = L.critmc_fh_run(0, d, 2, 8192, 4096, 1, 0, 1, d, 9, d, d, d, d, d, d, d, d, d, d, 10, 1, None, None, None)
+    assert st == -1 and "2^24" in _lib.last_error()
+    # Wang-Landau without its per-walker ln f arrays; multicanonical without outputs
+    st = L.critmc_fh_run(0, d, 2, 4, 4, 1, 0, 1, d, 9, d, d, d, d, d, d, None, d, d, d, 10, 1, None, None, None)
+    assert st == -1 and "ln_f" in _lib.last_error()
+    st = L.critmc_fh_run(1, d, 2, 4, 4, 1, 0, 1, d, 9, d, d, d, d, d, d, None, None, None, None, 10, 3, None,
+                         None, None)
+    assert st == -1 and "idx_out" in _lib.last_error()
+    # O(n) cluster moves: n = 4, an unknown algorithm, a negative beta
+    st = L.critmc_on_cluster_update(d, 2, 4, 4, 1, 4, 1, keys.ctypes.data, 1.0, 3, 0, d, d, None)
+    assert st == -3
+    st = L.critmc_on_cluster_update(d, 2, 4, 4, 1, 2, 1, keys.ctypes.data, 1.0, 0, 0, d, d, None)
+    assert st == -1 and "wolff" in _lib.last_error()
+    st = L.critmc_on_cluster_update(d, 2, 4, 4, 1, 2, 1, keys.ctypes.data, -1.0, 4, 0, d, d, None)
+    assert st == -1 and "beta" in _lib.last_error()
+
+
 @pytest.mark.parametrize("beta", [0.0, 0.44, 3.0])
 def test_potts_tables_are_monotone(beta):
     b = np.zeros(8, np.uint64)

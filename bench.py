@@ -174,10 +174,59 @@ def on_bench(dev, steps: int = 40, peak: float = 6650.0) -> dict:
     return out
 
 
+def cluster_bench(dev, updates: int = 20) -> dict:
+    """Cluster updates, ``updates`` timed per case after two warm-up updates:
+    Swendsen-Wang and Wolff on one 2D Ising chain of 1024 x 1024 (bit layout) at
+    beta_c, q = 3 Potts 512 x 512 at 1.0 and XY 512 x 512 at beta 1.1; rate in
+    sites per ns (one cluster update visits every site)."""
+    import torch
+
+    from critmc_b200 import ON, Ising, Potts, _lib, square
+    from critmc_b200.device import empty_bytes, ptr, stream_handle
+
+    out = {}
+    cases = (("ising_L1024", Ising(square(1024)), 0.4406868), ("potts3_L512", Potts(square(512), 3), 1.0),
+             ("xy_L512", ON(square(512), 2), 1.1))
+    for name, model, beta in cases:
+        rng = np.random.default_rng(1)
+        s0 = model.initial_state("random", rng)
+        ch = model.to_device(s0, rng, dev)
+        shape = tuple(model.lattice.shape)
+        dims = shape + (1,) * (3 - len(shape))
+        scratch = empty_bytes(_lib.lib().critmc_cluster_scratch_bytes(1, model.n_sites), dev)
+        stats = torch.zeros((1, 3), dtype=torch.int64, device=dev)
+        for algo, aname in ((4, "sw"), (3, "wolff")):
+            def one(sweep):
+                if isinstance(model, ON):
+                    _lib.call("critmc_on_cluster_update", ptr(ch.spins), 2, *dims, 2, 1, ch.key.ctypes.data, beta,
+                              algo, sweep, ptr(stats), ptr(scratch), stream_handle(dev))
+                else:
+                    bits = isinstance(model, Ising)
+                    q = 0 if bits else model.q
+                    run = torch.zeros((1, 2), dtype=torch.int64, device=dev)
+                    cnt = None if bits else torch.zeros(q, dtype=torch.int64, device=dev)
+                    _lib.call("critmc_cluster_update", int(bits), ptr(ch.words if bits else ch.spins), 2, *dims, q,
+                              1, ch.key.ctypes.data, beta, algo, sweep, ptr(run), ptr(cnt), ptr(stats),
+                              ptr(scratch), stream_handle(dev))
+            one(0)
+            one(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            for k in range(updates):
+                one(2 + k)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / updates
+            out[f"{name}_{aname}"] = {"ms_per_update": ms, "sites_per_ns": model.n_sites / (ms * 1e6)}
+    return out
+
+
 def fh_bench(dev) -> dict:
     """Wang-Landau moves on the q = 10 Potts 8 x 8 torus, energy window [-1.95, -0.6]
     per site (critmc's flat-histogram double-peak case): 4736 walkers (32 per SM)
-    x 200,000 moves in one launch, and one walker x 1,000,000 moves, each with
+    and 14208 walkers (96 per SM, three shared-memory blocks) x 200,000 moves in
+    one launch, and one walker x 1,000,000 moves, each with
     constant ln f and in 1/t mode; the C oracle runs one walker on one host core
     (2,000,000 moves) for comparison."""
     import torch
@@ -188,7 +237,7 @@ def fh_bench(dev) -> dict:
 
     model = Potts(square(8), 10)
     out = {}
-    for nw, moves in ((4736, 200_000), (1, 1_000_000)):
+    for nw, moves in ((4736, 200_000), (14208, 200_000), (1, 1_000_000)):
         for one_t in (0, 1):
             wl = WangLandau(model, e_window=(-1.95, -0.6), seed=5, n_walkers=nw, device=dev)
             W = wl.walkers
@@ -218,7 +267,7 @@ def fh_bench(dev) -> dict:
                   2_000_000)
     cpu = 2_000_000 / (time.perf_counter() - t0) / 1e9
     out["cpu_oracle_one_walker_one_core_moves_per_ns"] = cpu
-    out["batch_over_cpu_core"] = out["walkers4736_const_moves_per_ns"] / cpu
+    out["batch_over_cpu_core"] = out["walkers14208_const_moves_per_ns"] / cpu
     return out
 
 
@@ -549,6 +598,7 @@ def main() -> None:
         extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
         extras["on_batched"] = on_bench(dev, peak=peaks()[0])
         extras["flat_histogram"] = fh_bench(dev)
+        extras["cluster_updates"] = cluster_bench(dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -71,6 +71,7 @@ SIGNATURES: dict[str, tuple] = {
     "critmc_stream_state_bytes": (_I64, [_I32, _I32]),
     "critmc_fh_run": (_I32, [_I32, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P, _P, _P, _P, _P, _P, _P,
                              _P, _P, _P, _I64, _I32, _P, _P, _P]),
+    "critmc_fh_descend": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P, _P, _P, _I64, _P, _P]),
     "critmc_stream_update": (_I32, [_P, _I32, _I32, _I32, _I64, _P, _I32, _P]),
     "critmc_cluster_update": (
         _I32, [_I32, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _D, _I32, _U32, _P, _P, _P, _P, _P]),

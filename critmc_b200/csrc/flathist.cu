@@ -295,6 +295,75 @@ __global__ void __launch_bounds__(FH_STAGED_WALKERS) fh_kernel_staged(const __gr
   }
 }
 
+// Greedy descent into the window (critmc flathist.py:96-130, on the device):
+// step j draws Philox(j mod 2^32, j / 2^32, 0x0C, 0) with the walker's key
+// (word 0 the site, word 1 the Potts proposal, as for the walk) and keeps a
+// move when the level does not move away from the window.  steps_out gets the
+// number of steps taken, or -1 if the window was not reached in max_steps.
+constexpr uint32_t TAG_DESCEND = 0x0Cu;
+
+template <int POTTS, int DIM>
+__global__ void __launch_bounds__(FH_THREADS) fh_descend_kernel(const __grid_constant__ FhWalk P,
+                                                                long long* steps_out) {
+  constexpr int Z = 2 * DIM;
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.n_walkers) return;
+  const int n = P.lx * P.ly * P.lz;
+  int8_t* s = P.spins + (size_t)w * n;
+  const int lo = P.window[2 * w], hi = P.window[2 * w + 1];
+  const uint32_t k0 = P.keys[2 * w], k1 = P.keys[2 * w + 1];
+  long long idx = P.idx[w];
+  long long m = POTTS ? 0 : P.order[w];
+  long long* counts = POTTS ? P.order + (size_t)w * P.q : nullptr;
+  long long used = -1;
+  for (long long j = 0; j <= P.moves; ++j) {
+    if (lo <= idx && idx <= hi) {
+      used = j;
+      break;
+    }
+    if (j == P.moves) break;
+    const critmc_u32x4 r = critmc_philox4x32((uint32_t)j, (uint32_t)(j >> 32), TAG_DESCEND, 0u, k0, k1);
+    const int i = (int)(((unsigned long long)r.v[0] * (unsigned)n) >> 32);
+    int nb[Z];
+    fh_neighbours<DIM>(P, i, nb);
+    const int old = s[i];
+    int nv, d;
+    if (POTTS) {
+      int ns = (int)(((unsigned long long)r.v[1] * (unsigned)(P.q - 1)) >> 32);
+      ns += ns >= old;
+      nv = ns;
+      int n_old = 0, n_new = 0;
+      for (int k = 0; k < Z; ++k) {
+        const int v = s[nb[k]];
+        n_old += v == old;
+        n_new += v == ns;
+      }
+      d = n_old - n_new;
+    } else {
+      int field = 0;
+      for (int k = 0; k < Z; ++k) field += s[nb[k]];
+      nv = -old;
+      d = (old * field) / 2;
+    }
+    const long long nidx = idx + d;
+    if ((idx < lo && nidx >= idx) || (idx > hi && nidx <= idx)) {
+      s[i] = (int8_t)nv;
+      if (POTTS) {
+        if ((unsigned)old < (unsigned)P.q) {
+          --counts[old];
+          ++counts[nv];
+        }
+      } else {
+        m += nv - old;
+      }
+      idx = nidx;
+    }
+  }
+  P.idx[w] = idx;
+  if (!POTTS) P.order[w] = m;
+  steps_out[w] = used;
+}
+
 template <int MODE, int POTTS, int DIM>
 static int fh_launch(const FhWalk& P, bool staged, int wpb, cudaStream_t s) {
   if (!staged) {
@@ -398,4 +467,47 @@ extern "C" int32_t critmc_fh_run(int32_t mode, int8_t* spins, int32_t dim, int32
   cudaStream_t s = (cudaStream_t)stream;
   if (mode == 0) return q == 0 ? fh_launch_dim<0, 0>(P, staged, wpb, s) : fh_launch_dim<0, 1>(P, staged, wpb, s);
   return q == 0 ? fh_launch_dim<1, 0>(P, staged, wpb, s) : fh_launch_dim<1, 1>(P, staged, wpb, s);
+}
+
+extern "C" int32_t critmc_fh_descend(int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t q,
+                                     int32_t n_walkers, const uint32_t* keys, int32_t levels, int64_t* idx,
+                                     int64_t* order, const int32_t* window, int64_t max_steps, int64_t* steps_out,
+                                     void* stream) {
+  clear_error();
+  if (dim < 2) ly = 1;
+  if (dim < 3) lz = 1;
+  int st = fh_check(dim, lx, ly, lz, q, n_walkers, levels);
+  if (st) return st;
+  if (!spins || !keys || !idx || !order || !window || !steps_out) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (max_steps < 0) return fail(CRITMC_ERR_INVALID, "max_steps must not be negative");
+  FhWalk P;
+  std::memset(&P, 0, sizeof(P));
+  P.spins = spins;
+  P.idx = (long long*)idx;
+  P.order = (long long*)order;
+  P.window = window;
+  P.keys = keys;
+  P.n_walkers = n_walkers;
+  P.lx = lx;
+  P.ly = ly;
+  P.lz = lz;
+  P.dim = dim;
+  P.q = q;
+  P.levels = levels;
+  P.moves = max_steps;
+  P.div_x = fh_div_for((long long)lx * ly * lz, lx);
+  P.div_y = fh_div_for((long long)lx * ly * lz, ly);
+  const int blocks = (n_walkers + FH_THREADS - 1) / FH_THREADS;
+  cudaStream_t s = (cudaStream_t)stream;
+  long long* so = (long long*)steps_out;
+  if (q == 0) {
+    if (dim == 1) fh_descend_kernel<0, 1><<<blocks, FH_THREADS, 0, s>>>(P, so);
+    else if (dim == 2) fh_descend_kernel<0, 2><<<blocks, FH_THREADS, 0, s>>>(P, so);
+    else fh_descend_kernel<0, 3><<<blocks, FH_THREADS, 0, s>>>(P, so);
+  } else {
+    if (dim == 1) fh_descend_kernel<1, 1><<<blocks, FH_THREADS, 0, s>>>(P, so);
+    else if (dim == 2) fh_descend_kernel<1, 2><<<blocks, FH_THREADS, 0, s>>>(P, so);
+    else fh_descend_kernel<1, 3><<<blocks, FH_THREADS, 0, s>>>(P, so);
+  }
+  return cuda_check("launch");
 }

@@ -385,6 +385,18 @@ int32_t critmc_fh_run(int32_t mode, int8_t* spins, int32_t dim, int32_t lx, int3
                       const double* n_levels, const int32_t* one_over_t, const uint64_t* t_base, int64_t moves,
                       int32_t n_meas, int64_t* idx_out, int64_t* order_out, void* stream);
 
+/* Greedy descent of each walker into its window before a flat-histogram run:
+ * step j draws Philox(j mod 2^32, j / 2^32, 0x0C, 0) with the walker's key
+ * (site and Potts proposal as in critmc_fh_run) and keeps the move when the
+ * level does not move away from [window[0], window[1]].  spins, idx (the
+ * starting level of each configuration), order (Ising M; Potts counts [q])
+ * are updated; steps_out [w] gets the steps taken, -1 when max_steps did not
+ * reach the window.  All arrays are DEVICE arrays as for critmc_fh_run.
+ * Replaces critmc flathist.py:96-130 (_walk_into_window).                    */
+int32_t critmc_fh_descend(int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t q,
+                          int32_t n_walkers, const uint32_t* keys, int32_t levels, int64_t* idx, int64_t* order,
+                          const int32_t* window, int64_t max_steps, int64_t* steps_out, void* stream);
+
 /* ---- chains owned by the library (handles) ----------------------------------
  * The library allocates and keeps a chain's lattice, running sums, Philox key
  * and sweep counter; the caller passes states in critmc's site order (first

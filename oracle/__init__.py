@@ -72,6 +72,8 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_fh_run.argtypes = [_I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _P, _D, _D, _I,
                                 ctypes.c_uint64, ctypes.c_int64, _I, _P, _P]
     L.oracle_fh_run.restype = _I
+    L.oracle_fh_descend.argtypes = [_P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _I, ctypes.c_int64]
+    L.oracle_fh_descend.restype = ctypes.c_int64
     L.oracle_ea_pt_run.argtypes = [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _P, _P, _U32, _I, _I, _I,
                                    _P, _P, _P, _P, _P]
     L.oracle_ea_pt_run.restype = _I
@@ -116,6 +118,18 @@ def on_cluster_update(comps: np.ndarray, shape, key, beta: float, algo: int, swe
     if rc != 0:
         raise MemoryError("oracle_on_cluster_update")
     return st
+
+
+def fh_descend(s: np.ndarray, shape, q: int, key, idx: int, order: np.ndarray, window, max_steps: int):
+    """Greedy descent of one walker into its window (arrays in place); returns (idx, steps or -1)."""
+    lx, ly, lz = _dims(shape)
+    if s.dtype != np.int8 or order.dtype != np.int64 or not (s.flags["C_CONTIGUOUS"] and order.flags["C_CONTIGUOUS"]):
+        raise TypeError("s (int8) and order (int64) are updated in place")
+    k = np.ascontiguousarray(key, dtype=np.uint32).reshape(2)
+    i = ctypes.c_int64(idx)
+    steps = lib().oracle_fh_descend(_ptr(s), len(shape), lx, ly, lz, q, _ptr(k), ctypes.byref(i), _ptr(order),
+                                    int(window[0]), int(window[1]), int(max_steps))
+    return i.value, int(steps)
 
 
 def fh_run(mode: int, s: np.ndarray, shape, q: int, key, idx: int, order: np.ndarray, lng: np.ndarray,

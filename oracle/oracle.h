@@ -32,6 +32,8 @@ int oracle_fh_run(int mode, int8_t* s, int dim, int lx, int ly, int lz, int q, c
                   int64_t* idx_io, int64_t* order, double* lng, int64_t* hist, int lo, int hi,
                   uint64_t* trials, double ln_f, double n_levels, int one_over_t, uint64_t t_base,
                   int64_t moves, int n_meas, int64_t* idx_out, int64_t* order_out);
+int64_t oracle_fh_descend(int8_t* s, int dim, int lx, int ly, int lz, int q, const uint32_t key[2], int64_t* idx_io,
+                          int64_t* order, int lo, int hi, int64_t max_steps);
 int oracle_ea_pt_run(int8_t* spins, const double* J, int dim, int lx, int ly, int lz, int m,
                      const uint32_t* keys, const double* betas, const uint32_t* swap_thr, int width,
                      int* perm, int* labels, uint32_t t0, int n_steps, int n_bins,

@@ -109,3 +109,41 @@ int oracle_fh_run(int mode, int8_t* s, int dim, int lx, int ly, int lz, int q, c
   if (q == 0) order[0] = m;
   return 0;
 }
+
+/* Greedy descent into [lo, hi] (critmc flathist.py:96-130 _walk_into_window)
+ * with the GPU's stream: step j draws Philox(j mod 2^32, j / 2^32, 0x0C, 0);
+ * a move is kept when the level does not move away from the window.  Returns
+ * the steps taken, or -1 if max_steps did not reach the window. */
+int64_t oracle_fh_descend(int8_t* s, int dim, int lx, int ly, int lz, int q, const uint32_t key[2], int64_t* idx_io,
+                          int64_t* order, int lo, int hi, int64_t max_steps) {
+  if (dim < 2) ly = 1;
+  if (dim < 3) lz = 1;
+  const int n = lx * ly * lz;
+  int64_t idx = *idx_io;
+  for (int64_t j = 0; j <= max_steps; ++j) {
+    if (lo <= idx && idx <= hi) {
+      *idx_io = idx;
+      return j;
+    }
+    if (j == max_steps) break;
+    uint32_t w[4];
+    const uint32_t ctr[4] = {(uint32_t)j, (uint32_t)(j >> 32), 0x0Cu, 0u};
+    oracle_philox(ctr, key, w);
+    const int i = (int)(((uint64_t)w[0] * (uint64_t)n) >> 32);
+    int nv;
+    const int64_t nidx = idx + delta(s, dim, lx, ly, lz, q, i, w[1], &nv);
+    if ((idx < lo && nidx >= idx) || (idx > hi && nidx <= idx)) {
+      const int old = s[i];
+      s[i] = (int8_t)nv;
+      if (q == 0) {
+        order[0] += nv - old;
+      } else {
+        --order[old];
+        ++order[nv];
+      }
+      idx = nidx;
+    }
+  }
+  *idx_io = idx;
+  return -1;
+}

@@ -121,3 +121,31 @@ def test_oracle_multicanonical_potts_order_series_and_m2():
     got = out.canonical(beta)
     assert got["m2"][0] == pytest.approx(exact_m2, abs=0.02)
     assert got["u"][0] == pytest.approx(jd.average(beta, lambda e, o: e) / n, abs=0.02)
+
+
+@pytest.mark.parametrize("kind,shape,q,win", [("ising", (8, 8), 0, (-1.9, -1.6)), ("potts", (6, 6), 4, (-1.5, -1.2)),
+                                              ("ising", (4, 4, 4), 0, (-2.0, -1.5))])
+def test_oracle_descent_is_consistent_and_reaches_the_window_from_order(kind, shape, q, win):
+    """The oracle's greedy descent (critmc flathist.py:96-130 rule): the final
+    level is always the configuration's, with matching M / counts; from a random
+    start it may stall above the window (a straight domain wall), from the
+    ordered configuration it walks up into the window."""
+    from flathist_replay import initial_order
+
+    import oracle
+    from critmc_b200 import hypercubic
+
+    model = Ising(hypercubic(shape)) if kind == "ising" else Potts(hypercubic(shape), q)
+    lv = EnergyLevels.of(model)
+    lo, hi = lv.window(*win)
+    rng = np.random.default_rng(9)
+    for start in ["random"] * 5 + ["ordered"] * 2:
+        s = model.initial_state(start, rng).astype(np.int8)
+        order = initial_order(s, q)
+        key = rng.integers(0, 1 << 32, size=2, dtype=np.uint64).astype(np.uint32)
+        idx, steps = oracle.fh_descend(s, shape, q, key, lv.index(model.energy(s)), order, (lo, hi), 10**6)
+        assert idx == lv.index(model.energy(s))
+        np.testing.assert_array_equal(order, initial_order(s, q))
+        assert (steps >= 0) == (lo <= idx <= hi)
+        if start == "ordered":
+            assert steps >= 0

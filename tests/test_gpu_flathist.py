@@ -130,6 +130,45 @@ def test_shared_and_global_paths_agree_over_many_blocks(cuda, kind, shape, q):
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("kind,shape,q,win", [
+    ("ising", (8, 8), 0, (-1.9, -1.6)), ("ising", (4, 4, 4), 0, (-2.0, -1.5)), ("ising", (16,), 0, (-0.9, -0.5)),
+    ("potts", (8, 8), 10, (-1.95, -0.6)), ("potts", (6, 5), 4, (-1.5, -1.2)), ("potts", (4, 4, 2), 3, (-2.5, -1.5))])
+def test_descent_into_window_bit_identical_to_oracle(cuda, kind, shape, q, win):
+    """critmc_fh_descend against the oracle for 40 walkers, and the walkers it sets up."""
+    model = _model(kind, shape, q)
+    lv = EnergyLevels.of(model)
+    lo, hi = lv.window(*win)
+    rng = np.random.default_rng(zlib.crc32(repr((kind, shape)).encode()))
+    W = 40
+    states = [model.initial_state("random", rng).astype(np.int8) for _ in range(W)]
+    keys = rng.integers(0, 1 << 32, size=(W, 2), dtype=np.uint64).astype(np.uint32)
+    idx0 = [lv.index(model.energy(st)) for st in states]
+    orders = [initial_order(st, q) for st in states]
+    spins = torch.from_numpy(np.stack(states)).to(cuda)
+    idx = torch.tensor(idx0, dtype=torch.int64, device=cuda)
+    order = torch.from_numpy(np.concatenate(orders)).to(cuda)
+    window = torch.tensor([[lo, hi]] * W, dtype=torch.int32, device=cuda)
+    steps = torch.empty(W, dtype=torch.int64, device=cuda)
+    dkeys = torch.from_numpy(keys.view(np.int32)).to(cuda)
+    lx, ly, lz = tuple(shape) + (1,) * (3 - len(shape))
+    _lib.call("critmc_fh_descend", ptr(spins), len(shape), lx, ly, lz, q, W, ptr(dkeys), lv.size, ptr(idx),
+              ptr(order), ptr(window), 10**6, ptr(steps), stream_handle(cuda))
+    got_s, got_i, got_o, got_n = (t.cpu().numpy() for t in (spins, idx, order, steps))
+    got_o = got_o.reshape(W, -1)
+    for w in range(W):
+        i_ref, n_ref = oracle.fh_descend(states[w], shape, q, keys[w], idx0[w], orders[w], (lo, hi), 10**6)
+        np.testing.assert_array_equal(got_s[w], states[w])
+        assert got_i[w] == i_ref and got_n[w] == n_ref
+        np.testing.assert_array_equal(got_o[w], orders[w])
+    # the drivers start every walker inside its window (random start, else the
+    # ordered one), at its configuration's level
+    wl = WangLandau(model, e_window=win, seed=3, n_walkers=64)
+    s_all = wl.walkers.spins.cpu().numpy()
+    i_all = wl.walkers.idx.cpu().numpy()
+    for w in range(0, 64, 7):
+        assert lo <= i_all[w] <= hi and i_all[w] == lv.index(model.energy(s_all[w]))
+
+
 def _start(walkers, w):
     return (walkers.spins[w].cpu().numpy().copy(), int(walkers.idx[w]), walkers.keys[w].cpu().numpy().view(np.uint32))
 
@@ -237,6 +276,15 @@ def test_multicanonical_reweighting_to_canonical(cuda):
         assert out.canonical(b)["u"][0] == pytest.approx(kaufman_energy(b, 6), abs=0.01)
 
 
+# Equal-height point of the q = 10 Potts 8 x 8 torus in the window [-1.95, -0.6]
+# (split -1.3): 1.3788, from oracle Wang-Landau runs converged to ln f = 1e-6
+# for four seeds (spread 0.0006).  It lies 0.047 below beta_c, so critmc's own
+# bracket beta_c +- 0.05 (tests/test_flathist.py:69-81) holds the root only
+# 0.003 from its edge; the bracket here is wider and the root is checked
+# against the converged value.
+BETA_EQH_POTTS10_L8 = 1.3788
+
+
 def test_multicanonical_potts_double_peak(cuda):
     from exact_helpers import golden
 
@@ -244,11 +292,12 @@ def test_multicanonical_potts_double_peak(cuda):
     res = WangLandau(model, e_window=(-1.95, -0.6), seed=9).run(1e-5)
     out = Multicanonical(model, res.ln_g, e_window=(-1.95, -0.6), seed=10).run(100_000)
     bc = float(golden()["potts_beta_c"]["10"])
-    b = out.equal_height_beta((bc - 0.05, bc + 0.05), split=-1.3)
+    b = out.equal_height_beta((bc - 0.1, bc + 0.05), split=-1.3)
     dp = out.double_peak(b, split=-1.3)
     assert dp["p_ordered"] == pytest.approx(dp["p_disordered"], rel=1e-6)
     assert dp["e_ordered"] < -1.5 < -1.1 < dp["e_disordered"]
-    assert abs(b - bc) < 0.05
+    assert abs(b - BETA_EQH_POTTS10_L8) < 0.015
+    assert abs(b - bc) < 0.065
 
 
 def _wl_result_with_a_missed_level(L=6, level=12):

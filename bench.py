@@ -225,7 +225,7 @@ def cluster_bench(dev, updates: int = 20) -> dict:
 def fh_bench(dev) -> dict:
     """Wang-Landau moves on the q = 10 Potts 8 x 8 torus, energy window [-1.95, -0.6]
     per site (critmc's flat-histogram double-peak case): 4736 walkers (32 per SM)
-    and 14208 walkers (96 per SM, three shared-memory blocks) x 200,000 moves in
+    and 18944 walkers (128 per SM, four shared-memory blocks) x 200,000 moves in
     one launch, and one walker x 1,000,000 moves, each with
     constant ln f and in 1/t mode; the C oracle runs one walker on one host core
     (2,000,000 moves) for comparison."""
@@ -237,7 +237,7 @@ def fh_bench(dev) -> dict:
 
     model = Potts(square(8), 10)
     out = {}
-    for nw, moves in ((4736, 200_000), (14208, 200_000), (1, 1_000_000)):
+    for nw, moves in ((4736, 200_000), (18944, 200_000), (1, 1_000_000)):
         for one_t in (0, 1):
             wl = WangLandau(model, e_window=(-1.95, -0.6), seed=5, n_walkers=nw, device=dev)
             W = wl.walkers
@@ -267,7 +267,7 @@ def fh_bench(dev) -> dict:
                   2_000_000)
     cpu = 2_000_000 / (time.perf_counter() - t0) / 1e9
     out["cpu_oracle_one_walker_one_core_moves_per_ns"] = cpu
-    out["batch_over_cpu_core"] = out["walkers14208_const_moves_per_ns"] / cpu
+    out["batch_over_cpu_core"] = out["walkers18944_const_moves_per_ns"] / cpu
     return out
 
 
@@ -278,7 +278,7 @@ def small_case(dev, case: str) -> dict:
     temperatures, 31 steps.  on-small: the O(n) block kernel on 128 XY chains of
     128 x 128 (16 temperatures x 8), 2 steps of 1 heat bath + 4 over-relaxation.
     fh-single / fh-batch: Wang-Landau moves (ln f = 1e-3) of one walker (500,000
-    moves) or of 4736 walkers (32 per SM, 200,000 moves each) on the q = 10 Potts
+    moves) or of 18944 walkers (128 per SM, 200,000 moves each) on the q = 10 Potts
     8 x 8 torus, energy window [-1.95, -0.6] per site.
     """
     import torch
@@ -288,7 +288,7 @@ def small_case(dev, case: str) -> dict:
         from critmc_b200 import Potts, square
         from critmc_b200.flathist import WangLandau
 
-        nw, moves = (1, 500_000) if case == "fh-single" else (4736, 200_000)
+        nw, moves = (1, 500_000) if case == "fh-single" else (18944, 200_000)
         wl = WangLandau(Potts(square(8), 10), e_window=(-1.95, -0.6), seed=5, n_walkers=nw, device=dev)
         W = wl.walkers
         lng = torch.zeros((nw, wl.levels.size), dtype=torch.float64, device=dev)

@@ -115,9 +115,10 @@ __device__ __forceinline__ void fh_neighbours(const FhWalk& P, int i, int* nb) {
 // The entry of the current level and its pending visit count stay in
 // registers until the walk leaves the level: the additions to ln g(idx) are
 // the same, in the same order, as with a store after every move.
-template <int MODE, int POTTS, int DIM>  // MODE 0 Wang-Landau, 1 multicanonical
-__device__ __forceinline__ void fh_walk(const FhWalk& P, int w, int8_t* s, double* lng, long long* hist,
-                                        long long* counts) {
+// HT, CT: histogram and count types (int64 in global memory; int32 in shared
+// memory, where the histogram holds this launch's visits only)
+template <int MODE, int POTTS, int DIM, typename HT, typename CT>  // MODE 0 Wang-Landau, 1 multicanonical
+__device__ __forceinline__ void fh_walk(const FhWalk& P, int w, int8_t* s, double* lng, HT* hist, CT* counts) {
   constexpr int Z = 2 * DIM;
   const int n = P.lx * P.ly * P.lz;
   const int lo = P.window[2 * w], hi = P.window[2 * w + 1];
@@ -202,7 +203,7 @@ __device__ __forceinline__ void fh_walk(const FhWalk& P, int w, int8_t* s, doubl
       const bool moved = acc && nidx != idx;
       if (moved) {
         if (MODE == 0) lng[idx] = cur;
-        hist[idx] += pending;
+        hist[idx] += (HT)pending;
         pending = 0;
       }
       cur = moved ? g_new : cur;
@@ -218,13 +219,13 @@ __device__ __forceinline__ void fh_walk(const FhWalk& P, int w, int8_t* s, doubl
       long long o = m;
       if (POTTS) {
         o = 0;
-        for (int k = 0; k < P.q; ++k) o += counts[k] * counts[k];
+        for (int k = 0; k < P.q; ++k) o += (long long)counts[k] * counts[k];
       }
       P.order_out[(size_t)w * P.n_meas + meas] = o;
     }
   }
   if (MODE == 0) lng[idx] = cur;
-  hist[idx] += pending;
+  hist[idx] += (HT)pending;
   P.idx[w] = idx;
   P.trials[w] = t;
   if (!POTTS) P.order[w] = m;
@@ -235,14 +236,17 @@ __global__ void __launch_bounds__(FH_THREADS) fh_kernel_global(const __grid_cons
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.n_walkers) return;
   const size_t n = (size_t)P.lx * P.ly * P.lz;
-  fh_walk<MODE, POTTS, DIM>(P, w, P.spins + w * n, P.lng + (size_t)w * P.levels, P.hist + (size_t)w * P.levels,
-                            POTTS ? P.order + (size_t)w * P.q : nullptr);
+  fh_walk<MODE, POTTS, DIM, long long, long long>(P, w, P.spins + w * n, P.lng + (size_t)w * P.levels,
+                                                 P.hist + (size_t)w * P.levels,
+                                                 POTTS ? P.order + (size_t)w * P.q : nullptr);
 }
 
 // The walkers of a block keep their spins, ln g (or ln w), histogram and Potts
 // counts in shared memory for the whole launch: loads and stores of the move
-// chain then never leave the SM.  Per walker, at a 16-byte aligned stride:
-// ln g [levels] double | hist [levels] int64 | counts [q] int64 | spins [N] int8.
+// chain then never leave the SM.  Per walker, at a stride that is an odd
+// number of 8-byte words (so the lanes of a warp spread over the banks):
+// ln g [levels] double | this launch's visits [levels] int32 | counts [q] int32
+// | spins [N] int8.  The host keeps a launch below 2^31 moves per walker.
 template <int MODE, int POTTS, int DIM>
 __global__ void __launch_bounds__(FH_STAGED_WALKERS) fh_kernel_staged(const __grid_constant__ FhWalk P) {
   extern __shared__ __align__(16) unsigned char fh_smem[];
@@ -251,18 +255,18 @@ __global__ void __launch_bounds__(FH_STAGED_WALKERS) fh_kernel_staged(const __gr
   const int tid = threadIdx.x, nt = blockDim.x;
   const int n = P.lx * P.ly * P.lz, L = P.levels, Q = POTTS ? P.q : 0;
   const int stride = P.smem_stride;
-  const int off_hist = 8 * L, off_counts = 16 * L, off_spins = 16 * L + 8 * Q;
+  const int off_hist = 8 * L, off_counts = 12 * L, off_spins = 12 * L + 4 * Q;
   // cooperative, coalesced copies of the block's contiguous span of each array
   for (int e = tid; e < nb * L; e += nt) {
     const int ww = e / L, k = e - ww * L;
     unsigned char* base = fh_smem + (size_t)ww * stride;
     reinterpret_cast<double*>(base)[k] = P.lng[(size_t)w0 * L + e];
-    reinterpret_cast<long long*>(base + off_hist)[k] = P.hist[(size_t)w0 * L + e];
+    reinterpret_cast<int*>(base + off_hist)[k] = 0;
   }
   if constexpr (POTTS != 0) {
     for (int e = tid; e < nb * Q; e += nt) {
       const int ww = e / Q, k = e - ww * Q;
-      reinterpret_cast<long long*>(fh_smem + (size_t)ww * stride + off_counts)[k] = P.order[(size_t)w0 * Q + e];
+      reinterpret_cast<int*>(fh_smem + (size_t)ww * stride + off_counts)[k] = (int)P.order[(size_t)w0 * Q + e];
     }
   }
   for (int e = tid; e < nb * n; e += nt) {
@@ -272,21 +276,21 @@ __global__ void __launch_bounds__(FH_STAGED_WALKERS) fh_kernel_staged(const __gr
   __syncthreads();
   if (tid < nb) {
     unsigned char* base = fh_smem + (size_t)tid * stride;
-    fh_walk<MODE, POTTS, DIM>(P, w0 + tid, reinterpret_cast<int8_t*>(base + off_spins),
-                              reinterpret_cast<double*>(base), reinterpret_cast<long long*>(base + off_hist),
-                              POTTS ? reinterpret_cast<long long*>(base + off_counts) : nullptr);
+    fh_walk<MODE, POTTS, DIM, int, int>(P, w0 + tid, reinterpret_cast<int8_t*>(base + off_spins),
+                                        reinterpret_cast<double*>(base), reinterpret_cast<int*>(base + off_hist),
+                                        POTTS ? reinterpret_cast<int*>(base + off_counts) : nullptr);
   }
   __syncthreads();
   for (int e = tid; e < nb * L; e += nt) {
     const int ww = e / L, k = e - ww * L;
     const unsigned char* base = fh_smem + (size_t)ww * stride;
     if (MODE == 0) P.lng[(size_t)w0 * L + e] = reinterpret_cast<const double*>(base)[k];
-    P.hist[(size_t)w0 * L + e] = reinterpret_cast<const long long*>(base + off_hist)[k];
+    P.hist[(size_t)w0 * L + e] += reinterpret_cast<const int*>(base + off_hist)[k];
   }
   if constexpr (POTTS != 0) {
     for (int e = tid; e < nb * Q; e += nt) {
       const int ww = e / Q, k = e - ww * Q;
-      P.order[(size_t)w0 * Q + e] = reinterpret_cast<const long long*>(fh_smem + (size_t)ww * stride + off_counts)[k];
+      P.order[(size_t)w0 * Q + e] = reinterpret_cast<const int*>(fh_smem + (size_t)ww * stride + off_counts)[k];
     }
   }
   for (int e = tid; e < nb * n; e += nt) {
@@ -452,17 +456,23 @@ extern "C" int32_t critmc_fh_run(int32_t mode, int8_t* spins, int32_t dim, int32
   // that way, or when at least 256 fit an SM; otherwise (large lattices, many
   // walkers) the register-limited global-memory kernel keeps more in flight.
   const long long n = (long long)lx * ly * lz;
-  const long long stride = (16LL * levels + 8LL * (q ? q : 0) + n + 15) / 16 * 16;
+  long long stride = (12LL * levels + 4LL * (q ? q : 0) + n + 7) / 8 * 8;
+  if ((stride / 8) % 2 == 0) stride += 8;
+  const long long per_walker_moves = moves * (long long)P.n_meas;
   int dev = 0, smem_max = 0, smem_sm = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return cuda_fail("device attributes");
-  const long long fit = smem_max / stride, per_sm = smem_sm / stride;
-  if (force_shared && fit < 1) return fail(CRITMC_ERR_INVALID, "a walker does not fit in shared memory");
-  const bool staged = force_shared || (!force_global && fit >= 1 && (per_sm >= 256 || per_sm * sms >= n_walkers));
+  const long long fit = smem_max / stride;
   const int wpb = (int)std::min<long long>(FH_STAGED_WALKERS, std::max<long long>(fit, 1));
+  // resident walkers per SM: whole blocks, each with 1 KB of shared memory reserved
+  const long long per_sm = wpb * (smem_sm / (wpb * stride + 1024));
+  const bool can_stage = fit >= 1 && per_walker_moves < (1LL << 31);
+  if (force_shared && !can_stage)
+    return fail(CRITMC_ERR_INVALID, "a walker does not fit in shared memory, or 2^31 moves or more in one call");
+  const bool staged = force_shared || (!force_global && can_stage && (per_sm >= 256 || per_sm * sms >= n_walkers));
   P.smem_stride = (int)std::min<long long>(stride, 1 << 30);
   cudaStream_t s = (cudaStream_t)stream;
   if (mode == 0) return q == 0 ? fh_launch_dim<0, 0>(P, staged, wpb, s) : fh_launch_dim<0, 1>(P, staged, wpb, s);

@@ -375,9 +375,10 @@ int32_t critmc_stream_update(const void* values, int32_t is_double, int32_t n_ch
  * or, where one_over_t [w] is set, ln f = n_levels [w] / (trials - t_base [w]
  * + 1); `moves` per walker.  Mode 1: n_meas measurements of `moves` moves each,
  * idx_out / order_out [w][n_meas] (Ising M, Potts sum_k n_k^2).  Walkers
- * run in shared memory when all can be resident that way or >= 256 fit an SM,
- * else in global memory; mode | 0x10 forces global memory, mode | 0x20 shared
- * memory (same results).  At most 2^24 sites per walker.
+ * run in shared memory when all can be resident that way or >= 256 fit an SM
+ * (and a call makes fewer than 2^31 moves per walker), else in global memory;
+ * mode | 0x10 forces global memory, mode | 0x20 shared memory (same results).
+ * At most 2^24 sites per walker.
  * Replaces critmc kernels/flathist.py:28-132.                                */
 int32_t critmc_fh_run(int32_t mode, int8_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz, int32_t q,
                       int32_t n_walkers, const uint32_t* keys, int32_t levels, int64_t* idx, int64_t* order,

@@ -180,6 +180,8 @@ def test_wang_landau_matches_replay(cuda):
     res = wl.run(1e-4, checkpoints=[1000, 50_000, 10**9])
     lv = res.levels
     r = replay_wang_landau((4, 4), 0, s, key, idx, wl.window, lv.size, 16, 1e-4, checkpoints=[1000, 50_000, 10**9])
+    np.testing.assert_array_equal(wl.state, r["state"])
+    assert wl.idx == r["idx"]
     assert np.array_equal(res.ln_g, r["ln_g"])
     assert np.array_equal(res.visited, r["visited"])
     assert res.trials == r["trials"] and res.ln_f == r["ln_f"] and res.stages == r["stages"]
@@ -202,6 +204,9 @@ def test_wang_landau_batch_of_windows_matches_replay(cuda):
         assert res.window == wl.windows[w]
         assert np.array_equal(res.ln_g, r["ln_g"]), w
         assert res.trials == r["trials"] and res.stages == r["stages"]
+    # walkers that finished first were frozen during the run; their windows are back
+    np.testing.assert_array_equal(wl.walkers.window.cpu().numpy(), np.array(wl.windows))
+    assert wl.state.shape == (4, 12) and len(wl.idx) == 4
 
 
 @pytest.mark.parametrize("n_walkers", [1, 4])

@@ -42,6 +42,7 @@
 namespace critmc {
 
 constexpr int CL_THREADS = 256;
+static_assert(CL_THREADS % 32 == 0, "the decide kernel's warp-uniform loop needs whole warps");
 constexpr int CL_PCHAINS = 256;
 constexpr uint32_t TAG_BOND = 0x07u, TAG_CLFLIP = 0x08u, TAG_WOLFF = 0x09u, TAG_ONAXIS = 0x0Bu;
 
@@ -206,15 +207,25 @@ __global__ void __launch_bounds__(CL_THREADS) cl_decide_kernel(const __grid_cons
     }
   }
   long long flipped = 0;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < P.n; u += gridDim.x * blockDim.x) {
-    const int r = L[u];
+  // warp-uniform loop (blockDim is a multiple of 32): every lane takes part in
+  // the match below on every pass
+  for (uint32_t base = blockIdx.x * blockDim.x; base < P.n; base += gridDim.x * blockDim.x) {
+    const uint32_t u = base + threadIdx.x;
+    const bool valid = u < P.n;
+    const int r = valid ? L[u] : -1;
+    if (P.algo == CRITMC_SWENDSEN_WANG) {
+      // one atomic per group of lanes with the same root: the root of a giant
+      // cluster would otherwise take one atomic per site
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, r);
+      if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&S[r], __popc(peers));
+    }
+    if (!valid) continue;
     if (P.on_n) {  // O(n): newv is the reflect flag
       int f = 0;
       if (P.algo == CRITMC_WOLFF) {
         f = r == root;
         flipped += f;
       } else {
-        atomicAdd(&S[r], 1);
         f = (int)(critmc_philox4x32((uint32_t)r, P.sweep, TAG_CLFLIP, 0u, k0, k1).v[0] >> 31);
       }
       nv[u] = (int8_t)f;
@@ -228,7 +239,6 @@ __global__ void __launch_bounds__(CL_THREADS) cl_decide_kernel(const __grid_cons
         ++flipped;
       }
     } else {
-      atomicAdd(&S[r], 1);
       const uint32_t w = critmc_philox4x32((uint32_t)r, P.sweep, TAG_CLFLIP, 0u, k0, k1).v[0];
       v = P.potts ? (int)(((unsigned long long)w * (unsigned)P.q) >> 32) : ((w >> 31) ? -old : old);
     }

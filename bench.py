@@ -279,12 +279,37 @@ def small_case(dev, case: str) -> dict:
     128 x 128 (16 temperatures x 8), 2 steps of 1 heat bath + 4 over-relaxation.
     fh-single / fh-batch: Wang-Landau moves (ln f = 1e-3) of one walker (500,000
     moves) or of 18944 walkers (128 per SM, 200,000 moves each) on the q = 10 Potts
-    8 x 8 torus, energy window [-1.95, -0.6] per site.
+    8 x 8 torus, energy window [-1.95, -0.6] per site.  cluster-sw: Swendsen-Wang
+    updates of one 2D Ising chain of 1024 x 1024 (bit layout) at beta_c, two
+    warm-up updates and one timed.
     """
     import torch
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if case in ("fh-single", "fh-batch"):
+    if case == "cluster-sw":
+        from critmc_b200 import Ising, _lib, square
+        from critmc_b200.device import empty_bytes, ptr, stream_handle
+
+        model = Ising(square(1024))
+        rng = np.random.default_rng(1)
+        s0 = model.initial_state("random", rng)
+        ch = model.to_device(s0, rng, dev)
+        scratch = empty_bytes(_lib.lib().critmc_cluster_scratch_bytes(1, model.n_sites), dev)
+        stats = torch.zeros((1, 3), dtype=torch.int64, device=dev)
+        run = torch.zeros((1, 2), dtype=torch.int64, device=dev)
+
+        def sw(sweep):
+            _lib.call("critmc_cluster_update", 1, ptr(ch.words), 2, 1024, 1024, 1, 0, 1, ch.key.ctypes.data,
+                      0.4406868, 4, sweep, ptr(run), None, ptr(stats), ptr(scratch), stream_handle(dev))
+
+        sw(0)
+        sw(1)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        sw(2)
+        e1.record()
+        units = model.n_sites
+    elif case in ("fh-single", "fh-batch"):
         from critmc_b200 import Potts, square
         from critmc_b200.flathist import WangLandau
 
@@ -470,7 +495,7 @@ def main() -> None:
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
     ap.add_argument("--serve-grid-lanes", type=int, default=8, help="requests on multi-block lanes at once")
-    ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch"],
+    ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch", "cluster-sw"],
                     help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

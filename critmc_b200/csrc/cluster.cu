@@ -259,7 +259,22 @@ __global__ void cl_sw_clear_kernel(long long* stats, int c0, int nc) {
   }
 }
 
-// SW statistics: sum |C|^2 and the number of clusters (roots have L[u] == u)
+// block sum of one value per thread (blockDim a multiple of 32, at most 1024);
+// the result is valid in thread 0
+__device__ __forceinline__ long long cl_block_sum(long long v, long long* red) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  long long t = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// SW statistics: sum |C|^2 and the number of clusters (roots have L[u] == u);
+// one atomic per block and counter (a per-warp atomic on the same two
+// addresses serialises thousands of them)
 __global__ void cl_sw_stats_kernel(ClParams P) {
   const int chain = P.chain0 + blockIdx.y;
   const int* L = P.label + (size_t)chain * P.n;
@@ -270,9 +285,10 @@ __global__ void cl_sw_stats_kernel(ClParams P) {
       c2 += (long long)S[u] * S[u];
       ++ncl;
     }
-  c2 = warp_sum(c2);
-  ncl = warp_sum(ncl);
-  if ((threadIdx.x & 31) == 0) {
+  __shared__ long long red[32];
+  c2 = cl_block_sum(c2, red);
+  ncl = cl_block_sum(ncl, red);
+  if (threadIdx.x == 0) {
     unsigned long long* st = reinterpret_cast<unsigned long long*>(P.stats + 3 * chain);
     if (c2) atomicAdd(st + 1, as_ull(c2));
     if (ncl) atomicAdd(st + 2, as_ull(ncl));
@@ -299,8 +315,9 @@ __global__ void __launch_bounds__(CL_THREADS) cl_delta_kernel(const __grid_const
       else de += (long long)o0 * o1 - (long long)n0 * n1;                // E_b = -sum s s
     }
   }
-  de = warp_sum(de);
-  if ((threadIdx.x & 31) == 0 && de) {
+  __shared__ long long red[32];
+  de = cl_block_sum(de, red);  // one atomic per block
+  if (threadIdx.x == 0 && de) {
     long long* e = P.potts ? P.running + chain : P.running + 2 * chain;
     atomicAdd(reinterpret_cast<unsigned long long*>(e), as_ull(de));
   }
@@ -379,19 +396,21 @@ static int cl_launch(ClParams& P, int n_chains, const uint32_t* keys, cudaStream
     std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
     if (P.algo == CRITMC_SWENDSEN_WANG) cl_sw_clear_kernel<<<(nc + 127) / 128, 128, 0, s>>>(P.stats, c0, nc);
     const dim3 gs(bx_sites, nc), gb(bx_slots, nc), gw(std::max(1u, bx_words), nc);
+    // the reductions run on at most 2 blocks per SM: fewer same-address atomics
+    const dim3 gs_red(std::min(bx_sites, 296u), nc), gb_red(std::min(bx_slots, 296u), nc);
     cl_init_kernel<<<gs, CL_THREADS, 0, s>>>(P);
     if (P.g.dim == 1) cl_link_kernel<2><<<gb, CL_THREADS, 0, s>>>(P);
     else if (P.g.dim == 2) cl_link_kernel<4><<<gb, CL_THREADS, 0, s>>>(P);
     else cl_link_kernel<6><<<gb, CL_THREADS, 0, s>>>(P);
     cl_flatten_kernel<<<gs, CL_THREADS, 0, s>>>(P);
     cl_decide_kernel<<<gs, CL_THREADS, 0, s>>>(P);
-    if (P.algo == CRITMC_SWENDSEN_WANG) cl_sw_stats_kernel<<<gs, CL_THREADS, 0, s>>>(P);
+    if (P.algo == CRITMC_SWENDSEN_WANG) cl_sw_stats_kernel<<<gs_red, CL_THREADS, 0, s>>>(P);
     if (P.on_n) {
       cl_on_apply_kernel<<<gs, CL_THREADS, 0, s>>>(P);
     } else {
-      if (P.g.dim == 1) cl_delta_kernel<2><<<gb, CL_THREADS, 0, s>>>(P);
-      else if (P.g.dim == 2) cl_delta_kernel<4><<<gb, CL_THREADS, 0, s>>>(P);
-      else cl_delta_kernel<6><<<gb, CL_THREADS, 0, s>>>(P);
+      if (P.g.dim == 1) cl_delta_kernel<2><<<gb_red, CL_THREADS, 0, s>>>(P);
+      else if (P.g.dim == 2) cl_delta_kernel<4><<<gb_red, CL_THREADS, 0, s>>>(P);
+      else cl_delta_kernel<6><<<gb_red, CL_THREADS, 0, s>>>(P);
       cl_apply_kernel<<<P.bits ? gw : gs, CL_THREADS, 0, s>>>(P);
     }
     if (int e = cuda_check("launch")) return e;

@@ -17,9 +17,12 @@ from pathlib import Path
 
 import numpy as np
 
-from critmc import chain, square  # noqa: F401  (critmc must be on PYTHONPATH)
+from critmc import Potts, chain, square  # noqa: F401  (critmc must be on PYTHONPATH)
 from critmc.exact import chains, dos, enumeration, kaufman, onsager, potts
+from critmc.flathist import WangLandau
 from critmc.stats.autocorr import gamma_method
+from scipy.optimize import brentq
+from scipy.special import logsumexp
 
 OUT = Path(__file__).resolve().parent / "critmc_exact.json"
 
@@ -41,6 +44,21 @@ def ar1(seed: int, phi: float, n: int) -> np.ndarray:
     for i in range(1, n):
         x[i] = phi * x[i - 1] + e[i]
     return x
+
+
+def equal_height_beta(res, split: float, bracket) -> float:
+    """beta at which the two maxima of the energy distribution from ln g are equal."""
+    lv = res.levels
+    v = res.visited
+    e = lv.energies / lv.n_sites
+
+    def f(b):
+        a = np.where(v, res.ln_g - b * lv.energies, -np.inf)
+        p = np.exp(a - logsumexp(a[v]))
+        low = e < split
+        return np.log(p[low].max()) - np.log(p[~low].max())
+
+    return float(brentq(f, *bracket, xtol=1e-10))
 
 
 def main() -> None:
@@ -90,6 +108,13 @@ def main() -> None:
     out["kaufman_energy"]["6"] = {f"{b:.10f}": float(kaufman.energy(b, 6)) for b in (0.3, 0.44, 0.55, 0.6)}
     out["potts3_dos_square4x3"] = joint(enumeration.potts_joint_dos(square(4, 3), 3))
     out["potts_beta_c"] = {str(q): float(potts.beta_c(q)) for q in (3, 10)}
+    # equal-height point of q = 10 Potts on the 8 x 8 torus, window [-1.95, -0.6],
+    # split -1.3, from critmc's own Wang-Landau converged to ln f = 1e-6
+    model, bc = Potts(square(8), 10), float(potts.beta_c(10))
+    eq = [equal_height_beta(WangLandau(model, e_window=(-1.95, -0.6), seed=s).run(1e-6), -1.3, (bc - 0.2, bc + 0.1))
+          for s in (1, 2, 3, 4)]
+    out["potts10_L8_equal_height"] = {"beta": float(np.mean(eq)), "per_seed": eq, "ln_f_final": 1e-6,
+                                      "window": [-1.95, -0.6], "split": -1.3}
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

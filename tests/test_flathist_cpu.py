@@ -149,3 +149,33 @@ def test_oracle_descent_is_consistent_and_reaches_the_window_from_order(kind, sh
         assert (steps >= 0) == (lo <= idx <= hi)
         if start == "ordered":
             assert steps >= 0
+
+
+def test_oracle_wang_landau_equal_height_point_matches_critmc():
+    """The oracle's converged ln g of the q = 10 Potts 8 x 8 torus gives the
+    equal-height point that critmc's own Wang-Landau gives (fixture)."""
+    from exact_helpers import golden
+    from scipy.optimize import brentq
+    from scipy.special import logsumexp
+
+    ref = golden()["potts10_L8_equal_height"]
+    model = Potts(square(8), 10)
+    lv = EnergyLevels.of(model)
+    window = lv.window(*ref["window"])
+    lv, s, idx, key = _walker(model, 1, (0, lv.size - 1))
+    import oracle
+    from flathist_replay import initial_order
+
+    idx, steps = oracle.fh_descend(s, (8, 8), 10, key, idx, initial_order(s, 10), window, 10**6)
+    assert steps >= 0
+    r = replay_wang_landau((8, 8), 10, s, key, idx, window, lv.size, 64, ref["ln_f_final"])
+    e = lv.energies / 64
+    v = r["visited"]
+
+    def f(b):
+        a = np.where(v, r["ln_g"] - b * lv.energies, -np.inf)
+        p = np.exp(a - logsumexp(a[v]))
+        low = e < ref["split"]
+        return np.log(p[low].max()) - np.log(p[~low].max())
+
+    assert brentq(f, 1.2, 1.5) == pytest.approx(ref["beta"], abs=0.002)

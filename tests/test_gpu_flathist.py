@@ -282,12 +282,10 @@ def test_multicanonical_reweighting_to_canonical(cuda):
 
 
 # Equal-height point of the q = 10 Potts 8 x 8 torus in the window [-1.95, -0.6]
-# (split -1.3): 1.3788, from oracle Wang-Landau runs converged to ln f = 1e-6
-# for four seeds (spread 0.0006).  It lies 0.047 below beta_c, so critmc's own
-# bracket beta_c +- 0.05 (tests/test_flathist.py:69-81) holds the root only
-# 0.003 from its edge; the bracket here is wider and the root is checked
-# against the converged value.
-BETA_EQH_POTTS10_L8 = 1.3788
+# (split -1.3): critmc's own Wang-Landau converged to ln f = 1e-6, four seeds
+# (fixture).  It lies 0.047 below beta_c, so critmc's own test bracket
+# beta_c +- 0.05 (tests/test_flathist.py:69-81) holds the root only 0.003 from
+# its edge; the bracket here is wider and the root is checked against it.
 
 
 def test_multicanonical_potts_double_peak(cuda):
@@ -301,7 +299,7 @@ def test_multicanonical_potts_double_peak(cuda):
     dp = out.double_peak(b, split=-1.3)
     assert dp["p_ordered"] == pytest.approx(dp["p_disordered"], rel=1e-6)
     assert dp["e_ordered"] < -1.5 < -1.1 < dp["e_disordered"]
-    assert abs(b - BETA_EQH_POTTS10_L8) < 0.015
+    assert abs(b - golden()["potts10_L8_equal_height"]["beta"]) < 0.015
     assert abs(b - bc) < 0.065
 
 

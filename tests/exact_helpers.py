@@ -130,3 +130,26 @@ def ising_log_g_square6() -> np.ndarray:
 
     g = [int(v) for v in golden()["ising_dos_square6"]["g"]]
     return np.array([math.log(v) if v > 0 else -np.inf for v in g])
+
+
+def synthetic_muca(seed: int = 20261204):
+    """A seeded bimodal multicanonical record on the q = 10 Potts 8 x 8 levels.
+
+    Energies per site are drawn from two Gaussians (ordered near -1.65,
+    disordered near -0.97) inside the window [-1.95, -0.6], with weights
+    ln g(E) = 1.40 E + const, so reweighting to beta near 1.40 returns the drawn
+    mixture.  Returns (ln_g, level_series, order_series, window, hist) for the
+    analysis methods of the multicanonical and Wang-Landau results.
+    """
+    rng = np.random.default_rng(seed)
+    n_sites, n_bonds, levels = 64, 128, 129
+    lo, hi = 4, 89  # window [-1.95, -0.6] per site
+    n = 40_000
+    pick = rng.random(n) < 0.45
+    e = np.where(pick, rng.normal(-1.65, 0.06, n), rng.normal(-0.97, 0.09, n))
+    idx = np.clip(np.rint(e * n_sites + n_bonds).astype(np.int64), lo, hi)
+    energies = np.arange(levels) - float(n_bonds)
+    ln_g = 1.40 * energies + 7.0
+    order = rng.integers(n_sites ** 2 // 10, n_sites ** 2, n).astype(np.int64)
+    hist = np.bincount(idx, minlength=levels).astype(np.int64)
+    return ln_g, idx, order, (lo, hi), hist

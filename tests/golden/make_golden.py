@@ -19,7 +19,7 @@ import numpy as np
 
 from critmc import Potts, chain, square  # noqa: F401  (critmc must be on PYTHONPATH)
 from critmc.exact import chains, dos, enumeration, kaufman, onsager, potts
-from critmc.flathist import WangLandau
+from critmc.flathist import EnergyLevels, MucaResult, WangLandau, WLResult
 from critmc.stats.autocorr import gamma_method
 from scipy.optimize import brentq
 from scipy.special import logsumexp
@@ -115,6 +115,32 @@ def main() -> None:
           for s in (1, 2, 3, 4)]
     out["potts10_L8_equal_height"] = {"beta": float(np.mean(eq)), "per_seed": eq, "ln_f_final": 1e-6,
                                       "window": [-1.95, -0.6], "split": -1.3}
+    # critmc's analysis methods on a seeded synthetic multicanonical record
+    import sys
+
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+    from exact_helpers import synthetic_muca
+
+    ln_g, idx, order, window, hist = synthetic_muca()
+    lv = EnergyLevels("potts", 64, 128, 10)
+    mu = MucaResult(lv, ln_g, idx, order, window, hist)
+    ana: dict = {"canonical": {k: v.tolist() for k, v in mu.canonical([1.36, 1.40, 1.44]).items()},
+                 "m2_head": mu.order_parameter_m2()[:8].tolist(),
+                 "average_m2": mu.average(1.40, mu.order_parameter_m2())}
+    for smooth in (0.0, 0.01):
+        ana[f"p_smooth{smooth}"] = mu.energy_distribution(1.40, smooth)[1].tolist()
+        ana[f"double_peak_smooth{smooth}"] = mu.double_peak(1.40, -1.3, smooth)
+        ana[f"equal_height_smooth{smooth}"] = mu.equal_height_beta((1.2, 1.6), -1.3, smooth)
+    ana["double_peak_auto_split"] = mu.double_peak(1.40)
+    ana["phase_means"] = mu.phase_means(1.40, -1.3)
+    ana["equal_weight"] = mu.equal_weight_beta((1.2, 1.6), -1.3)
+    visited = hist > 0
+    for win in (window, (0, lv.size - 1)):
+        wl = WLResult(lv, np.where(visited, ln_g, 0.0), visited, win, 0, 0.0, 0.0)
+        key = "wl_full" if win == (0, lv.size - 1) else "wl_window"
+        ana[key] = {"normalized": np.where(visited, wl.normalized(), 0.0).tolist(),
+                    "canonical": {k: v.tolist() for k, v in wl.canonical([1.36, 1.40]).items()}}
+    out["flathist_analysis"] = ana
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

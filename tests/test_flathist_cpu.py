@@ -179,3 +179,38 @@ def test_oracle_wang_landau_equal_height_point_matches_critmc():
         return np.log(p[low].max()) - np.log(p[~low].max())
 
     assert brentq(f, 1.2, 1.5) == pytest.approx(ref["beta"], abs=0.002)
+
+
+def test_analysis_methods_match_critmc_on_a_synthetic_record():
+    """MucaResult / WLResult analysis (critmc flathist.py:133-171, 322-452) on a
+    seeded synthetic record equals critmc's own methods on it (fixture)."""
+    from exact_helpers import golden, synthetic_muca
+
+    ref = golden()["flathist_analysis"]
+    ln_g, idx, order, window, hist = synthetic_muca()
+    lv = EnergyLevels("potts", 64, 128, 10)
+    mu = MucaResult(lv, ln_g, idx, order, window, hist)
+    got = mu.canonical([1.36, 1.40, 1.44])
+    for k, v in ref["canonical"].items():
+        np.testing.assert_allclose(got[k], v, rtol=1e-12)
+    np.testing.assert_allclose(mu.order_parameter_m2()[:8], ref["m2_head"], rtol=1e-12)
+    assert mu.average(1.40, mu.order_parameter_m2()) == pytest.approx(ref["average_m2"], rel=1e-12)
+    for smooth in (0.0, 0.01):
+        np.testing.assert_allclose(mu.energy_distribution(1.40, smooth)[1], ref[f"p_smooth{smooth}"],
+                                   rtol=1e-10, atol=1e-300)
+        for k, v in mu.double_peak(1.40, -1.3, smooth).items():
+            assert v == pytest.approx(ref[f"double_peak_smooth{smooth}"][k], rel=1e-10, nan_ok=True), k
+        assert mu.equal_height_beta((1.2, 1.6), -1.3, smooth) == pytest.approx(ref[f"equal_height_smooth{smooth}"],
+                                                                             abs=1e-9)
+    for k, v in mu.double_peak(1.40).items():
+        assert v == pytest.approx(ref["double_peak_auto_split"][k], rel=1e-10, nan_ok=True), k
+    for k, v in mu.phase_means(1.40, -1.3).items():
+        assert v == pytest.approx(ref["phase_means"][k], rel=1e-12), k
+    assert mu.equal_weight_beta((1.2, 1.6), -1.3) == pytest.approx(ref["equal_weight"], abs=1e-9)
+    visited = hist > 0
+    for win, key in ((window, "wl_window"), ((0, lv.size - 1), "wl_full")):
+        wl = WLResult(lv, np.where(visited, ln_g, 0.0), visited, win, 0, 0.0, 0.0)
+        np.testing.assert_allclose(np.where(visited, wl.normalized(), 0.0), ref[key]["normalized"], rtol=1e-12)
+        got = wl.canonical([1.36, 1.40])
+        for k, v in ref[key]["canonical"].items():
+            np.testing.assert_allclose(got[k], v, rtol=1e-10)

@@ -77,3 +77,34 @@ def replay_multicanonical(shape, q: int, state: np.ndarray, key, idx: int, windo
     idx, trials, io, oo = oracle.fh_run(1, s, shape, q, key, idx, order, lw, hist, window, trials, 0.0, 0.0, False,
                                         0, moves, n_meas)
     return {"level_series": io, "order_series": oo, "hist": hist, "state": s, "idx": idx, "trials": trials}
+
+
+def walk_into_window(model, state: np.ndarray, levels, lo: int, hi: int, rng, max_steps: int = 10**7) -> int:
+    """Host restatement of critmc's greedy walk into a level window (flathist.py:96-130).
+
+    A random site gets a proposal (Ising: the flip; Potts: another state drawn
+    uniformly) that is kept when the level does not move away from [lo, hi].
+    ``state`` is changed in place; returns the level reached.
+    """
+    nbr = model.lattice.nbr
+    level = levels.index(model.energy(state))
+    ising = levels.kind == "ising"
+    for _ in range(max_steps):
+        if lo <= level <= hi:
+            return level
+        site = int(rng.integers(model.n_sites))
+        here = int(state[site])
+        around = state[nbr[site]]
+        if ising:
+            proposal = -here
+            new_level = level + here * int(around.astype(np.int64).sum()) // 2
+        else:
+            proposal = int(rng.integers(levels.q - 1))
+            if proposal >= here:
+                proposal += 1
+            new_level = level + int((around == here).sum()) - int((around == proposal).sum())
+        toward = new_level >= level if level < lo else new_level <= level
+        if toward:
+            state[site] = proposal
+            level = new_level
+    raise RuntimeError("the walk did not reach the window")

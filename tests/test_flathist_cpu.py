@@ -7,10 +7,10 @@ from __future__ import annotations
 import numpy as np
 import pytest
 from exact_helpers import JointDOS, ising_log_g_square6, kaufman_energy
-from flathist_replay import replay_multicanonical, replay_wang_landau
+from flathist_replay import replay_multicanonical, replay_wang_landau, walk_into_window
 
 from critmc_b200 import Ising, Potts, square
-from critmc_b200.flathist import EnergyLevels, MucaResult, WLResult, _walk_into_window
+from critmc_b200.flathist import EnergyLevels, MucaResult, WLResult
 
 
 def test_energy_levels_mapping():
@@ -34,7 +34,7 @@ def test_walk_into_window_reaches_the_window(kind):
     lo, hi = lv.window(-1.9, -1.6) if kind == "ising" else lv.window(-1.5, -1.2)
     rng = np.random.default_rng(5)
     s = model.initial_state("random", rng)
-    idx = _walk_into_window(model, s, lv, lo, hi, rng)
+    idx = walk_into_window(model, s, lv, lo, hi, rng)
     assert lo <= idx <= hi and idx == lv.index(model.energy(s))
 
 
@@ -42,7 +42,7 @@ def _walker(model, seed, window):
     lv = EnergyLevels.of(model)
     rng = np.random.default_rng(seed)
     s = model.initial_state("random", rng)
-    idx = _walk_into_window(model, s, lv, *window, rng)
+    idx = walk_into_window(model, s, lv, *window, rng)
     key = rng.integers(0, 1 << 32, size=2, dtype=np.uint64).astype(np.uint32)
     return lv, s.astype(np.int8), idx, key
 
@@ -214,3 +214,52 @@ def test_analysis_methods_match_critmc_on_a_synthetic_record():
         got = wl.canonical([1.36, 1.40])
         for k, v in ref[key]["canonical"].items():
             np.testing.assert_allclose(got[k], v, rtol=1e-10)
+
+
+def _with_oracle_walkers(monkeypatch):
+    import fake_walkers
+
+    import critmc_b200.flathist as fh
+
+    monkeypatch.setattr(fh, "_Walkers", fake_walkers.OracleWalkers)
+    return fh
+
+
+def _start(walkers, w):
+    return walkers.spins[w].numpy().copy(), int(walkers.idx[w]), walkers.keys[w].numpy().view(np.uint32).copy()
+
+
+def test_wang_landau_schedule_on_the_cpu_equals_the_replay(monkeypatch):
+    """WangLandau.run's host schedule (critmc flathist.py:247-320), driven through
+    oracle-backed walkers: every walker of a batch equals the replay of its run."""
+    fh = _with_oracle_walkers(monkeypatch)
+    model = Potts(square(4, 3), 3)
+    wins = [None, (-2.0, -1.0), (-1.5, -0.5)]
+    wl = fh.WangLandau(model, e_window=wins, n_walkers=3, seed=2)
+    starts = [_start(wl.walkers, w) for w in range(3)]
+    results = wl.run(1e-3, checkpoints=[500, 20_000, 10**9])
+    for w, res in enumerate(results):
+        s, idx, key = starts[w]
+        r = replay_wang_landau((4, 3), 3, s, key, idx, wl.windows[w], res.levels.size, 12, 1e-3,
+                               checkpoints=[500, 20_000, 10**9])
+        assert np.array_equal(res.ln_g, r["ln_g"]) and np.array_equal(res.visited, r["visited"])
+        assert res.trials == r["trials"] and res.ln_f == r["ln_f"] and res.stages == r["stages"]
+        assert [c[0] for c in res.checkpoints] == [c[0] for c in r["checkpoints"]]
+        for a, b in zip(res.checkpoints, r["checkpoints"]):
+            assert a[1] == b[1] and np.array_equal(a[2], b[2])
+    np.testing.assert_array_equal(wl.walkers.window.numpy(), np.array(wl.windows))
+
+
+def test_multicanonical_run_on_the_cpu_equals_the_replay(monkeypatch):
+    fh = _with_oracle_walkers(monkeypatch)
+    model = Ising(square(6))
+    lng = ising_log_g_square6()
+    mu = fh.Multicanonical(model, lng, seed=8, n_walkers=2)
+    starts = [_start(mu.walkers, w) for w in range(2)]
+    outs = mu.run(500, sweeps_per_meas=2, n_therm=20)
+    for w, o in enumerate(outs):
+        s, idx, key = starts[w]
+        r = replay_multicanonical((6, 6), 0, s, key, idx, mu.window, mu.ln_w, 72, 500, n_therm=20)
+        np.testing.assert_array_equal(o.level_series, r["level_series"])
+        np.testing.assert_array_equal(o.order_series, r["order_series"])
+        np.testing.assert_array_equal(o.hist, r["hist"])

@@ -11,13 +11,13 @@ import numpy as np
 import pytest
 import torch
 from exact_helpers import JointDOS, ising_log_g_square6, kaufman_energy
-from flathist_replay import initial_order, replay_multicanonical, replay_wang_landau
+from flathist_replay import initial_order, replay_multicanonical, replay_wang_landau, walk_into_window
 
 import oracle
 from critmc_b200 import Ising, Potts, hypercubic, square
 from critmc_b200 import _lib
 from critmc_b200.device import ptr, stream_handle
-from critmc_b200.flathist import EnergyLevels, Multicanonical, WangLandau, _walk_into_window
+from critmc_b200.flathist import EnergyLevels, Multicanonical, WangLandau
 
 pytestmark = pytest.mark.gpu
 
@@ -51,7 +51,7 @@ def test_fh_kernel_bit_identical_to_oracle(cuda, kind, shape, q, mode, path):
     states, idxs, orders = [], [], []
     for lo, hi in windows:
         s = model.initial_state("random", rng)
-        idxs.append(_walk_into_window(model, s, lv, lo, hi, rng))
+        idxs.append(walk_into_window(model, s, lv, lo, hi, rng))
         states.append(s.astype(np.int8))
         orders.append(initial_order(s, q))
     keys = rng.integers(0, 1 << 32, size=(W, 2), dtype=np.uint64).astype(np.uint32)

@@ -141,6 +141,13 @@ def main() -> None:
         ana[key] = {"normalized": np.where(visited, wl.normalized(), 0.0).tolist(),
                     "canonical": {k: v.tolist() for k, v in wl.canonical([1.36, 1.40]).items()}}
     out["flathist_analysis"] = ana
+    # a series written by critmc itself (TimeSeries.save: .npz + JSON metadata),
+    # read back by this project's loader in the format tests
+    from critmc import Ising, Simulation
+
+    sim = Simulation(Ising(square(4)), 0.44, "metropolis", seed=5)
+    sim.thermalize(20)
+    sim.run(200).save(OUT.parent / "critmc_series_ising4.npz")
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

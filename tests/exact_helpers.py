@@ -153,3 +153,49 @@ def synthetic_muca(seed: int = 20261204):
     order = rng.integers(n_sites ** 2 // 10, n_sites ** 2, n).astype(np.int64)
     hist = np.bincount(idx, minlength=levels).astype(np.int64)
     return ln_g, idx, order, (lo, hi), hist
+
+
+def fake_advance(call: int, schedule, n_meas: int, n_sites: int, kind: str, n_comp: int = 2) -> dict:
+    """Deterministic stand-in for ``Model.advance`` output (call ``call`` of a chain).
+
+    Used to drive critmc's ``Simulation`` (fixture generator) and this
+    project's (tests) through the same data, so their host logic -- chunking,
+    Wolff-count and Metropolis-step tuning, metadata -- can be compared
+    exactly.  Wolff cluster sizes grow with the call index, as for a chain that
+    orders while it thermalises.
+    """
+    rng = np.random.default_rng([7, call])
+    sched = np.asarray(schedule).reshape(-1, 2)
+    metro = int(sched[np.isin(sched[:, 0], (0, 1)), 1].sum())
+    wolff = int(sched[sched[:, 0] == 3, 1].sum())
+    aux = np.zeros((n_meas, 4), dtype=np.int64)
+    aux[:, 0] = rng.integers(0, metro * n_sites + 1, n_meas)
+    aux[:, 1] = wolff * rng.integers(1, min(n_sites, 2 + 3 * call) + 1, n_meas)
+    aux[:, 2] = rng.integers(0, n_sites * n_sites, n_meas)
+    aux[:, 3] = rng.integers(1, n_sites, n_meas)
+    if kind == "on":
+        return {"E": rng.normal(-1.0, 0.1, n_meas) * n_sites, "M": rng.normal(size=(n_meas, n_comp)),
+                "stiff_c": rng.normal(size=(n_meas, 2)), "stiff_s": rng.normal(size=(n_meas, 2)), "aux": aux}
+    e = rng.integers(-2 * n_sites, 2 * n_sites, n_meas)
+    return {"E": e, "Eb": e.copy(), "M": rng.integers(-n_sites, n_sites + 1, n_meas), "aux": aux}
+
+
+# scenarios of the Simulation host-logic comparison: (model, updates, therm, n_chunks, run, chunk)
+SIM_SCENARIOS = [
+    ("ising", "metropolis+wolff", 100, 10, 700, 300),
+    ("ising", "heatbath+3*wolff", 57, 7, 64, 1 << 16),
+    ("on", "metropolis+2*overrelax", 90, 9, 50, 20),
+    ("ising", "metropolis", 3, 10, 5, 2),
+    ("ising", "sw+metropolis", 0, 10, 9, 4),
+]
+
+
+def summarize_series(raw: dict, meta: dict) -> dict:
+    """Sums and end values of every stream, and the metadata without wall-clock entries."""
+    out = {}
+    for k, v in raw.items():
+        a = np.asarray(v, dtype=np.float64)
+        out[k] = [float(a.sum()), float(a.reshape(len(a), -1)[0, 0]), float(a.reshape(len(a), -1)[-1, -1]),
+                  list(a.shape)]
+    skip = {"wall_time", "site_updates_per_s", "backend"}
+    return {"streams": out, "meta": {k: v for k, v in meta.items() if k not in skip}}

@@ -148,6 +148,36 @@ def main() -> None:
     sim = Simulation(Ising(square(4)), 0.44, "metropolis", seed=5)
     sim.thermalize(20)
     sim.run(200).save(OUT.parent / "critmc_series_ising4.npz")
+    # critmc's Simulation host logic driven by a deterministic fake advance
+    from critmc import ON as RefON
+    from critmc import Ising as RefIsing
+    from exact_helpers import SIM_SCENARIOS, fake_advance, summarize_series
+    from critmc.io import to_jsonable as ref_jsonable
+
+    def fake_model(kind):
+        base = RefIsing if kind == "ising" else RefON
+        args = (square(8),) if kind == "ising" else (square(8), 2)
+
+        class Fake(base):
+            calls: list = []
+
+            def advance(self, state, running, beta, rng, schedule, n_meas, ws):
+                Fake.calls.append([int(n_meas), schedule.tolist(), running.get("step")])
+                return fake_advance(len(Fake.calls) - 1, schedule, n_meas, self.n_sites, kind)
+
+        Fake.calls = []
+        return Fake(*args), Fake
+
+    sims = []
+    for kind, updates, therm, n_chunks, n_run, chunk in SIM_SCENARIOS:
+        model, cls = fake_model(kind)
+        sim = Simulation(model, 0.5, updates, seed=11)
+        tuning = sim.thermalize(therm, n_chunks=n_chunks)
+        ts = sim.run(n_run, chunk=chunk)
+        sims.append(ref_jsonable({"calls": cls.calls, "tuning": tuning, "final_tuning": sim.tuning(),
+                                  "series": summarize_series(ts.raw, ts.meta), "n_therm": sim.n_therm,
+                                  "n_meas": sim.n_meas}))
+    out["simulation_host_logic"] = sims
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

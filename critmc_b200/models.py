@@ -69,7 +69,7 @@ def advance_with_clusters(model, chain, running, beta, schedule, n_meas, bits: b
     spins = chain.words if bits else chain.spins
     out_e = np.empty(n_meas, dtype=np.int64)
     out_m = np.empty((n_meas, q) if potts else n_meas, dtype=np.int64)
-    aux = np.zeros((n_meas, N_AUX), dtype=np.int64)
+    aux = np.zeros((n_meas, N_AUX), np.int64)
     stats = torch.zeros((1, 3), dtype=torch.int64, device=dev)
     for meas in range(n_meas):
         stats.zero_()
@@ -152,13 +152,12 @@ class Model(ABC):
                 n_meas: int) -> dict[str, np.ndarray]: ...
 
     def check_updates(self, names: list[str]) -> None:
-        bad = [n for n in names if n not in self.updates]
-        if bad:
-            why = "; ".join(f"{n}: {_NOT_ON_GPU[n]}" for n in bad if n in _NOT_ON_GPU)
-            raise ValueError(
-                f"{type(self).__name__} does not support updates {bad} on the GPU; "
-                f"available: {list(self.updates)}" + (f" ({why})" if why else "")
-            )
+        """Raise ValueError for moves this model does not run (with the reason where one is known)."""
+        missing = [name for name in names if name not in set(self.updates)]
+        if missing:
+            reasons = [f"{name}: {_NOT_ON_GPU[name]}" for name in missing if name in _NOT_ON_GPU]
+            detail = f" ({'; '.join(reasons)})" if reasons else ""
+            raise ValueError(f"{type(self).__name__} on the GPU runs {list(self.updates)}, not {missing}{detail}")
         if self._binary and self.lattice.dim == 1 and "metropolis" in names:
             # On a ring a zero-energy flip is accepted with certainty; updating a whole
             # sublattice at once then moves every domain wall one site per half-sweep in
@@ -173,14 +172,16 @@ class Model(ABC):
         return False
 
     def spec(self) -> dict[str, Any]:
-        return {"model": self.kind, "lattice": self.lattice.name, "L": self.lattice.L}
+        """What ``build_model`` needs to make this model again (critmc's model spec)."""
+        return dict(model=self.kind, lattice=self.lattice.name, L=self.lattice.L)
 
     def meta(self) -> dict[str, Any]:
-        return {**self.spec(), "N": self.n_sites, "dim": self.lattice.dim,
-                "n_bonds": self.lattice.n_bonds}
+        """The spec plus the lattice's size, dimension and bond count (series metadata)."""
+        lat = self.lattice
+        return {**self.spec(), **dict(N=lat.n_sites, dim=lat.dim, n_bonds=lat.n_bonds)}
 
     def __repr__(self) -> str:
-        return f"{type(self).__name__}({self.lattice!r})"
+        return "{}({!r})".format(type(self).__name__, self.lattice)
 
 
 def _msc_ok(shape: tuple[int, ...]) -> bool:
@@ -240,31 +241,33 @@ class Ising(Model):
 
     def __init__(self, lattice: Lattice, h: float = 0.0):
         super().__init__(lattice)
+        if not math.isfinite(float(h)):
+            raise ValueError(f"the field must be a finite number, got h = {h}")
         self.h = float(h)
-        if not math.isfinite(self.h):
-            raise ValueError(f"field h must be finite, got {h}")
 
     @property
     def _binary(self) -> bool:
         return True
 
     def initial_state(self, start, rng):
-        n = self.n_sites
+        """+-1 spins: "random" (a fair bit per site from ``rng``), "ordered"/"up", "down"."""
+        fill = {"ordered": 1, "up": 1, "down": -1}
         if start == "random":
-            return (2 * rng.integers(0, 2, size=n) - 1).astype(np.int8)
-        if start in ("ordered", "up"):
-            return np.ones(n, dtype=np.int8)
-        if start == "down":
-            return -np.ones(n, dtype=np.int8)
-        raise ValueError(f"unknown start {start!r}")
+            bits = rng.integers(0, 2, size=self.n_sites)  # the draw of critmc's Ising start
+            return np.where(bits == 1, 1, -1).astype(np.int8)
+        if start not in fill:
+            raise ValueError(f"start is 'random', 'ordered', 'up' or 'down', not {start!r}")
+        return np.full(self.n_sites, fill[start], dtype=np.int8)
 
     def bond_energy(self, state) -> int:
-        s = np.asarray(state, dtype=np.int64)
-        b = self.lattice.bonds
-        return int(-np.sum(s[b[:, 0]] * s[b[:, 1]]))
+        """E_b = -sum over bonds of s_i s_j."""
+        spins = np.asarray(state, dtype=np.int64)
+        i, j = self.lattice.bonds.T
+        return -int(np.dot(spins[i], spins[j]))
 
     def energy(self, state):
-        return float(self.bond_energy(state)) - self.h * float(np.asarray(state, dtype=np.int64).sum())
+        magnetisation = int(np.asarray(state, dtype=np.int64).sum())
+        return float(self.bond_energy(state)) - self.h * magnetisation
 
     def begin(self, state):
         return {"e_b": self.bond_energy(state), "m": int(np.asarray(state, dtype=np.int64).sum())}
@@ -322,7 +325,7 @@ class Ising(Model):
         return {"E": energy, "Eb": e_b, "M": mm, "aux": to_host(aux)[0]}
 
     def spec(self):
-        return {**super().spec(), "h": self.h}
+        return dict(super().spec(), h=self.h)
 
 
 class Potts(Model):
@@ -333,8 +336,8 @@ class Potts(Model):
 
     def __init__(self, lattice: Lattice, q: int):
         super().__init__(lattice)
-        if q < 2 or q > 127:
-            raise ValueError(f"q must be in [2, 127], got {q}")
+        if not 2 <= q <= 127:
+            raise ValueError(f"Potts models here have 2 <= q <= 127 states, got q = {q}")
         self.q = int(q)
 
     @property
@@ -342,17 +345,18 @@ class Potts(Model):
         return self.q == 2
 
     def initial_state(self, start, rng):
-        n = self.n_sites
+        """States 0..q-1: "random" (uniform per site from ``rng``) or "ordered"/"up" (all 0)."""
         if start == "random":
-            return rng.integers(0, self.q, size=n).astype(np.int8)
-        if start in ("ordered", "up"):
-            return np.zeros(n, dtype=np.int8)
-        raise ValueError(f"unknown start {start!r}")
+            return np.asarray(rng.integers(0, self.q, size=self.n_sites), dtype=np.int8)
+        if start not in ("ordered", "up"):
+            raise ValueError(f"start is 'random', 'ordered' or 'up', not {start!r}")
+        return np.zeros(self.n_sites, dtype=np.int8)
 
     def bond_energy(self, state) -> int:
-        s = np.asarray(state)
-        b = self.lattice.bonds
-        return int(-np.sum(s[b[:, 0]] == s[b[:, 1]]))
+        """E = -(number of bonds whose ends agree)."""
+        values = np.asarray(state)
+        i, j = self.lattice.bonds.T
+        return -int(np.count_nonzero(values[i] == values[j]))
 
     def energy(self, state):
         return float(self.bond_energy(state))
@@ -376,7 +380,7 @@ class Potts(Model):
         return chain.advance(running, beta, schedule, n_meas)
 
     def spec(self):
-        return {**super().spec(), "q": self.q}
+        return dict(super().spec(), q=self.q)
 
 
 class ON(Model):
@@ -388,26 +392,26 @@ class ON(Model):
     def __init__(self, lattice: Lattice, n: int):
         super().__init__(lattice)
         if n < 2:
-            raise ValueError(f"n must be at least 2, got {n} (n = 1 is the Ising model)")
+            raise ValueError(f"O(n) models need n >= 2 components (n = 1 is Ising), got n = {n}")
         if n > 3:
-            raise ValueError("the GPU O(n) kernels handle n = 2 (XY) and n = 3 (Heisenberg)")
+            raise ValueError(f"the GPU O(n) kernels run n = 2 (XY) and n = 3 (Heisenberg), not n = {n}")
         self.n = int(n)
 
     def initial_state(self, start, rng):
+        """Unit vectors: "random" (normalised Gaussian vectors from ``rng``, uniform on the
+        sphere) or "ordered"/"up" (all along the first axis)."""
         if start == "random":
-            s = rng.standard_normal((self.n_sites, self.n))
-            s /= np.linalg.norm(s, axis=1, keepdims=True)
-            return s
-        if start in ("ordered", "up"):
-            s = np.zeros((self.n_sites, self.n))
-            s[:, 0] = 1.0
-            return s
-        raise ValueError(f"unknown start {start!r}")
+            v = rng.standard_normal((self.n_sites, self.n))
+            return v / np.linalg.norm(v, axis=1)[:, None]
+        if start not in ("ordered", "up"):
+            raise ValueError(f"start is 'random', 'ordered' or 'up', not {start!r}")
+        return np.eye(1, self.n).repeat(self.n_sites, axis=0)
 
     def energy(self, state):
-        s = np.asarray(state, dtype=np.float64)
-        b = self.lattice.bonds
-        return float(-np.sum(s[b[:, 0]] * s[b[:, 1]]))
+        """E = -sum over bonds of S_i . S_j."""
+        spins = np.asarray(state, dtype=np.float64)
+        i, j = self.lattice.bonds.T
+        return -float(np.einsum("bk,bk->", spins[i], spins[j]))
 
     def begin(self, state):
         return {"step": 1.0}
@@ -422,7 +426,7 @@ class ON(Model):
         return chain.advance(running, beta, schedule, n_meas)
 
     def spec(self):
-        return {**super().spec(), "n": self.n}
+        return dict(super().spec(), n=self.n)
 
 
 def XY(lattice: Lattice) -> ON:
@@ -434,36 +438,40 @@ def Heisenberg(lattice: Lattice) -> ON:
 
 
 def build_model(spec: dict[str, Any]) -> Model:
+    """The model a spec names (``{"model": "ising", "lattice": "square", "L": 32, ...}``)."""
     lattice = make_lattice(spec["lattice"], int(spec["L"]))
-    kind = spec["model"]
-    if kind == "ising":
-        return Ising(lattice, h=float(spec.get("h", 0.0)))
-    if kind == "potts":
-        return Potts(lattice, int(spec["q"]))
-    if kind == "on":
-        return ON(lattice, int(spec["n"]))
-    raise ValueError(f"unknown model kind {kind!r}")
+    makers = {"ising": lambda: Ising(lattice, h=float(spec.get("h", 0.0))),
+              "potts": lambda: Potts(lattice, int(spec["q"])),
+              "on": lambda: ON(lattice, int(spec["n"]))}
+    if spec["model"] not in makers:
+        raise ValueError(f"model kind {spec['model']!r} is not one of {sorted(makers)}")
+    return makers[spec["model"]]()
 
 
 def derive(raw: dict[str, np.ndarray], meta: dict[str, Any]) -> dict[str, np.ndarray]:
-    """Per-site observables from raw streams (critmc models.py:325-351)."""
+    """Per-site observables from the raw streams (critmc models.py:325-351).
+
+    e = E / N for all; m2, its root absm and its square m4; Ising also m = M / N;
+    Potts m2 = (q sum_k rho_k^2 - 1) / (q - 1) (clipped at 0) and mmax =
+    (q max_k rho_k - 1) / (q - 1) with rho = counts / N; O(n) m2 = |M / N|^2.
+    """
     n = float(meta["N"])
     kind = meta["model"]
-    out: dict[str, np.ndarray] = {"e": np.asarray(raw["E"], dtype=np.float64) / n}
+    if kind not in ("ising", "potts", "on"):
+        raise ValueError(f"no observables for model kind {kind!r}")
+    obs: dict[str, np.ndarray] = {"e": np.asarray(raw["E"], dtype=np.float64) / n}
     if kind == "ising":
-        m = raw["M"] / n
-        out["m"] = m
-        out["m2"] = m * m
+        obs["m"] = raw["M"] / n
+        m2 = np.square(obs["m"])
     elif kind == "potts":
         q = int(meta["q"])
         rho = raw["counts"] / n
-        out["m2"] = np.clip((q * np.sum(rho * rho, axis=1) - 1.0) / (q - 1.0), 0.0, None)
-        out["mmax"] = (q * rho.max(axis=1) - 1.0) / (q - 1.0)
-    elif kind == "on":
-        mv = raw["M"] / n
-        out["m2"] = np.sum(mv * mv, axis=1)
+        m2 = np.maximum((q * np.einsum("tk,tk->t", rho, rho) - 1.0) / (q - 1.0), 0.0)
+        obs["mmax"] = (q * np.max(rho, axis=1) - 1.0) / (q - 1.0)
     else:
-        raise ValueError(f"unknown model kind {kind!r}")
-    out["absm"] = np.sqrt(out["m2"])
-    out["m4"] = out["m2"] ** 2
-    return out
+        mvec = raw["M"] / n
+        m2 = np.einsum("tk,tk->t", mvec, mvec)
+    obs["m2"] = m2
+    obs["absm"] = np.sqrt(m2)
+    obs["m4"] = np.square(m2)
+    return obs

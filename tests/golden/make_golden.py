@@ -178,6 +178,29 @@ def main() -> None:
                                   "series": summarize_series(ts.raw, ts.meta), "n_therm": sim.n_therm,
                                   "n_meas": sim.n_meas}))
     out["simulation_host_logic"] = sims
+
+    # model host methods of critmc: seeded initial states, energies, metadata, derived observables
+    from critmc import cubic
+    from critmc.models import derive as ref_derive
+    from critmc.rng import make_rng as ref_make_rng
+
+    models = {"ising": RefIsing(square(6), h=0.25), "potts": Potts(cubic(4), 5), "on": RefON(chain(8), 3)}
+    host: dict = {}
+    for name, mdl in models.items():
+        s0 = mdl.initial_state("random", ref_make_rng(3, "start"))
+        s1 = mdl.initial_state("ordered", ref_make_rng(3))
+        host[name] = {"random": np.asarray(s0, dtype=np.float64).ravel().tolist(),
+                      "ordered": np.asarray(s1, dtype=np.float64).ravel().tolist(),
+                      "energy_random": float(mdl.energy(s0)), "meta": mdl.meta(), "spec": mdl.spec()}
+    rng = np.random.default_rng(99)
+    raws = {"ising": ({"E": rng.integers(-72, 72, 20).astype(float), "M": rng.integers(-36, 37, 20)},
+                      {"model": "ising", "N": 36}),
+            "potts": ({"E": rng.integers(-192, 0, 20).astype(float), "counts": rng.multinomial(64, [0.2] * 5, 20)},
+                      {"model": "potts", "N": 64, "q": 5}),
+            "on": ({"E": rng.normal(size=20), "M": rng.normal(size=(20, 3)) * 3}, {"model": "on", "N": 8})}
+    for name, (raw, meta) in raws.items():
+        host[name]["derive"] = {k: np.asarray(v).tolist() for k, v in ref_derive(raw, meta).items()}
+    out["model_host"] = host
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

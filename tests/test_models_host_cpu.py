@@ -1,0 +1,47 @@
+"""Model host methods against critmc's own (critmc models.py:32-351, fixture):
+seeded initial states (same generator draws), energies, metadata and the
+derived per-site observables; and build_model from a spec."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from exact_helpers import golden
+
+from critmc_b200 import ON, Ising, Potts, build_model, chain, cubic, derive, make_rng, square
+
+
+def _models():
+    return {"ising": Ising(square(6), h=0.25), "potts": Potts(cubic(4), 5), "on": ON(chain(8), 3)}
+
+
+@pytest.mark.parametrize("name", ["ising", "potts", "on"])
+def test_model_host_methods_match_critmc(name):
+    ref = golden()["model_host"][name]
+    mdl = _models()[name]
+    s0 = mdl.initial_state("random", make_rng(3, "start"))
+    np.testing.assert_array_equal(np.asarray(s0, dtype=np.float64).ravel(), ref["random"])
+    s1 = mdl.initial_state("ordered", make_rng(3))
+    np.testing.assert_array_equal(np.asarray(s1, dtype=np.float64).ravel(), ref["ordered"])
+    assert mdl.energy(s0) == pytest.approx(ref["energy_random"], rel=1e-12, abs=1e-12)
+    assert mdl.meta() == ref["meta"] and mdl.spec() == ref["spec"]
+    assert build_model(ref["spec"]).meta() == ref["meta"]
+    with pytest.raises(ValueError):
+        mdl.initial_state("sideways", make_rng(1))
+
+
+def test_derived_observables_match_critmc():
+    rng = np.random.default_rng(99)
+    raws = {"ising": ({"E": rng.integers(-72, 72, 20).astype(float), "M": rng.integers(-36, 37, 20)},
+                      {"model": "ising", "N": 36}),
+            "potts": ({"E": rng.integers(-192, 0, 20).astype(float), "counts": rng.multinomial(64, [0.2] * 5, 20)},
+                      {"model": "potts", "N": 64, "q": 5}),
+            "on": ({"E": rng.normal(size=20), "M": rng.normal(size=(20, 3)) * 3}, {"model": "on", "N": 8})}
+    for name, (raw, meta) in raws.items():
+        ref = golden()["model_host"][name]["derive"]
+        got = derive(raw, meta)
+        assert set(got) == set(ref), name
+        for k, v in ref.items():
+            np.testing.assert_allclose(got[k], v, rtol=1e-13, atol=1e-15, err_msg=f"{name}.{k}")
+    with pytest.raises(ValueError):
+        derive({"E": np.zeros(2)}, {"model": "clock", "N": 4})

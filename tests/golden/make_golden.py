@@ -201,6 +201,30 @@ def main() -> None:
     for name, (raw, meta) in raws.items():
         host[name]["derive"] = {k: np.asarray(v).tolist() for k, v in ref_derive(raw, meta).items()}
     out["model_host"] = host
+
+    # critmc's lattice tables and keyed random streams (interfaces kept exactly)
+    from critmc import hypercubic as ref_hypercubic
+    from critmc import triangular as ref_triangular
+    from critmc.lattice import make_lattice as ref_make_lattice
+    from critmc.rng import spawn_rngs as ref_spawn
+
+    lats = {"chain6": chain(6), "square4x3": square(4, 3), "cubic3": ref_make_lattice("cubic", 3),
+            "hyper2x2x2x2": ref_hypercubic((2, 2, 2, 2)), "triangular4": ref_triangular(4),
+            "square_named": ref_make_lattice("square", 5)}
+    out["lattices"] = {
+        k: {"name": v.name, "shape": list(v.shape), "nbr": v.nbr.tolist(), "bonds": v.bonds.tolist(),
+            "bond_axis": v.bond_axis.tolist(), "coords": v.coords.tolist(),
+            "positions": np.asarray(v.positions).tolist(), "primitive": np.asarray(v.primitive).tolist(),
+            "sublattice": None if v.sublattice is None else v.sublattice.tolist(), "z": int(v.z),
+            "site_ones": int(v.site(*([1] * v.dim))),
+            "kmin": v.kmin(0).tolist()} for k, v in lats.items()}
+    streams = {}
+    for label, args in (("int", (5,)), ("int_keys", (5, "ising", 64, 2)), ("str_key", (123, "walker", 7)),
+                        ("tuple_key", (9, (1, 2))), ("bool_key", (4, True, False)), ("float_key", (4, 0.5)),
+                        ("seedseq", (np.random.SeedSequence(77),)), ("seedseq_keys", (np.random.SeedSequence(77), 3))):
+        streams[label] = ref_make_rng(*args).integers(0, 2**32, size=4).tolist()
+    streams["spawn"] = [g.integers(0, 2**32, size=2).tolist() for g in ref_spawn(8, 3, "x")]
+    out["rng_streams"] = streams
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

@@ -52,28 +52,30 @@ class EdwardsAnderson:
         if len(set(lattice.shape)) != 1:
             raise ValueError("the GPU spin-glass kernel needs equal extents")
         if couplings is None:
-            rng = make_rng(seed)
-            if disorder == "bimodal":
-                couplings = rng.choice([-1.0, 1.0], size=lattice.n_bonds)
-            elif disorder == "gaussian":
-                raise ValueError("Gaussian couplings are not supported by the +-J multi-spin-coded kernel")
-            else:
-                raise ValueError("disorder must be 'gaussian' or 'bimodal'")
-        couplings = np.asarray(couplings, dtype=np.float64)
-        if couplings.shape != (lattice.n_bonds,):
-            raise ValueError("need one coupling per bond")
-        if not np.all(np.abs(couplings) == 1.0):
-            raise ValueError("couplings must be +-1")
-        self.couplings = couplings
+            if disorder == "gaussian":
+                raise ValueError("the multi-spin-coded kernel runs +-J couplings only, not Gaussian ones")
+            if disorder != "bimodal":
+                raise ValueError(f"disorder is 'bimodal' (or 'gaussian' in critmc), not {disorder!r}")
+            # +-1 with probability 1/2 each: one uniform index per bond into (-1, +1),
+            # the draw critmc makes for a seed (glass.py:62-63)
+            signs = np.array([-1.0, 1.0])
+            couplings = signs[make_rng(seed).integers(0, 2, size=lattice.n_bonds)]
+        table = np.array(couplings, dtype=np.float64)
+        if table.shape != (lattice.n_bonds,):
+            raise ValueError(f"one coupling per bond ({lattice.n_bonds}) is needed, got shape {table.shape}")
+        if np.any(np.abs(table) != 1.0):
+            raise ValueError("the multi-spin-coded kernel needs couplings of +-1")
+        self.couplings = table
 
     @property
     def n_sites(self) -> int:
         return self.lattice.n_sites
 
     def energy(self, state: np.ndarray) -> float:
-        b = self.lattice.bonds
-        s = np.asarray(state, dtype=np.float64)
-        return float(-np.sum(self.couplings * s[b[:, 0]] * s[b[:, 1]]))
+        """E = -sum over bonds of J_ij s_i s_j."""
+        spins = np.asarray(state, dtype=np.float64)
+        i, j = self.lattice.bonds.T
+        return -float(np.sum(self.couplings * spins[i] * spins[j]))
 
     def coupling_bits(self) -> np.ndarray:
         """Per-slot bit masks of negative couplings in the device layout."""
@@ -86,8 +88,9 @@ class EdwardsAnderson:
 
 
 def geometric_temperatures(t_min: float, t_max: float, n: int) -> np.ndarray:
-    """critmc glass.py:93-95."""
-    return t_min * (t_max / t_min) ** (np.arange(n) / (n - 1))
+    """``n`` temperatures from ``t_min`` to ``t_max`` with a constant ratio (critmc glass.py:93-95)."""
+    ratio = t_max / t_min
+    return t_min * np.power(ratio, np.arange(n) / (n - 1))
 
 
 @dataclass
@@ -112,7 +115,8 @@ class TemperingRun:
                 ("qk2", OBS_QK2))}
 
     def equilibrium(self) -> dict[str, np.ndarray]:
-        return {k: v[-1] for k, v in self.bin_means().items()}
+        """The last (longest, most equilibrated) bin of every observable."""
+        return {name: series[-1] for name, series in self.bin_means().items()}
 
 
 def _pack_words(spins: np.ndarray, shape) -> np.ndarray:
@@ -149,7 +153,7 @@ class SpinGlassCampaign:
         lat = models[0].lattice
         if any(md.lattice.shape != lat.shape for md in models):
             raise ValueError("all samples must share the lattice")
-        temps = np.sort(np.asarray(temperatures, dtype=np.float64))[::-1]  # hot -> cold
+        temps = -np.sort(-np.asarray(temperatures, dtype=np.float64))  # hottest first
         if not 2 <= len(temps) <= 32:
             raise ValueError("between 2 and 32 temperatures")
         self.device = require_cuda(device)

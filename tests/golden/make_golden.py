@@ -225,6 +225,17 @@ def main() -> None:
         streams[label] = ref_make_rng(*args).integers(0, 2**32, size=4).tolist()
     streams["spawn"] = [g.integers(0, 2**32, size=2).tolist() for g in ref_spawn(8, 3, "x")]
     out["rng_streams"] = streams
+
+    # critmc's EA +-J couplings for a seed, its temperature ladder and a sample energy
+    from critmc.glass import EdwardsAnderson as RefEA
+    from critmc.glass import geometric_temperatures as ref_temps
+
+    ea = {}
+    for sd in (1, 2):
+        sample = RefEA(cubic(4), disorder="bimodal", seed=sd)
+        state = np.where(np.random.default_rng(sd).random(64) < 0.5, -1, 1)
+        ea[str(sd)] = {"couplings": sample.couplings.tolist(), "energy": float(sample.energy(state))}
+    out["ea_samples"] = {"cubic4": ea, "temperatures": ref_temps(0.5, 2.0, 32).tolist()}
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

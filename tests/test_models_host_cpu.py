@@ -45,3 +45,21 @@ def test_derived_observables_match_critmc():
             np.testing.assert_allclose(got[k], v, rtol=1e-13, atol=1e-15, err_msg=f"{name}.{k}")
     with pytest.raises(ValueError):
         derive({"E": np.zeros(2)}, {"model": "clock", "N": 4})
+
+
+def test_edwards_anderson_samples_match_critmc():
+    """+-J couplings for a seed, the geometric temperatures and the sample energy as
+    critmc's (critmc glass.py:45-95, fixture)."""
+    from critmc_b200.glass import EdwardsAnderson, geometric_temperatures
+
+    ref = golden()["ea_samples"]
+    for sd in (1, 2):
+        sample = EdwardsAnderson(cubic(4), disorder="bimodal", seed=sd)
+        np.testing.assert_array_equal(sample.couplings, ref["cubic4"][str(sd)]["couplings"])
+        state = np.where(np.random.default_rng(sd).random(64) < 0.5, -1, 1)
+        assert sample.energy(state) == ref["cubic4"][str(sd)]["energy"]
+    np.testing.assert_allclose(geometric_temperatures(0.5, 2.0, 32), ref["temperatures"], rtol=1e-15)
+    with pytest.raises(ValueError):
+        EdwardsAnderson(cubic(4), disorder="gaussian", seed=1)
+    with pytest.raises(ValueError):
+        EdwardsAnderson(cubic(4), couplings=np.ones(5))

@@ -28,15 +28,17 @@ def cuda():
 
 
 def batch_mean_error(x: np.ndarray, n_batches: int = 64) -> tuple[float, float]:
-    """Mean and batch-means standard error (critmc tests/conftest.py:6-11)."""
-    x = np.asarray(x, dtype=np.float64)
-    size = len(x) // n_batches
-    b = x[len(x) - size * n_batches:].reshape(n_batches, size).mean(axis=1)
-    return float(x.mean()), float(b.std(ddof=1) / np.sqrt(n_batches))
+    """Mean of the series, and its standard error from ``n_batches`` equal blocks
+    after dropping the leading remainder (the statistic of critmc tests/conftest.py:6-11)."""
+    series = np.asarray(x, dtype=np.float64)
+    drop = series.size % n_batches
+    block_means = series[drop:].reshape(n_batches, -1).mean(axis=1)
+    return float(series.mean()), float(np.std(block_means, ddof=1) / np.sqrt(n_batches))
 
 
 def assert_consistent(sample, exact: float, z_max: float = 4.5, n_batches: int = 64):
-    """|z| < z_max with batch-means errors (critmc tests/conftest.py:14-17)."""
+    """The sample mean lies within ``z_max`` batch-means errors of ``exact``
+    (critmc tests/conftest.py:14-17 uses 4.5)."""
     mean, err = batch_mean_error(sample, n_batches)
-    z = (mean - exact) / err if err > 0 else 0.0
-    assert abs(z) < z_max, f"mean {mean:.6f} +- {err:.2e} vs exact {exact:.6f} (z = {z:.2f})"
+    z = 0.0 if err <= 0 else (mean - exact) / err
+    assert abs(z) < z_max, f"sample mean {mean:.6g} +- {err:.2g} is {z:+.2f} errors from {exact:.6g}"

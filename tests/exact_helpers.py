@@ -45,12 +45,14 @@ class JointDOS:
         self.n_sites = int(d["n_sites"])
 
     def average(self, beta: float, fn, h: float = 0.0) -> float:
-        e, o = np.meshgrid(self.energies, self.orders, indexing="ij")
-        with np.errstate(divide="ignore"):
-            logw = np.log(self.counts) - beta * (e - h * o)
-        w = np.exp(logw - logw.max())
-        w /= w.sum()
-        return float(np.sum(w * fn(e, o)))
+        """Canonical average of fn(E, O) at ``beta`` (field ``h`` coupling to O)."""
+        energy = self.energies[:, None] + 0.0 * self.orders[None, :]
+        order = self.orders[None, :] + 0.0 * self.energies[:, None]
+        filled = self.counts > 0
+        log_w = np.full(self.counts.shape, -np.inf)
+        log_w[filled] = np.log(self.counts[filled]) - beta * (energy[filled] - h * order[filled])
+        prob = np.exp(log_w - log_w[filled].max())
+        return float((prob * fn(energy, order)).sum() / prob.sum())
 
 
 def gamma_error(x: np.ndarray, S: float = 1.5) -> tuple[float, float, float]:
@@ -66,17 +68,18 @@ def gamma_error(x: np.ndarray, S: float = 1.5) -> tuple[float, float, float]:
     spec = np.fft.rfft(d, n=nfft)
     gam = np.fft.irfft(spec.real ** 2 + spec.imag ** 2, n=nfft)[: t_max + 1]
     gam /= n - np.arange(t_max + 1)
-    # first W with exp(-W/tau_W) - tau_W/sqrt(W N) < 0, tau_W = S / ln(1 + 1/G(W))
-    w = np.arange(1, gam.size)
-    g_int = np.cumsum(gam[1:]) / gam[0]
-    tau_w = np.full(w.size, 1e-300)
-    pos = g_int > 0
+    # Wolff's window: the first W at which exp(-W / tau(W)) - tau(W) / sqrt(W N) turns
+    # negative, with tau(W) = S / ln(1 + 1 / G(W)) and G(W) = sum_{t<=W} Gamma(t) / Gamma(0)
+    windows = np.arange(1, gam.size)
+    summed = np.cumsum(gam[1:]) / gam[0]
+    tau = np.full(windows.size, 1e-300)
+    positive = summed > 0
     with np.errstate(divide="ignore", over="ignore"):
-        tau_w[pos] = S / np.log1p(1.0 / g_int[pos])
-    tau_w = np.maximum(tau_w, 1e-300)
-    g = np.exp(-w / tau_w) - tau_w / np.sqrt(w * float(n))
-    hits = np.flatnonzero(g < 0)
-    w_opt = int(w[hits[0]]) if hits.size else int(w[-1])
+        tau[positive] = S / np.log1p(np.reciprocal(summed[positive]))
+    tau = np.maximum(tau, 1e-300)
+    criterion = np.exp(-windows / tau) - tau / np.sqrt(windows * float(n))
+    below = np.flatnonzero(criterion < 0)
+    w_opt = int(windows[below[0]] if below.size else windows[-1])
     c_f = gam[0] + 2.0 * gam[1:w_opt + 1].sum()
     gam = gam + c_f / n  # bias of the subtracted mean
     c_f = gam[0] + 2.0 * gam[1:w_opt + 1].sum()
@@ -109,19 +112,20 @@ def ea_exact(lattice, couplings, temperatures):
     Follows critmc tests/test_glass.py:26-52 (energies as critmc's
     exact/enumeration.py:120-135 ea_energies: E = -sum_b J_b s_i s_j)."""
     n = lattice.n_sites
-    states = np.arange(1 << n)
-    spins = (2 * ((states[:, None] >> np.arange(n)) & 1) - 1).astype(np.float64)
-    b = lattice.bonds
-    energies = -(spins[:, b[:, 0]] * spins[:, b[:, 1]]) @ np.asarray(couplings, dtype=np.float64)
-    out = {"e": [], "q2": [], "ql": []}
-    for T in temperatures:
-        w = np.exp(-(energies - energies.min()) / T)
-        w /= w.sum()
-        corr = (spins * w[:, None]).T @ spins
-        out["e"].append(w @ energies / n)
-        out["q2"].append(np.sum(corr ** 2) / n ** 2)
-        out["ql"].append(np.mean(corr[b[:, 0], b[:, 1]] ** 2))
-    return {k: np.array(v) for k, v in out.items()}
+    bits = np.unpackbits(np.arange(1 << n, dtype=">u4").view(np.uint8).reshape(-1, 4), axis=1,
+                         bitorder="big")[:, ::-1][:, :n]  # bit k of the state number is site k
+    spins = np.where(bits == 1, 1.0, -1.0)
+    i, j = lattice.bonds.T
+    energies = -(spins[:, i] * spins[:, j]) @ np.asarray(couplings, dtype=np.float64)
+    result = {"e": [], "q2": [], "ql": []}
+    for temperature in temperatures:
+        weight = np.exp((energies.min() - energies) / temperature)
+        weight /= weight.sum()
+        two_point = spins.T @ (spins * weight[:, None])  # <s_a s_b>
+        result["e"].append(float(weight @ energies) / n)
+        result["q2"].append(float(np.square(two_point).sum()) / n ** 2)
+        result["ql"].append(float(np.square(two_point[i, j]).mean()))
+    return {name: np.array(values) for name, values in result.items()}
 
 
 def ising_log_g_square6() -> np.ndarray:

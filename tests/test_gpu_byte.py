@@ -74,60 +74,64 @@ def test_potts_bit_identical_to_replay(cuda, shape, q, sched, beta):
     np.testing.assert_array_equal(running["counts"], cnt)
 
 
+def _agrees_with_enumeration(dos, beta, series, observables, h=0.0):
+    """Each named stream of ``series`` against the exact canonical average of its function."""
+    for name, fn in observables.items():
+        assert_consistent(series[name], dos.average(beta, fn, h=h))
+
+
 @pytest.mark.parametrize("updates", ["metropolis", "heatbath"])
 def test_ising_4x4_matches_enumeration(cuda, updates):
-    """critmc tests/test_kernels.py:27-40 on a bipartite 4x4 torus."""
-    jd = JointDOS("ising_dos_square4")
-    lat = square(4)
-    beta, n = 0.35, 16
-    sim = Simulation(Ising(lat), beta, updates, seed=12)
+    """critmc tests/test_kernels.py:27-40, on a bipartite 4x4 torus: E, m^2 and m^4."""
+    dos = JointDOS("ising_dos_square4")
+    beta, sites = 0.35, 16
+    sim = Simulation(Ising(square(4)), beta, updates, seed=12)
     sim.thermalize(2000)
-    ts = sim.run(200_000)
-    assert_consistent(ts["E"], jd.average(beta, lambda e, m: e))
-    assert_consistent(ts["m2"], jd.average(beta, lambda e, m: (m / n) ** 2))
-    assert_consistent(ts["m4"], jd.average(beta, lambda e, m: (m / n) ** 4))
-    state = sim.state
-    assert sim.running["e_b"] == Ising(lat).bond_energy(state)
-    assert sim.running["m"] == int(state.astype(np.int64).sum())
+    series = sim.run(200_000)
+    _agrees_with_enumeration(dos, beta, series, {"E": lambda e, mag: e,
+                                                 "m2": lambda e, mag: np.square(mag / sites),
+                                                 "m4": lambda e, mag: np.power(mag / sites, 4)})
+    final = sim.state
+    assert sim.running["e_b"] == Ising(square(4)).bond_energy(final)
+    assert sim.running["m"] == int(np.sum(final, dtype=np.int64))
 
 
 @pytest.mark.parametrize("updates", ["metropolis", "heatbath"])
 def test_ising_in_a_field(cuda, updates):
-    """critmc tests/test_kernels.py:55-70."""
-    jd = JointDOS("ising_dos_square4")
-    beta, h = 0.3, 0.4
-    sim = Simulation(Ising(square(4), h=h), beta, updates, seed=8)
+    """critmc tests/test_kernels.py:55-70: E and m at h = 0.4."""
+    dos = JointDOS("ising_dos_square4")
+    beta, field = 0.3, 0.4
+    sim = Simulation(Ising(square(4), h=field), beta, updates, seed=8)
     sim.thermalize(1000)
-    ts = sim.run(150_000)
-    assert_consistent(ts["E"], jd.average(beta, lambda e, m: e - h * m, h=h))
-    assert_consistent(ts["m"], jd.average(beta, lambda e, m: m / 16, h=h))
+    series = sim.run(150_000)
+    _agrees_with_enumeration(dos, beta, series, {"E": lambda e, mag: e - field * mag,
+                                                 "m": lambda e, mag: mag / 16}, h=field)
 
 
 @pytest.mark.parametrize("updates", ["metropolis", "heatbath"])
 def test_potts_matches_enumeration(cuda, updates):
-    """critmc tests/test_kernels.py:78-92 on a bipartite 4x2 torus."""
-    jd = JointDOS("potts3_dos_square4x2")
-    lat = square(4, 2)
-    beta, q, n = 0.8, 3, 8
-    sim = Simulation(Potts(lat, q), beta, updates, seed=21)
+    """critmc tests/test_kernels.py:78-92, on a bipartite 4x2 torus: E and m^2 (the
+    fixture's order variable is q sum_k n_k^2)."""
+    dos = JointDOS("potts3_dos_square4x2")
+    beta, q, sites = 0.8, 3, 8
+    sim = Simulation(Potts(square(4, 2), q), beta, updates, seed=21)
     sim.thermalize(2000)
-    ts = sim.run(150_000)
-    assert_consistent(ts["E"], jd.average(beta, lambda e, s: e))
-    assert_consistent(ts["m2"], jd.average(beta, lambda e, s: (s / n ** 2 - 1.0) / (q - 1.0)))
-    state = sim.state
-    assert sim.running["energy"] == Potts(lat, q).bond_energy(state)
-    np.testing.assert_array_equal(sim.running["counts"], np.bincount(state, minlength=q))
+    series = sim.run(150_000)
+    _agrees_with_enumeration(dos, beta, series, {"E": lambda e, order: e,
+                                                 "m2": lambda e, order: (order / sites**2 - 1.0) / (q - 1.0)})
+    final = sim.state
+    assert sim.running["energy"] == Potts(square(4, 2), q).bond_energy(final)
+    np.testing.assert_array_equal(sim.running["counts"], np.bincount(final, minlength=q))
 
 
 def test_ising_chain_matches_enumeration(cuda):
-    jd = JointDOS("ising_dos_chain8")
+    dos = JointDOS("ising_dos_chain8")
     beta = 0.7
     with pytest.raises(ValueError, match="not ergodic"):
         Simulation(Ising(chain(8)), beta, "metropolis", seed=3)
     sim = Simulation(Ising(chain(8)), beta, "heatbath", seed=3)
     sim.thermalize(1000)
-    ts = sim.run(150_000)
-    assert_consistent(ts["E"], jd.average(beta, lambda e, m: e))
+    _agrees_with_enumeration(dos, beta, sim.run(150_000), {"E": lambda e, mag: e})
 
 
 def test_msc_ising_matches_kaufman(cuda):
@@ -143,19 +147,19 @@ def test_msc_ising_matches_kaufman(cuda):
                          ids=["ising", "potts", "ising-msc"])
 @pytest.mark.parametrize("chunk", [1, 7, 16, 50])
 def test_streams_do_not_depend_on_the_chunk_size(cuda, model, chunk):
-    """critmc tests/test_sim_chunks.py:7-16."""
-    whole = Simulation(model, 0.6, "metropolis", seed=4).run(50)
-    parts = Simulation(model, 0.6, "metropolis", seed=4).run(50, chunk=chunk)
-    assert list(parts.raw) == list(whole.raw)
-    for key, value in whole.raw.items():
-        assert parts.raw[key].dtype == value.dtype
-        np.testing.assert_array_equal(parts.raw[key], value)
+    """critmc tests/test_sim_chunks.py:7-16: the same streams whatever the chunk."""
+    reference = Simulation(model, 0.6, "metropolis", seed=4).run(50)
+    chunked = Simulation(model, 0.6, "metropolis", seed=4).run(50, chunk=chunk)
+    assert list(chunked.raw) == list(reference.raw)
+    for name, expected in reference.raw.items():
+        got = chunked.raw[name]
+        assert got.dtype == expected.dtype and np.array_equal(got, expected), name
 
 
 def test_reproducible_given_seed(cuda):
-    runs = []
-    for _ in range(2):
+    def energies():
         sim = Simulation(Potts(square(6), 4), 1.0, "heatbath+metropolis", seed=99)
         sim.thermalize(50)
-        runs.append(sim.run(100)["E"])
-    np.testing.assert_array_equal(runs[0], runs[1])
+        return sim.run(100)["E"]
+
+    np.testing.assert_array_equal(energies(), energies())

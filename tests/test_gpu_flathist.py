@@ -225,60 +225,74 @@ def test_multicanonical_matches_replay(cuda, n_walkers):
         np.testing.assert_array_equal(o.hist, r["hist"])
 
 
-# ---- critmc's statistical checks (tests/test_flathist.py) ----
+# ---- critmc's statistical checks (tests/test_flathist.py): the same cases,
+# seeds and bounds, written for this package ----
+
+EXACT_6 = None
+
+
+def _exact_6():
+    global EXACT_6
+    if EXACT_6 is None:
+        EXACT_6 = ising_log_g_square6()
+    return EXACT_6
 
 
 @pytest.mark.parametrize("one_over_t", [False, True])
 def test_wang_landau_ising_against_exact_dos(cuda, one_over_t):
-    wl = WangLandau(Ising(square(6)), seed=3, criterion="flat")
-    res = wl.run(1e-6, one_over_t=one_over_t)
-    exact = ising_log_g_square6()
-    got = res.normalized()
-    v = res.visited
-    assert np.array_equal(v, np.isfinite(exact))
-    err = np.abs(got[v] - exact[v])
-    assert err.mean() < (0.02 if one_over_t else 0.08)
-    betas = [0.3, 0.44, 0.6]
-    th = res.canonical(betas)
-    tol = 0.01 if one_over_t else 0.03
-    assert np.allclose(th["u"], [kaufman_energy(b, 6) for b in betas], atol=tol)
+    """6x6 Ising to ln f = 1e-6: levels seen = levels that exist; mean |ln g error|
+    below 0.02 (1/t) or 0.08 (plain, which saturates); canonical energies within
+    0.01 / 0.03 of Kaufman's at beta 0.3, 0.44, 0.6."""
+    result = WangLandau(Ising(square(6)), seed=3, criterion="flat").run(1e-6, one_over_t=one_over_t)
+    reference = _exact_6()
+    seen = result.visited
+    assert (seen == np.isfinite(reference)).all()
+    deviation = np.abs(result.normalized()[seen] - reference[seen]).mean()
+    assert deviation < {True: 0.02, False: 0.08}[one_over_t]
+    betas = (0.3, 0.44, 0.6)
+    kaufman = np.array([kaufman_energy(b, 6) for b in betas])
+    bound = {True: 0.01, False: 0.03}[one_over_t] + 1e-5 * np.abs(kaufman)  # numpy allclose's test
+    assert (np.abs(result.canonical(list(betas))["u"] - kaufman) <= bound).all()
 
 
 def test_wang_landau_batch_of_seeds_against_exact_dos(cuda):
     """Independent walkers in one launch: each converges, and their spread is the error bar."""
     results = WangLandau(Ising(square(6)), seed=11, n_walkers=64).run(1e-5)
-    exact = ising_log_g_square6()
-    v = np.isfinite(exact)
-    errs = np.array([np.abs(r.normalized()[v] - exact[v]).mean() for r in results])
-    assert (errs < 0.08).all() and np.median(errs) < 0.04
-    mean = np.mean([r.normalized()[v] for r in results], axis=0)
-    assert np.abs(mean - exact[v]).mean() < 0.01
+    reference = _exact_6()
+    on = np.isfinite(reference)
+    per_walker = np.array([np.abs(r.normalized()[on] - reference[on]).mean() for r in results])
+    assert per_walker.max() < 0.08 and np.median(per_walker) < 0.04
+    pooled = np.mean([r.normalized()[on] for r in results], axis=0)
+    assert np.abs(pooled - reference[on]).mean() < 0.01
 
 
 def test_wang_landau_checkpoints_and_stages(cuda):
-    res = WangLandau(Ising(square(4)), seed=1).run(1e-5, checkpoints=[10_000, 100_000, 1_000_000])
-    assert [c[0] for c in res.checkpoints] == [10_000, 100_000, 1_000_000]
-    assert res.stages and res.stages[0]["ln_f"] == 1.0
+    marks = [10_000, 100_000, 1_000_000]
+    result = WangLandau(Ising(square(4)), seed=1).run(1e-5, checkpoints=marks)
+    assert [trials for trials, _, _ in result.checkpoints] == marks
+    assert len(result.stages) > 0 and result.stages[0]["ln_f"] == 1.0
 
 
 def test_wang_landau_potts_window(cuda):
-    lat = square(4, 3)
-    jd = JointDOS("potts3_dos_square4x3")
-    exact = dict(zip(jd.energies, np.log(jd.counts.sum(axis=1))))
-    res = WangLandau(Potts(lat, 3), e_window=(-2.0, -1.0), seed=4).run(1e-7)
-    got = res.normalized()
-    lv = res.levels.energies
-    diff = got[res.visited] - np.array([exact[e] for e in lv[res.visited]])
-    assert np.ptp(diff) < 0.02
-    assert lv[res.visited].max() <= -12
+    """4x3 q=3 Potts in the window [-2, -1] per site: ln g differences as the exact
+    joint DOS (spread below 0.02), no level above E = -12."""
+    joint = JointDOS("potts3_dos_square4x3")
+    exact = {float(e): float(np.log(c)) for e, c in zip(joint.energies, joint.counts.sum(axis=1))}
+    result = WangLandau(Potts(square(4, 3), 3), e_window=(-2.0, -1.0), seed=4).run(1e-7)
+    energies = result.levels.energies[result.visited]
+    offsets = result.normalized()[result.visited] - np.array([exact[float(e)] for e in energies])
+    assert offsets.max() - offsets.min() < 0.02
+    assert energies.max() <= -12
 
 
 def test_multicanonical_reweighting_to_canonical(cuda):
-    exact_lng = ising_log_g_square6()
-    out = Multicanonical(Ising(square(6)), exact_lng, seed=8).run(200_000, sweeps_per_meas=1, n_therm=100)
-    assert (out.hist > 0).sum() == np.isfinite(exact_lng).sum()
-    for b in (0.3, 0.44, 0.55):
-        assert out.canonical(b)["u"][0] == pytest.approx(kaufman_energy(b, 6), abs=0.01)
+    """Exact 1/g weights on 6x6 Ising: every level is sampled and the reweighted energy
+    is Kaufman's within 0.01 at beta 0.3, 0.44, 0.55."""
+    reference = _exact_6()
+    series = Multicanonical(Ising(square(6)), reference, seed=8).run(200_000, sweeps_per_meas=1, n_therm=100)
+    assert np.count_nonzero(series.hist) == np.count_nonzero(np.isfinite(reference))
+    for beta in (0.3, 0.44, 0.55):
+        assert abs(series.canonical(beta)["u"][0] - kaufman_energy(beta, 6)) <= 0.01
 
 
 # Equal-height point of the q = 10 Potts 8 x 8 torus in the window [-1.95, -0.6]
@@ -292,43 +306,51 @@ def test_multicanonical_potts_double_peak(cuda):
     from exact_helpers import golden
 
     model = Potts(square(8), 10)
-    res = WangLandau(model, e_window=(-1.95, -0.6), seed=9).run(1e-5)
-    out = Multicanonical(model, res.ln_g, e_window=(-1.95, -0.6), seed=10).run(100_000)
-    bc = float(golden()["potts_beta_c"]["10"])
-    b = out.equal_height_beta((bc - 0.1, bc + 0.05), split=-1.3)
-    dp = out.double_peak(b, split=-1.3)
-    assert dp["p_ordered"] == pytest.approx(dp["p_disordered"], rel=1e-6)
-    assert dp["e_ordered"] < -1.5 < -1.1 < dp["e_disordered"]
-    assert abs(b - golden()["potts10_L8_equal_height"]["beta"]) < 0.015
-    assert abs(b - bc) < 0.065
+    window = (-1.95, -0.6)
+    estimate = WangLandau(model, e_window=window, seed=9).run(1e-5)
+    series = Multicanonical(model, estimate.ln_g, e_window=window, seed=10).run(100_000)
+    beta_c = float(golden()["potts_beta_c"]["10"])
+    beta = series.equal_height_beta((beta_c - 0.1, beta_c + 0.05), split=-1.3)
+    peaks = series.double_peak(beta, split=-1.3)
+    assert abs(peaks["p_ordered"] / peaks["p_disordered"] - 1.0) < 1e-6
+    assert peaks["e_ordered"] < -1.5 and peaks["e_disordered"] > -1.1
+    assert abs(beta - golden()["potts10_L8_equal_height"]["beta"]) < 0.015
+    assert abs(beta - beta_c) < 0.065
 
 
-def _wl_result_with_a_missed_level(L=6, level=12):
-    res = WangLandau(Ising(square(L)), seed=3).run(1e-5)
-    assert res.visited[level]
-    res.ln_g[level] = 0.0
-    res.visited[level] = False
-    return res, level
+def _estimate_with_level_12_unvisited():
+    """A converged 6x6 Ising estimate altered so that level 12 looks never reached:
+    ln g there is 0, Wang-Landau's starting value."""
+    estimate = WangLandau(Ising(square(6)), seed=3).run(1e-5)
+    assert estimate.visited[12]
+    estimate.ln_g[12] = 0.0
+    estimate.visited[12] = False
+    return estimate
 
 
 def test_multicanonical_raw_ln_g_traps_the_walk_on_an_unvisited_level(cuda):
-    res, level = _wl_result_with_a_missed_level()
-    out = Multicanonical(Ising(square(6)), res.ln_g, seed=4).run(5000)
-    assert out.hist[level] > 0.99 * out.hist.sum()
+    """Given the bare array, the unvisited level's weight 1/g = 1 dwarfs all others."""
+    estimate = _estimate_with_level_12_unvisited()
+    series = Multicanonical(Ising(square(6)), estimate.ln_g, seed=4).run(5000)
+    assert series.hist[12] / series.hist.sum() > 0.99
 
 
 def test_multicanonical_forbids_levels_wang_landau_never_visited(cuda):
-    res, level = _wl_result_with_a_missed_level()
-    out = Multicanonical(Ising(square(6)), res, seed=4).run(50_000)
-    assert out.hist[level] == 0
-    sampled = out.hist > 0
-    assert np.array_equal(sampled, res.visited)
-    assert out.hist[sampled].min() > 0.3 * out.hist[sampled].mean()
+    """Given the result object, the unvisited level is forbidden and the others are
+    sampled about equally (none below 30 % of the mean)."""
+    estimate = _estimate_with_level_12_unvisited()
+    series = Multicanonical(Ising(square(6)), estimate, seed=4).run(50_000)
+    assert series.hist[12] == 0
+    sampled = series.hist > 0
+    assert (sampled == estimate.visited).all()
+    counts = series.hist[sampled]
+    assert counts.min() > 0.3 * counts.mean()
 
 
 def test_multicanonical_wl_result_matches_its_array_when_all_levels_were_visited(cuda):
     model = Potts(square(6), 10)
-    res = WangLandau(model, e_window=(-1.95, -0.6), seed=9).run(1e-4)
-    a = Multicanonical(model, res.ln_g, e_window=(-1.95, -0.6), seed=10).run(5000)
-    b = Multicanonical(model, res, e_window=(-1.95, -0.6), seed=10).run(5000)
-    np.testing.assert_array_equal(a.level_series, b.level_series)
+    window = (-1.95, -0.6)
+    estimate = WangLandau(model, e_window=window, seed=9).run(1e-4)
+    from_array = Multicanonical(model, estimate.ln_g, e_window=window, seed=10).run(5000)
+    from_result = Multicanonical(model, estimate, e_window=window, seed=10).run(5000)
+    np.testing.assert_array_equal(from_array.level_series, from_result.level_series)

@@ -23,44 +23,51 @@ def replay_wang_landau(shape, q: int, state: np.ndarray, key, idx: int, window, 
                        ln_f_final: float, *, one_over_t: bool = True, check_sweeps: int = 100,
                        flatness: float = 0.8, criterion: str = "flat", max_trials: float = 1e12,
                        checkpoints=None) -> dict:
-    s = np.ascontiguousarray(state, dtype=np.int8).copy()
-    order = initial_order(s, q)
+    """One walker through critmc's Wang-Landau schedule, the moves on the oracle.
+
+    Blocks of ``check_sweeps`` N moves (cut short at checkpoints); after each:
+    the levels visited so far, ln f = n_levels / t once in 1/t mode, copies of
+    ln g at passed checkpoints, and (before 1/t mode) the flatness or visit
+    test, whose success records a stage, halves ln f, clears the histogram and
+    may switch to 1/t mode when ln f < n_seen / t.  Stops at ln f < ln_f_final
+    or ``max_trials``; later checkpoints get the final ln g.
+    """
+    spins = np.ascontiguousarray(state, dtype=np.int8).copy()
+    order = initial_order(spins, q)
     ln_g = np.zeros(levels)
-    hist = np.zeros(levels, dtype=np.int64)
+    visits = np.zeros(levels, dtype=np.int64)
     seen = np.zeros(levels, dtype=bool)
-    cps = list(sorted(checkpoints)) if checkpoints is not None else []
-    saved, stages = [], []
-    check_moves = max(1, int(check_sweeps) * n_sites)
-    ln_f, mode_1t, n_lev, t, trials = 1.0, False, 0.0, 0, 0
-    while True:
-        block = check_moves
-        if cps and cps[0] - t < block:
-            block = int(cps[0] - t)
-        if block > 0:
-            idx, trials, _, _ = oracle.fh_run(0, s, shape, q, key, idx, order, ln_g, hist, window, trials, ln_f,
-                                              n_lev, mode_1t, 0, block)
-            t += block
-        seen |= hist > 0
-        if mode_1t:
-            ln_f = n_lev / t
-        while cps and cps[0] <= t:
-            saved.append((int(cps.pop(0)), float(ln_f), ln_g.copy()))
-        if not mode_1t:
-            h = hist[seen]
-            ok = h.min() > 0 if criterion == "visit" else h.min() >= flatness * h.mean()
-            if ok:
-                stages.append({"ln_f": ln_f, "trials": t})
-                ln_f /= 2.0
-                hist[:] = 0
-                if one_over_t and ln_f < seen.sum() / t:
-                    mode_1t = True
-                    n_lev = float(seen.sum())
-                    ln_f = n_lev / t
-        if ln_f < ln_f_final or t >= max_trials:
-            break
-    saved.extend((int(c), float(ln_f), ln_g.copy()) for c in cps)
-    return {"ln_g": ln_g, "visited": seen, "trials": t, "ln_f": ln_f, "stages": stages, "checkpoints": saved,
-            "state": s, "idx": idx}
+    marks = sorted(checkpoints) if checkpoints is not None else []
+    kept, stages = [], []
+    ln_f, inverse_t, n_levels, t, trials = 1.0, False, 0.0, 0, 0
+    while ln_f >= ln_f_final and t < max_trials:
+        step = max(1, int(check_sweeps) * n_sites)
+        if marks:
+            step = min(step, int(marks[0] - t))
+        if step > 0:
+            idx, trials, _, _ = oracle.fh_run(0, spins, shape, q, key, idx, order, ln_g, visits, window, trials,
+                                              ln_f, n_levels, inverse_t, 0, step)
+            t += step
+        seen = seen | (visits > 0)
+        if inverse_t:
+            ln_f = n_levels / t
+        while marks and marks[0] <= t:
+            kept.append((int(marks.pop(0)), float(ln_f), ln_g.copy()))
+        if inverse_t:
+            continue
+        counts = visits[seen]
+        passed = counts.min() > 0 if criterion == "visit" else counts.min() >= flatness * counts.mean()
+        if not passed:
+            continue
+        stages.append({"ln_f": ln_f, "trials": t})
+        ln_f = ln_f / 2.0
+        visits[:] = 0
+        if one_over_t and ln_f < seen.sum() / t:
+            inverse_t, n_levels = True, float(seen.sum())
+            ln_f = n_levels / t
+    kept += [(int(m), float(ln_f), ln_g.copy()) for m in marks]
+    return {"ln_g": ln_g, "visited": seen, "trials": t, "ln_f": ln_f, "stages": stages, "checkpoints": kept,
+            "state": spins, "idx": idx}
 
 
 def replay_multicanonical(shape, q: int, state: np.ndarray, key, idx: int, window, ln_w: np.ndarray,

@@ -63,55 +63,91 @@ def profile_traffic() -> dict | None:
 
 
 class Clocks:
-    """Samples nvidia-smi clocks every 200 ms while running."""
+    """Samples the SM clock, its maximum and the clock-event reasons of one GPU
+    every 100 ms from a host thread (NVML queries only; no setting is changed).
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML is read in-process rather than through a piped ``nvidia-smi -lms``:
+    that child buffers its output and, stopped by a signal, can lose every
+    sample it took.
+    """
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, device, period_s: float = 0.1):
+        self.device = device
+        self.period = period_s
+        self.samples: list[tuple[float, float, int]] = []
+        self.error = None
+        self._stop = None
+        self._thread = None
+
+    def _handle(self, nvml):
+        import torch
+
+        try:  # match the CUDA device to its NVML handle by PCI address (CUDA_VISIBLE_DEVICES may remap)
+            p = torch.cuda.get_device_properties(self.device)
+            return nvml.nvmlDeviceGetHandleByPciBusId(f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0")
+        except Exception:
+            return nvml.nvmlDeviceGetHandleByIndex(int(getattr(self.device, "index", 0) or 0))
 
     def __enter__(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.index)],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            h = self._handle(nvml)
+        except Exception as exc:  # no NVML: the line says so instead of carrying no record
+            self.error = f"NVML unavailable: {exc}"
+            return self
+        self._stop = threading.Event()
+
+        def loop():
+            get_reasons = getattr(nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            while not self._stop.is_set():
+                try:
+                    sm = nvml.nvmlDeviceGetClockInfo(h, nvml.NVML_CLOCK_SM)
+                    mx = nvml.nvmlDeviceGetMaxClockInfo(h, nvml.NVML_CLOCK_SM)
+                    self.samples.append((float(sm), float(mx), int(get_reasons(h))))
+                except Exception as exc:
+                    self.error = str(exc)
+                self._stop.wait(self.period)
+
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
         return False
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in getattr(self, "lines", []):
-            f = [x.strip() for x in ln.split(",")]
-            try:
-                sm.append(float(f[0]))
-                mx.append(float(f[1]))
-            except (ValueError, IndexError):
-                continue
-            for name, v in zip(names, f[4:8]):
-                if v.lower() == "active":
+        if not self.samples:
+            out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            if self.error:
+                out["error"] = self.error
+            return out
+        try:
+            import pynvml as nvml
+        except Exception:
+            nvml = None
+        reasons = set()
+        for _, _, mask in self.samples:
+            for name, const in self.REASONS:
+                bit = getattr(nvml, const, 0) if nvml else 0
+                if bit and mask & bit:
                     reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples),
+                "sm_max_mhz": max(x[1] for x in self.samples), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": "NVML, 100 ms period, during the timed steps"}
 
 
 def ea_bench(dev, n_bins: int = 16, peak: float = 6650.0) -> dict:
@@ -554,15 +590,20 @@ def main() -> None:
     # launch shape (rows per thread, inline planes) from the autotuner; results do not depend on it
     ens = IsingEnsemble(L_HEAD, BETAS, CHAINS_PER_BETA, seed=1000 + rank, device=dev, tune=True)
     tuning = ens.tuning
+    tuning_mode = (ens.mode & 0xFF) or 3  # 0 means the library's default, graph replay
     n_upd = ens.n_chains * ens.n_sites  # per step and rank
     for _ in range(args.warmup):
         ens.run(1, "metropolis", host=False)
-    with Clocks(local) as clk:
+    with Clocks(dev) as clk:
         ms = timed(lambda: ens.run(1, "metropolis", host=False), args.steps)
     value = world * n_upd * args.steps / (ms * 1e6)
 
-    # end to end through the public API: host outputs (pinned) every step
+    # end to end through the public API: host outputs (pinned) every step; the
+    # pinned output buffers are made by untimed warm-up calls, as a caller that
+    # advances its chains step after step would reuse them
     out = None
+    for _ in range(2):
+        out = ens.run(1, "metropolis", host=True, out=out)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -640,7 +681,8 @@ def main() -> None:
                        "chains_per_gpu": len(BETAS) * CHAINS_PER_BETA, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (384 MiB of spins per GPU)"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-            "gpu_launches": args.steps * (1 + launches_per_step + 1),
+            # per step: the half-sweep launches, the finalize scan, and with graph mode a cursor reset
+            "gpu_launches": args.steps * (launches_per_step + 1 + (1 if tuning_mode != 1 else 0)),
             "tuning": tuning,
             "clocks": clk.summary(), "extras": extras, "serving": serving,
         }

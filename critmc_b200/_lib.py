@@ -144,3 +144,28 @@ def call(name: str, *args) -> int:
     status = getattr(lib(), name)(*args)
     check(status)
     return status
+
+
+# Entry points that only fill host tables: they touch no device and need no guard.
+HOST_ONLY = frozenset({
+    "critmc_version", "critmc_last_error", "critmc_ising_class_table", "critmc_ising_msc_scratch_bytes",
+    "critmc_item_prepare", "critmc_items_buffer_bytes", "critmc_ising_msc_noalloc_max_scratch_bytes",
+    "critmc_potts_tables", "critmc_pt_swap_table", "critmc_ea_coupling_bits", "critmc_on_grid_scratch_bytes",
+    "critmc_graph_cache_set_capacity", "critmc_cluster_scratch_bytes", "critmc_stream_state_bytes",
+    "critmc_ea_campaign_buffer_bytes", "critmc_graph_cache_size",
+})
+
+
+def call_on(device, name: str, *args) -> int:
+    """Call ``name`` with ``device`` made current for the duration of the call.
+
+    The C entry points launch on the calling thread's current CUDA device
+    (``cudaGetDevice``); buffers and the stream handle that a wrapper passes
+    belong to the wrapper's own device.  Without this guard a chain on cuda:1,
+    driven from a thread whose current device is 0, would launch on GPU 0
+    against GPU 1's memory.
+    """
+    import torch
+
+    with torch.cuda.device(device):
+        return call(name, *args)

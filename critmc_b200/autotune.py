@@ -107,9 +107,10 @@ def tune_msc(shape, n_chains: int, *, beta: float = 0.4406868, h: float = 0.0, s
     words = torch.empty((n_chains, 2, rows, lx // 64), dtype=torch.int32, device=dev)
     keys = np.arange(2 * n_chains, dtype=np.uint32).reshape(n_chains, 2)
     st = stream_handle(dev)
-    _lib.call("critmc_ising_msc_init", ptr(words), len(shape), lx, ly, lz, n_chains, ptr(to_dev(keys, dev)), 0, st)
+    _lib.call_on(dev, "critmc_ising_msc_init", ptr(words), len(shape), lx, ly, lz, n_chains, ptr(to_dev(keys, dev)),
+                 0, st)
     running = torch.empty((n_chains, 2), dtype=torch.int64, device=dev)
-    _lib.call("critmc_ising_msc_measure", ptr(words), len(shape), lx, ly, lz, n_chains, ptr(running), st)
+    _lib.call_on(dev, "critmc_ising_msc_measure", ptr(words), len(shape), lx, ly, lz, n_chains, ptr(running), st)
     tables = ising_tables(2 * len(shape), beta, h)
     e = torch.empty((n_chains, n_meas), dtype=torch.int64, device=dev)
     m = torch.empty_like(e)
@@ -119,9 +120,9 @@ def tune_msc(shape, n_chains: int, *, beta: float = 0.4406868, h: float = 0.0, s
     per_meas = int(sched[:, 1].sum())
 
     def call(run, k_inline, mode):
-        _lib.call("critmc_ising_msc_run", ptr(words), len(shape), lx, ly, lz, n_chains, keys.ctypes.data,
-                  tables.ctypes.data, 1, sweep[0], sched.ctypes.data, len(sched), n_meas, ptr(running), ptr(e),
-                  ptr(m), ptr(aux), ptr(scratch), msc_mode(run, mode), k_inline, st)
+        _lib.call_on(dev, "critmc_ising_msc_run", ptr(words), len(shape), lx, ly, lz, n_chains, keys.ctypes.data,
+                     tables.ctypes.data, 1, sweep[0], sched.ctypes.data, len(sched), n_meas, ptr(running), ptr(e),
+                     ptr(m), ptr(aux), ptr(scratch), msc_mode(run, mode), k_inline, st)
         sweep[0] += per_meas * n_meas
 
     trials = []

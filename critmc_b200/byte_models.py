@@ -40,9 +40,9 @@ class IsingByteChain(_ByteChain):
         m = torch.empty((1, n_meas), dtype=torch.int64, device=dev)
         aux = torch.empty((1, n_meas, N_AUX), dtype=torch.int64, device=dev)
         lx, ly, lz = self.dims
-        _lib.call("critmc_ising_byte_run", ptr(self.spins), len(self.shape), lx, ly, lz, 1,
-                  self.key.ctypes.data, tables.ctypes.data, 1, self.sweep, sched.ctypes.data,
-                  len(sched), n_meas, ptr(run), ptr(e), ptr(m), ptr(aux), stream_handle(dev))
+        _lib.call_on(dev, "critmc_ising_byte_run", ptr(self.spins), len(self.shape), lx, ly, lz, 1,
+                     self.key.ctypes.data, tables.ctypes.data, 1, self.sweep, sched.ctypes.data, len(sched), n_meas,
+                     ptr(run), ptr(e), ptr(m), ptr(aux), stream_handle(dev))
         self.sweep += int(sched[:, 1].sum()) * n_meas
         r = to_host(run)[0]
         running["e_b"], running["m"] = int(r[0]), int(r[1])
@@ -67,10 +67,9 @@ class PottsChain(_ByteChain):
         co = torch.empty((1, n_meas, q), dtype=torch.int64, device=dev)
         aux = torch.empty((1, n_meas, N_AUX), dtype=torch.int64, device=dev)
         lx, ly, lz = self.dims
-        _lib.call("critmc_potts_run", ptr(self.spins), len(self.shape), lx, ly, lz, q, 1,
-                  self.key.ctypes.data, betas.ctypes.data, 1, self.sweep, sched.ctypes.data,
-                  len(sched), n_meas, ptr(energy), ptr(counts), ptr(e), ptr(co), ptr(aux),
-                  stream_handle(dev))
+        _lib.call_on(dev, "critmc_potts_run", ptr(self.spins), len(self.shape), lx, ly, lz, q, 1,
+                     self.key.ctypes.data, betas.ctypes.data, 1, self.sweep, sched.ctypes.data, len(sched), n_meas,
+                     ptr(energy), ptr(counts), ptr(e), ptr(co), ptr(aux), stream_handle(dev))
         self.sweep += int(sched[:, 1].sum()) * n_meas
         running["energy"] = int(to_host(energy)[0])
         running["counts"] = to_host(counts)[0].copy()

@@ -48,10 +48,9 @@ class Chain:
         if state is not None:
             start = "state"
             init = self._host_state(state)
-        with torch.cuda.device(self.device):
-            _lib.call("critmc_chain_create", KINDS[kind], dims, self.q_or_n, float(h), seed & 0xFFFFFFFF,
-                      (seed >> 32) & 0xFFFFFFFF, int(chain_id), STARTS[start],
-                      init.ctypes.data if init is not None else None, ctypes.byref(handle))
+        _lib.call_on(self.device, "critmc_chain_create", KINDS[kind], dims, self.q_or_n, float(h), seed & 0xFFFFFFFF,
+                     (seed >> 32) & 0xFFFFFFFF, int(chain_id), STARTS[start],
+                     init.ctypes.data if init is not None else None, ctypes.byref(handle))
         self._h = handle
 
     def _host_state(self, state) -> np.ndarray:
@@ -61,12 +60,12 @@ class Chain:
 
     def info(self) -> dict:
         layout, sweep, key = ctypes.c_int32(), ctypes.c_uint32(), (ctypes.c_uint32 * 2)()
-        _lib.call("critmc_chain_info", self._h, ctypes.byref(layout), ctypes.byref(sweep), key)
+        _lib.call_on(self.device, "critmc_chain_info", self._h, ctypes.byref(layout), ctypes.byref(sweep), key)
         return {"layout": ("msc", "byte", "float")[layout.value], "sweep": sweep.value,
                 "key": np.array(list(key), dtype=np.uint32)}
 
     def set_step(self, step: float) -> None:
-        _lib.call("critmc_chain_set_step", self._h, float(step))
+        _lib.call_on(self.device, "critmc_chain_set_step", self._h, float(step))
 
     def outputs(self, n_meas: int) -> dict[str, torch.Tensor]:
         dev, n = self.device, n_meas
@@ -95,9 +94,9 @@ class Chain:
     def advance(self, beta: float, updates, n_meas: int) -> dict[str, np.ndarray]:
         sched = schedule_array(updates)
         out = self.outputs(n_meas)
-        _lib.call("critmc_advance", self._h, float(beta), sched.ctypes.data, len(sched), int(n_meas),
-                  ptr(out.get("e")), ptr(out.get("m")), ptr(out["aux"]), ptr(out.get("f64")),
-                  stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_advance", self._h, float(beta), sched.ctypes.data, len(sched), int(n_meas),
+                     ptr(out.get("e")), ptr(out.get("m")), ptr(out["aux"]), ptr(out.get("f64")),
+                     stream_handle(self.device))
         return self.raw(out, n_meas)
 
     def state(self) -> tuple[np.ndarray, np.ndarray | None]:
@@ -108,13 +107,13 @@ class Chain:
         else:
             s = np.empty(self.n_sites, dtype=np.int8)
             run = np.empty(2 if self.kind == "ising" else 1 + self.q_or_n, dtype=np.int64)
-        _lib.call("critmc_get_state", self._h, s.ctypes.data, run.ctypes.data if run is not None else None,
-                  stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_get_state", self._h, s.ctypes.data,
+                     run.ctypes.data if run is not None else None, stream_handle(self.device))
         return s, run
 
     def set_state(self, state) -> None:
         s = self._host_state(state)
-        _lib.call("critmc_set_state", self._h, s.ctypes.data, stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_set_state", self._h, s.ctypes.data, stream_handle(self.device))
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -134,7 +133,7 @@ class Batch:
     def __init__(self, device=None):
         self.device = require_cuda(device)
         handle = ctypes.c_void_p()
-        _lib.call("critmc_batch_create", ctypes.byref(handle))
+        _lib.call_on(self.device, "critmc_batch_create", ctypes.byref(handle))
         self._h = handle
         self._subs: dict[int, tuple] = {}
 
@@ -142,13 +141,14 @@ class Batch:
         sched = schedule_array(updates)
         out = chain.outputs(n_meas)
         ticket = ctypes.c_int64()
-        _lib.call("critmc_batch_submit", self._h, chain._h, float(beta), sched.ctypes.data, len(sched), int(n_meas),
-                  ptr(out.get("e")), ptr(out.get("m")), ptr(out["aux"]), ptr(out.get("f64")), ctypes.byref(ticket))
+        _lib.call_on(self.device, "critmc_batch_submit", self._h, chain._h, float(beta), sched.ctypes.data,
+                     len(sched), int(n_meas), ptr(out.get("e")), ptr(out.get("m")), ptr(out["aux"]),
+                     ptr(out.get("f64")), ctypes.byref(ticket))
         self._subs[ticket.value] = (chain, out, n_meas)
         return ticket.value
 
     def cancel(self, ticket: int) -> None:
-        _lib.call("critmc_batch_cancel", self._h, int(ticket))
+        _lib.call_on(self.device, "critmc_batch_cancel", self._h, int(ticket))
         self._subs.pop(ticket, None)
 
     def pending(self) -> int:
@@ -159,7 +159,8 @@ class Batch:
         n = min(max_done, max(1, len(self._subs)))
         done = (ctypes.c_int64 * n)()
         n_done = ctypes.c_int32()
-        _lib.call("critmc_batch_poll", self._h, stream_handle(self.device), done, n, ctypes.byref(n_done))
+        _lib.call_on(self.device, "critmc_batch_poll", self._h, stream_handle(self.device), done, n,
+                     ctypes.byref(n_done))
         res = {}
         for t in list(done)[:n_done.value]:
             chain, out, n_meas = self._subs.pop(t)

@@ -75,10 +75,14 @@ int CaptureStream::begin(void* stream) {
     private_stream = false;
     return CRITMC_OK;
   }
-  static thread_local cudaStream_t priv = nullptr;
-  if (!priv && cudaStreamCreateWithFlags(&priv, cudaStreamNonBlocking) != cudaSuccess)
+  constexpr int MAX_DEVICES = 64;
+  static thread_local cudaStream_t priv[MAX_DEVICES] = {};
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail("cudaGetDevice");
+  if (dev < 0 || dev >= MAX_DEVICES) return fail(CRITMC_ERR_UNSUPPORTED, "device ordinal out of range");
+  if (!priv[dev] && cudaStreamCreateWithFlags(&priv[dev], cudaStreamNonBlocking) != cudaSuccess)
     return cuda_fail("stream create");
-  work = priv;
+  work = priv[dev];
   private_stream = true;
   cudaEvent_t ev;
   if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");

@@ -53,6 +53,7 @@ struct critmc_batch {
   };
   std::vector<Sub> pending;
   int64_t next_ticket = 1;
+  int device = -1;  // device of the first submitted chain; every chain of a batch lives there
   void* buffer = nullptr;
   size_t buffer_bytes = 0;
 };
@@ -316,6 +317,7 @@ extern "C" int32_t critmc_chain_create(int32_t model_kind, const int32_t dims[3]
 
 extern "C" int32_t critmc_chain_destroy(critmc_chain* c) {
   if (!c) return CRITMC_OK;
+  DeviceScope ds(c->device);
   cudaDeviceSynchronize();  // no work of this chain may still be in flight
   if (c->lattice) cudaFree(c->lattice);
   if (c->running) cudaFree(c->running);
@@ -346,6 +348,8 @@ extern "C" int32_t critmc_chain_set_step(critmc_chain* c, double step) {
 extern "C" int32_t critmc_get_state(critmc_chain* c, void* host_out, int64_t* running_out, void* stream) {
   clear_error();
   if (!c || !host_out) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  DeviceScope ds(c->device);
+  if (ds.status) return ds.status;
   std::vector<unsigned char> img(c->lattice_bytes);
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemcpyAsync(img.data(), c->lattice, img.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -365,6 +369,8 @@ extern "C" int32_t critmc_set_state(critmc_chain* c, const void* host_in, void* 
   if (!c) return fail(CRITMC_ERR_INVALID, "null chain");
   int st = check_state(*c, host_in);
   if (st) return st;
+  DeviceScope ds(c->device);
+  if (ds.status) return ds.status;
   return upload(*c, host_in, stream);
 }
 
@@ -374,6 +380,8 @@ extern "C" int32_t critmc_advance(critmc_chain* c, double beta, const int64_t* s
   clear_error();
   if (!c || !schedule || !aux_out) return fail(CRITMC_ERR_INVALID, "null pointer argument");
   if (n_meas < 0) return fail(CRITMC_ERR_INVALID, "n_meas must not be negative");
+  DeviceScope ds(c->device);
+  if (ds.status) return ds.status;
   const long long per = sweeps_of(schedule, n_rows);
   int st = CRITMC_OK;
   cudaStream_t s = (cudaStream_t)stream;
@@ -421,6 +429,7 @@ extern "C" int32_t critmc_batch_create(critmc_batch** b) {
 extern "C" int32_t critmc_batch_destroy(critmc_batch* b) {
   if (!b) return CRITMC_OK;
   if (b->buffer) {
+    DeviceScope ds(b->device);
     cudaDeviceSynchronize();
     cudaFree(b->buffer);
   }
@@ -437,6 +446,9 @@ extern "C" int32_t critmc_batch_submit(critmc_batch* b, critmc_chain* c, double 
   if (!std::isfinite(beta)) return fail(CRITMC_ERR_INVALID, "beta must be finite");
   if (c->kind != CRITMC_MODEL_ON && (!e_out || !m_out)) return fail(CRITMC_ERR_INVALID, "missing e_out or m_out");
   if (c->kind == CRITMC_MODEL_ON && !f64_out) return fail(CRITMC_ERR_INVALID, "O(n) chains need f64_out");
+  if (b->device >= 0 && c->device != b->device)
+    return fail(CRITMC_ERR_INVALID, "every chain of a batch must live on the device of its first chain");
+  b->device = c->device;
   critmc_batch::Sub sub;
   sub.ticket = b->next_ticket++;
   sub.c = c;
@@ -516,6 +528,12 @@ extern "C" int32_t critmc_batch_poll(critmc_batch* b, void* stream, int64_t* don
   if (!b || !n_done || (max_done > 0 && !done)) return fail(CRITMC_ERR_INVALID, "null pointer argument");
   *n_done = 0;
   cudaStream_t s = (cudaStream_t)stream;
+  if (b->pending.empty()) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) return cuda_fail("synchronize");
+    return CRITMC_OK;
+  }
+  DeviceScope ds(b->device);
+  if (ds.status) return ds.status;
   // rounds: each takes the first pending submission of every chain (FIFO per chain)
   while (!b->pending.empty() && *n_done < max_done) {
     std::vector<size_t> take;

@@ -23,9 +23,34 @@ int cuda_fail(const char* what);
 // CRITMC_OK if no CUDA error is pending, else record and clear it (CRITMC_ERR_CUDA)
 int cuda_check(const char* what);
 
+// Makes `dev` the calling thread's current device for the guard's lifetime
+// and restores the previous one.  Handle-based entry points (chains, batches)
+// remember the device they were created on and must launch there whatever
+// device the caller's thread has current.
+struct DeviceScope {
+  int prev = -1;
+  int status = CRITMC_OK;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      status = cuda_fail("cudaGetDevice");
+    } else if (prev != dev && cudaSetDevice(dev) != cudaSuccess) {
+      status = cuda_fail("cudaSetDevice");
+    }
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
 // A stream the library may capture into a CUDA graph: the caller's stream, or,
 // when the caller passed the legacy default stream, a per-thread private
 // stream ordered after it (and `finish` orders the legacy stream after it).
+// The private stream is kept per thread and per device, so a thread that
+// switches devices never enqueues work on another device's stream.
 struct CaptureStream {
   cudaStream_t user = nullptr;
   cudaStream_t work = nullptr;

@@ -5,6 +5,8 @@
 // Replaces critmc src/critmc/kernels/ising.py:174-237 (`run`), :69-87
 // (`metropolis_sweep`), :91-107 (`heatbath_sweep`) and :32-45
 // (`bond_energy`, `magnetization`).
+#include <cuda.h>
+
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -572,26 +574,69 @@ namespace critmc {
 constexpr size_t MSC_NOALLOC_SCRATCH_BYTES = 1u << 20;  // 1 MiB on every device that loads the library
 static __device__ __align__(256) unsigned char g_msc_noalloc_scratch[MSC_NOALLOC_SCRATCH_BYTES];
 
-// Device address of the array on each device, looked up once per device.  In
-// host code the array's name is only a stand-in for the symbol, never a
-// device address, so it must be resolved with cudaGetSymbolAddress while that
-// device is current.
-static void* g_noalloc_addr[64];
-static std::once_flag g_noalloc_once[64];
-static cudaError_t g_noalloc_err[64];
+// Device address of the array on each device.  In host code the array's name
+// is only a stand-in for the symbol, never a device address, so it is resolved
+// with cudaGetSymbolAddress while that device is current.  The address is
+// cached per device together with the unique id of the context it belongs to:
+// a lookup that failed is retried on the next call, and after a
+// cudaDeviceReset (which unloads the module, so the array may come back at
+// another address) the new context's id differs and the address is looked
+// up again instead of being written through stale.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+
+struct NoallocSlot {
+  void* addr = nullptr;
+  unsigned long long ctx_id = 0;
+  bool valid = false;
+};
+static NoallocSlot g_noalloc[64];
+static std::mutex g_noalloc_mu;
+
+// unique id of the calling thread's current context (0 if unavailable)
+static unsigned long long current_context_id() {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (PfnCtxGetCurrent)fn;
+    fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (PfnCtxGetId)fn;
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 static int noalloc_scratch(void** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail("cudaGetDevice");
   if (dev < 0 || dev >= 64) return fail(CRITMC_ERR_UNSUPPORTED, "device ordinal out of range");
-  std::call_once(g_noalloc_once[dev], [dev] {
-    g_noalloc_err[dev] = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_msc_noalloc_scratch);
-  });
-  if (g_noalloc_err[dev] != cudaSuccess) {
-    set_error(cudaGetErrorString(g_noalloc_err[dev]));
-    return CRITMC_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoallocSlot& slot = g_noalloc[dev];
+  const unsigned long long ctx_id = current_context_id();
+  if (!slot.valid || ctx_id == 0 || slot.ctx_id != ctx_id) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_msc_noalloc_scratch);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      slot.valid = false;  // not cached: the next call looks it up again
+      set_error(cudaGetErrorString(e));
+      return CRITMC_ERR_CUDA;
+    }
+    slot.addr = addr;
+    slot.ctx_id = current_context_id();  // the lookup has made the context current if it was not
+    slot.valid = slot.ctx_id != 0;
   }
-  *out = g_noalloc_addr[dev];
+  *out = slot.addr;
   return CRITMC_OK;
 }
 

@@ -65,14 +65,15 @@ class IsingEnsemble:
         code = {"random": 0, "ordered": 1, "up": 1, "down": -1}[start]
         dkeys = to_dev(self.keys, self.device)
         st = stream_handle(self.device)
-        _lib.call("critmc_ising_msc_init", ptr(self.words), len(shape), lx, ly, lz, self.n_chains,
-                  ptr(dkeys), code, st)
+        _lib.call_on(self.device, "critmc_ising_msc_init", ptr(self.words), len(shape), lx, ly, lz, self.n_chains,
+                     ptr(dkeys), code, st)
         self.running = torch.empty((self.n_chains, 2), dtype=torch.int64, device=self.device)
-        _lib.call("critmc_ising_msc_measure", ptr(self.words), len(shape), lx, ly, lz, self.n_chains,
-                  ptr(self.running), st)
+        _lib.call_on(self.device, "critmc_ising_msc_measure", ptr(self.words), len(shape), lx, ly, lz, self.n_chains,
+                     ptr(self.running), st)
         self.tables = np.ascontiguousarray(np.stack([self.model.tables(b)[0] for b in self.betas]))
         self.sweep = 0
         self._scratch = None
+        self._dev_out = None
         self.tuning = None
         if tune:
             # launch shape from the autotuner (cached per GPU, shape, batch): results do not change
@@ -101,17 +102,25 @@ class IsingEnsemble:
         sched = self._schedule(updates)
         dev = self.device
         n = self.n_chains
-        e = torch.empty((n, n_meas), dtype=torch.int64, device=dev)
-        m = torch.empty((n, n_meas), dtype=torch.int64, device=dev)
-        aux = torch.empty((n, n_meas, 4), dtype=torch.int64, device=dev)
+        if host:
+            # device outputs are staging only: reuse them from call to call
+            if self._dev_out is None or self._dev_out[0].shape[1] != n_meas:
+                self._dev_out = (torch.empty((n, n_meas), dtype=torch.int64, device=dev),
+                                 torch.empty((n, n_meas), dtype=torch.int64, device=dev),
+                                 torch.empty((n, n_meas, 4), dtype=torch.int64, device=dev))
+            e, m, aux = self._dev_out
+        else:  # returned to the caller: fresh tensors
+            e = torch.empty((n, n_meas), dtype=torch.int64, device=dev)
+            m = torch.empty((n, n_meas), dtype=torch.int64, device=dev)
+            aux = torch.empty((n, n_meas, 4), dtype=torch.int64, device=dev)
         need = _lib.lib().critmc_ising_msc_scratch_bytes(n, n_meas)
         if self._scratch is None or self._scratch.numel() < need:
             self._scratch = empty_bytes(need, dev)
         lx, ly, lz = self.dims
-        _lib.call("critmc_ising_msc_run", ptr(self.words), len(self.shape), lx, ly, lz, n,
-                  self.keys.ctypes.data, self.tables.ctypes.data, len(self.betas), self.sweep,
-                  sched.ctypes.data, len(sched), n_meas, ptr(self.running), ptr(e), ptr(m), ptr(aux),
-                  ptr(self._scratch), self.mode, self.k_inline, stream_handle(dev))
+        _lib.call_on(dev, "critmc_ising_msc_run", ptr(self.words), len(self.shape), lx, ly, lz, n,
+                     self.keys.ctypes.data, self.tables.ctypes.data, len(self.betas), self.sweep, sched.ctypes.data,
+                     len(sched), n_meas, ptr(self.running), ptr(e), ptr(m), ptr(aux), ptr(self._scratch), self.mode,
+                     self.k_inline, stream_handle(dev))
         self.sweep += int(sched[:, 1].sum()) * n_meas
         if not host:
             return EnsembleSeries(e, m, aux)

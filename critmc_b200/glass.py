@@ -39,10 +39,16 @@ SWAP_WIDTH = 2048
 
 
 class EdwardsAnderson:
-    """One disorder realisation with +-1 couplings (critmc glass.py:45-90)."""
+    """One disorder realisation with +-1 couplings (critmc glass.py:45-90).
+
+    The default disorder is critmc's, ``"gaussian"``, which the multi-spin-coded
+    kernel cannot run: a sample without explicit couplings must ask for
+    ``disorder="bimodal"``, so that ``EdwardsAnderson(lat, seed=s)`` never
+    builds a different model from the one critmc builds for the same call.
+    """
 
     def __init__(self, lattice: Lattice, couplings: np.ndarray | None = None, *,
-                 disorder: str = "bimodal", seed=None):
+                 disorder: str = "gaussian", seed=None):
         self.lattice = lattice
         self.disorder = disorder
         if not lattice.hypercubic or not lattice.bipartite or lattice.dim not in (2, 3):
@@ -53,7 +59,8 @@ class EdwardsAnderson:
             raise ValueError("the GPU spin-glass kernel needs equal extents")
         if couplings is None:
             if disorder == "gaussian":
-                raise ValueError("the multi-spin-coded kernel runs +-J couplings only, not Gaussian ones")
+                raise ValueError("Gaussian couplings (critmc's default disorder) are not supported: the "
+                                 "multi-spin-coded kernel runs +-J couplings only; pass disorder=\"bimodal\"")
             if disorder != "bimodal":
                 raise ValueError(f"disorder is 'bimodal' (or 'gaussian' in critmc), not {disorder!r}")
             # +-1 with probability 1/2 each: one uniform index per bond into (-1, +1),
@@ -195,10 +202,10 @@ class SpinGlassCampaign:
         shape = self.lattice.shape
         dims = tuple(shape) + (1,) * (3 - len(shape))
         t0 = time.perf_counter()
-        _lib.call("critmc_ea_pt_run", ptr(self.words), ptr(self.jneg), len(shape), *dims,
-                  len(self.temperatures), self.n_samples, self.keys.ctypes.data, self.betas.ctypes.data,
-                  ptr(self.swap_thr), SWAP_WIDTH, ptr(self.conf_at), ptr(self.labels), self.step, n_steps,
-                  n_bins, self.sweeps_per_step, *(ptr(out[k]) for k in _OUT_KEYS), stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_ea_pt_run", ptr(self.words), ptr(self.jneg), len(shape), *dims,
+                     len(self.temperatures), self.n_samples, self.keys.ctypes.data, self.betas.ctypes.data,
+                     ptr(self.swap_thr), SWAP_WIDTH, ptr(self.conf_at), ptr(self.labels), self.step, n_steps, n_bins,
+                     self.sweeps_per_step, *(ptr(out[k]) for k in _OUT_KEYS), stream_handle(self.device))
         torch.cuda.synchronize(self.device)
         self.step += n_steps
         return self._collect(out, n_bins, time.perf_counter() - t0)
@@ -290,10 +297,10 @@ class MultiSizeCampaign:
             z.label_hist, z.trips = ptr(o["label_hist"]), ptr(o["trips"])
             z.lx, z.ly, z.lz = dims
             z.n_samples = c.n_samples
-        _lib.call("critmc_ea_campaign_run", ctypes.cast(sizes, ctypes.c_void_p), len(self.campaigns),
-                  c0.lattice.dim, len(c0.temperatures), c0.betas.ctypes.data, ptr(c0.swap_thr), SWAP_WIDTH,
-                  c0.step, n_steps, n_bins, c0.sweeps_per_step, ptr(self._buffer), self._bytes,
-                  self._staging.data_ptr(), stream if stream is not None else stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_ea_campaign_run", ctypes.cast(sizes, ctypes.c_void_p), len(self.campaigns),
+                     c0.lattice.dim, len(c0.temperatures), c0.betas.ctypes.data, ptr(c0.swap_thr), SWAP_WIDTH,
+                     c0.step, n_steps, n_bins, c0.sweeps_per_step, ptr(self._buffer), self._bytes,
+                     self._staging.data_ptr(), stream if stream is not None else stream_handle(self.device))
         for c in self.campaigns:
             c.step += n_steps
         return outs

@@ -157,8 +157,8 @@ def launch_items(items, device, buffer: torch.Tensor | None, *, staging: torch.T
     if staging is not None and staging.numel() < n * ctypes.sizeof(CritmcItem):
         raise ValueError("staging buffer too small")
     st = stream if stream is not None else stream_handle(device)
-    _lib.call("critmc_run_items", ctypes.cast(arr, ctypes.c_void_p), n, ptr(buffer), int(need),
-              staging.data_ptr() if staging is not None else None, int(smem_limit), st)
+    _lib.call_on(device, "critmc_run_items", ctypes.cast(arr, ctypes.c_void_p), n, ptr(buffer), int(need),
+                 staging.data_ptr() if staging is not None else None, int(smem_limit), st)
     return buffer
 
 

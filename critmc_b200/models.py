@@ -82,9 +82,9 @@ def advance_with_clusters(model, chain, running, beta, schedule, n_meas, bits: b
                     run_t = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
                     cnt_t = None
                 for _ in range(int(reps)):
-                    _lib.call("critmc_cluster_update", int(bits), ptr(spins), len(chain.shape), *dims, q, 1,
-                              chain.key.ctypes.data, float(beta), int(code), chain.sweep, ptr(run_t), ptr(cnt_t),
-                              ptr(stats), ptr(chain._cl_scratch), stream_handle(dev))
+                    _lib.call_on(dev, "critmc_cluster_update", int(bits), ptr(spins), len(chain.shape), *dims, q, 1,
+                                 chain.key.ctypes.data, float(beta), int(code), chain.sweep, ptr(run_t), ptr(cnt_t),
+                                 ptr(stats), ptr(chain._cl_scratch), stream_handle(dev))
                     chain.sweep += 1
                 r = to_host(run_t).ravel()
                 if potts:
@@ -217,16 +217,16 @@ class _IsingMscChain:
         self.mode = 0
         self.k_inline = 8
         dkey = to_dev(self.key, self.device)
-        _lib.call("critmc_ising_msc_init", ptr(self.words), len(self.shape), lx, ly, lz, 1, ptr(dkey), start,
-                  stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_ising_msc_init", ptr(self.words), len(self.shape), lx, ly, lz, 1, ptr(dkey),
+                     start, stream_handle(self.device))
         return self
 
     def measure(self) -> torch.Tensor:
         """Device int64 (E_b, M) of the current configuration."""
         out = torch.empty((1, 2), dtype=torch.int64, device=self.device)
         lx, ly, lz = self.dims
-        _lib.call("critmc_ising_msc_measure", ptr(self.words), len(self.shape), lx, ly, lz, 1, ptr(out),
-                  stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_ising_msc_measure", ptr(self.words), len(self.shape), lx, ly, lz, 1,
+                     ptr(out), stream_handle(self.device))
         return out
 
     def fetch(self) -> np.ndarray:
@@ -312,10 +312,9 @@ class Ising(Model):
         aux = torch.empty((1, n_meas, N_AUX), dtype=torch.int64, device=dev)
         scratch = empty_bytes(_lib.lib().critmc_ising_msc_scratch_bytes(1, n_meas), dev)
         lx, ly, lz = chain.dims
-        _lib.call("critmc_ising_msc_run", ptr(chain.words), len(chain.shape), lx, ly, lz, 1,
-                  chain.key.ctypes.data, tables.ctypes.data, 1, chain.sweep, sched.ctypes.data, len(sched),
-                  n_meas, ptr(run), ptr(e), ptr(m), ptr(aux), ptr(scratch), chain.mode,
-                  chain.k_inline, stream_handle(dev))
+        _lib.call_on(dev, "critmc_ising_msc_run", ptr(chain.words), len(chain.shape), lx, ly, lz, 1,
+                     chain.key.ctypes.data, tables.ctypes.data, 1, chain.sweep, sched.ctypes.data, len(sched), n_meas,
+                     ptr(run), ptr(e), ptr(m), ptr(aux), ptr(scratch), chain.mode, chain.k_inline, stream_handle(dev))
         chain.sweep += int(sched[:, 1].sum()) * n_meas
         r = to_host(run)[0]
         running["e_b"], running["m"] = int(r[0]), int(r[1])

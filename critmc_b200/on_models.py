@@ -90,9 +90,9 @@ class ONChain:
             for kind, seg in segments:
                 if kind == "cluster":
                     for _ in range(int(seg[1])):
-                        _lib.call("critmc_on_cluster_update", ptr(self.spins), len(self.shape), lx, ly, lz, self.n, 1,
-                                  self.key.ctypes.data, float(beta), int(seg[0]), self.sweep, ptr(stats),
-                                  ptr(self._cl_scratch), stream_handle(dev))
+                        _lib.call_on(dev, "critmc_on_cluster_update", ptr(self.spins), len(self.shape), lx, ly, lz,
+                                     self.n, 1, self.key.ctypes.data, float(beta), int(seg[0]), self.sweep,
+                                     ptr(stats), ptr(self._cl_scratch), stream_handle(dev))
                         self.sweep += 1
                 else:
                     part = self._advance_sweeps(running, beta, seg, 1)
@@ -122,9 +122,10 @@ class ONChain:
             need = _lib.lib().critmc_on_grid_scratch_bytes(1, n_meas, n, dim)
             if self._scratch is None or self._scratch.numel() < need:
                 self._scratch = empty_bytes(need, dev)
-            _lib.call("critmc_on_run_grid", *args, ptr(self._scratch), self.blocks_per_chain, stream_handle(dev))
+            _lib.call_on(dev, "critmc_on_run_grid", *args, ptr(self._scratch), self.blocks_per_chain,
+                         stream_handle(dev))
         else:
-            _lib.call("critmc_on_run", *args, stream_handle(dev))
+            _lib.call_on(dev, "critmc_on_run", *args, stream_handle(dev))
         self.sweep += int(sched[:, 1].sum()) * n_meas
         return {"E": to_host(e)[0], "M": to_host(m)[0], "stiff_c": to_host(sc)[0],
                 "stiff_s": to_host(ss)[0], "aux": to_host(aux)[0]}
@@ -183,10 +184,10 @@ class ONEnsemble:
                "stiff_s": torch.empty((nc, n_meas, dim), dtype=torch.float64, device=dev),
                "aux": torch.empty((nc, n_meas, N_AUX), dtype=torch.int64, device=dev)}
         lx, ly, lz = self.dims
-        _lib.call("critmc_on_run", ptr(self.spins), dim, lx, ly, lz, n, nc, self.keys.ctypes.data,
-                  self.betas.ctypes.data, self.steps.ctypes.data, len(self.betas), self.sweep,
-                  sched.ctypes.data, len(sched), n_meas, *(ptr(out[k]) for k in ("E", "M", "stiff_c", "stiff_s")),
-                  ptr(out["aux"]), stream if stream is not None else stream_handle(dev))
+        _lib.call_on(dev, "critmc_on_run", ptr(self.spins), dim, lx, ly, lz, n, nc, self.keys.ctypes.data,
+                     self.betas.ctypes.data, self.steps.ctypes.data, len(self.betas), self.sweep, sched.ctypes.data,
+                     len(sched), n_meas, *(ptr(out[k]) for k in ("E", "M", "stiff_c", "stiff_s")), ptr(out["aux"]),
+                     stream if stream is not None else stream_handle(dev))
         self.sweep += int(sched[:, 1].sum()) * n_meas
         return out
 

@@ -553,16 +553,16 @@ class Server:
         c = j.chain
         lx, ly, lz = c.dims
         if j.family == "msc":
-            _lib.call("critmc_ising_msc_run", ptr(c.words), len(c.shape), lx, ly, lz, 1, c.key.ctypes.data,
-                      j.tables.ctypes.data, 1, c.sweep, j.sched.ctypes.data, len(j.sched), n,
-                      ptr(j.tensors["running"]), ptrs[0], ptrs[1], ptrs[2], ptr(scratch), 0, c.k_inline,
-                      s.cuda_stream)
+            _lib.call_on(self.device, "critmc_ising_msc_run", ptr(c.words), len(c.shape), lx, ly, lz, 1,
+                         c.key.ctypes.data, j.tables.ctypes.data, 1, c.sweep, j.sched.ctypes.data, len(j.sched), n,
+                         ptr(j.tensors["running"]), ptrs[0], ptrs[1], ptrs[2], ptr(scratch), 0, c.k_inline,
+                         s.cuda_stream)
         else:
             betas, steps = j.tables
-            _lib.call("critmc_on_run_grid", ptr(c.spins), len(c.shape), lx, ly, lz, c.n, 1, c.key.ctypes.data,
-                      betas.ctypes.data, steps.ctypes.data, 1, c.sweep, j.sched.ctypes.data, len(j.sched), n,
-                      ptrs[0], ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptr(scratch), c.blocks_per_chain,
-                      s.cuda_stream)
+            _lib.call_on(self.device, "critmc_on_run_grid", ptr(c.spins), len(c.shape), lx, ly, lz, c.n, 1,
+                         c.key.ctypes.data, betas.ctypes.data, steps.ctypes.data, 1, c.sweep, j.sched.ctypes.data,
+                         len(j.sched), n, ptrs[0], ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptr(scratch),
+                         c.blocks_per_chain, s.cuda_stream)
 
     def _grid_scratch(self, stream: torch.cuda.Stream) -> torch.Tensor:
         key = stream.cuda_stream

@@ -85,8 +85,9 @@ class StreamStats:
         if values.dtype not in (torch.int64, torch.float64):
             values = values.to(torch.float64)
         v = values.contiguous()
-        _lib.call("critmc_stream_update", ptr(v), int(v.dtype == torch.float64), self.n_chains, v.shape[1],
-                  v.shape[1], ptr(self.state), self.W, stream if stream is not None else stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_stream_update", ptr(v), int(v.dtype == torch.float64), self.n_chains,
+                     v.shape[1], v.shape[1], ptr(self.state), self.W,
+                     stream if stream is not None else stream_handle(self.device))
 
     def result(self, S: float = 1.5) -> list[dict[str, float]]:
         st = to_host(self.state).reshape(self.n_chains, -1)

@@ -478,7 +478,9 @@ int32_t critmc_graph_cache_size(void);
  * n_chains * n_meas <= 43690; larger calls fail with CRITMC_ERR_INVALID
  * before any launch.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
+ * capture.  A lookup that fails is not cached (the next call tries again), and
+ * the address is looked up again after cudaDeviceReset, which gives the device
+ * a new context in which the array may sit elsewhere.  All calls share the array: calls that overlap on the GPU (other
  * streams, other host threads) race and must be serialised by the caller.
  * It calls no cudaMalloc/cudaFree and creates no streams, events or graphs.  */
 int64_t critmc_ising_msc_noalloc_max_scratch_bytes(void);

@@ -75,7 +75,7 @@ def test_same_seed_same_couplings_and_spins_as_critmc_convention(cuda):
     from critmc_b200.rng import make_rng
 
     lat = cubic(4)
-    ea = EdwardsAnderson(lat, seed=77)
+    ea = EdwardsAnderson(lat, disorder="bimodal", seed=77)
     np.testing.assert_array_equal(ea.couplings, make_rng(77).choice([-1.0, 1.0], size=lat.n_bonds))
     with pytest.raises(ValueError):
         EdwardsAnderson(lat, disorder="gaussian", seed=1)

@@ -63,3 +63,14 @@ def test_edwards_anderson_samples_match_critmc():
         EdwardsAnderson(cubic(4), disorder="gaussian", seed=1)
     with pytest.raises(ValueError):
         EdwardsAnderson(cubic(4), couplings=np.ones(5))
+
+
+def test_edwards_anderson_default_is_critmcs_gaussian_and_refused():
+    """critmc's EdwardsAnderson defaults to Gaussian couplings (critmc glass.py:52); the
+    +-J kernel refuses that default and names the disorder it runs, instead of
+    silently building a different model for the same call."""
+    from critmc_b200.glass import EdwardsAnderson
+
+    with pytest.raises(ValueError, match='disorder="bimodal"'):
+        EdwardsAnderson(cubic(4), seed=1)
+    assert EdwardsAnderson(cubic(4), disorder="bimodal", seed=1).disorder == "bimodal"

@@ -21,6 +21,9 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libcritmc_b200.so"
+# bounds-checked flavour (-DCRITMC_CHECK, see critmc_check_report): own objects and library
+BUILD_CHECK = PKG / "_build_check"
+LIB_CHECK = PKG / "libcritmc_b200_check.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
@@ -59,16 +62,23 @@ def _compile(src: Path, obj: Path, extra: list[str]) -> None:
         raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stdout}\n{res.stderr}")
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
-    """Build the shared library (incrementally) and return its path."""
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None, check: bool = False) -> Path:
+    """Build the shared library (incrementally) and return its path.
+
+    ``check``: the bounds-checked flavour (-DCRITMC_CHECK) into its own
+    object folder and ``libcritmc_b200_check.so``."""
     extra = list(extra or [])
-    BUILD.mkdir(exist_ok=True)
+    build_dir, lib_path = BUILD, LIB
+    if check:
+        extra.append("-DCRITMC_CHECK")
+        build_dir, lib_path = BUILD_CHECK, LIB_CHECK
+    build_dir.mkdir(exist_ok=True)
     sources = sorted(CSRC.glob("*.cu"))
     newest_header = max((p.stat().st_mtime for p in _headers()), default=0.0)
     jobs = []
     objects = []
     for src in sources:
-        obj = BUILD / (src.stem + ".o")
+        obj = build_dir / (src.stem + ".o")
         objects.append(obj)
         stale = (
             force
@@ -85,17 +95,17 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
                 f.result()
         if verbose:
             print(f"compiled {[s.name for s, _ in jobs]}")
-    if jobs or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objects):
-        tmp = LIB.with_suffix(".so.tmp")
+    if jobs or not lib_path.exists() or lib_path.stat().st_mtime < max(o.stat().st_mtime for o in objects):
+        tmp = lib_path.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objects), "-lcudart"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
     import sys
 
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, check="--check" in sys.argv))

@@ -12,6 +12,8 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libcritmc_b200.so"
+# CRITMC_B200_CHECK=1 loads the bounds-checked flavour (built on first use)
+LIB_CHECK_PATH = PKG / "libcritmc_b200_check.so"
 
 _lib: ctypes.CDLL | None = None
 
@@ -25,6 +27,7 @@ _D = ctypes.c_double
 SIGNATURES: dict[str, tuple] = {
     "critmc_version": (_I32, []),
     "critmc_last_error": (_I32, [_P, _I32]),
+    "critmc_check_report": (_I64, [_P, _I32]),
     "critmc_ising_class_table": (_I32, [_I32, _I32, _D, _D, _P, _P, _P]),
     "critmc_ising_msc_scratch_bytes": (_I64, [_I32, _I32]),
     "critmc_ising_msc_run": (
@@ -89,6 +92,15 @@ SIGNATURES: dict[str, tuple] = {
     "critmc_batch_poll": (_I32, [_P, _P, _P, _I32, _P]),
     "critmc_batch_cancel": (_I32, [_P, ctypes.c_int64]),
     "critmc_batch_pending": (_I32, [_P]),
+    "critmc_control_create": (_I32, [_P]),
+    "critmc_control_destroy": (_I32, [_P]),
+    "critmc_control_arm": (_I32, [_P, _I64]),
+    "critmc_control_cancel": (_I32, [_P]),
+    "critmc_control_status": (_I32, [_P]),
+    "critmc_control_wait": (_I32, [_P, _P]),
+    "critmc_ea_campaign_run_ctl": (
+        _I32, [_P, _I32, _I32, _I32, _P, _P, _I32, _U32, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
+    "critmc_run_items_ctl": (_I32, [_P, _I32, _P, _I64, _P, _I32, _P, _P]),
     "critmc_ea_campaign_buffer_bytes": (_I64, [_I32, _I64]),
     "critmc_ea_campaign_run": (
         _I32, [_P, _I32, _I32, _I32, _P, _P, _I32, _U32, _I32, _I32, _I32, _P, _I64, _P, _P]),
@@ -113,13 +125,16 @@ def lib() -> ctypes.CDLL:
     """Load the shared library (once)."""
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
+        check = os.environ.get("CRITMC_B200_CHECK", "") not in ("", "0")
+        path = LIB_CHECK_PATH if check else LIB_PATH
+        if not path.exists():
             if os.environ.get("CRITMC_B200_NO_BUILD"):
-                raise RuntimeError(f"{LIB_PATH} is missing; build it with python -m critmc_b200._build")
+                raise RuntimeError(f"{path} is missing; build it with python -m critmc_b200._build"
+                                   + (" --check" if check else ""))
             from . import _build
 
-            _build.build()
-        L = ctypes.CDLL(str(LIB_PATH))
+            _build.build(check=check)
+        L = ctypes.CDLL(str(path))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)
             fn.restype = res
@@ -153,6 +168,7 @@ HOST_ONLY = frozenset({
     "critmc_potts_tables", "critmc_pt_swap_table", "critmc_ea_coupling_bits", "critmc_on_grid_scratch_bytes",
     "critmc_graph_cache_set_capacity", "critmc_cluster_scratch_bytes", "critmc_stream_state_bytes",
     "critmc_ea_campaign_buffer_bytes", "critmc_graph_cache_size",
+    "critmc_control_arm", "critmc_control_cancel", "critmc_control_status",
 })
 
 

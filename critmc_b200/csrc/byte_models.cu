@@ -47,6 +47,8 @@ struct ByteParams {
 
 // Everything one thread block needs to advance one byte-lattice chain.
 struct ByteChain {
+  const RunCtl* ctl = nullptr;  // bounded run (work items), polled between measurements
+  CtlPoll* poll = nullptr;
   int8_t* gl;            // lattice in HBM, [colour][slot]
   long long* running;    // Ising: (E_b, M); Potts: E
   long long* counts;     // Potts: [q]
@@ -69,6 +71,7 @@ template <int MODEL, int Z>
 __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
   __shared__ long long red[16];
   __shared__ int cnt[128];
+  __shared__ int s_stop;
   const ByteGeom& g = a.g;
   const uint32_t k0 = a.k0, k1 = a.k1;
   const size_t n_sites = 2 * (size_t)g.slots;
@@ -86,6 +89,11 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
   long long m_run = (MODEL == MODEL_ISING) ? a.running[1] : 0;
   uint32_t sweep = a.sweep0;
   for (int meas = 0; meas < a.n_meas; ++meas) {
+    if (a.ctl) {  // stop between measurements when the budget or a cancel says so
+      if (tid == 0) s_stop = a.poll->check(*a.ctl);
+      __syncthreads();
+      if (s_stop) break;
+    }
     long long dE = 0, dM = 0, nacc = 0;
     for (int row = 0; row < a.n_rows; ++row) {
       const int code = a.codes[row];
@@ -101,11 +109,11 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
             byte_neighbours<Z>(g, c, r, i, nb);
             const critmc_u32x4 rnd =
                 critmc_philox4x32(s, sweep, CRITMC_TAG_SITE | ((uint32_t)c << 16), 0u, k0, k1);
-            const int old = own[s];
+            const int old = own[CRITMC_IDX(s, g.slots)];
             if constexpr (MODEL == MODEL_ISING) {
               int field = 0;
 #pragma unroll
-              for (int k = 0; k < Z; ++k) field += other[nb[k]];
+              for (int k = 0; k < Z; ++k) field += other[CRITMC_IDX(nb[k], g.slots)];
               const int sb = old > 0;
               int v;
               if (slot_alg == 0) v = (Z - old * field) / 2;  // anti-aligned neighbours
@@ -124,7 +132,7 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
             } else {
               int nbs[Z];
 #pragma unroll
-              for (int k = 0; k < Z; ++k) nbs[k] = other[nb[k]];
+              for (int k = 0; k < Z; ++k) nbs[k] = other[CRITMC_IDX(nb[k], g.slots)];
               int nw;
               if (slot_alg == 0) {
                 // propose a uniformly chosen different state (potts.py:53-56)
@@ -422,17 +430,23 @@ __device__ __forceinline__ int byte_geom_device(const critmc_item& it, ByteGeom&
 }
 
 __global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_item* items, int n,
-                                                                  unsigned* queue, size_t smem) {
+                                                                  unsigned* queue, size_t smem, RunCtl ctl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int cur;
+  CtlPoll poll;
+  poll.start();
   for (;;) {
-    if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+    if (threadIdx.x == 0) cur = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
     __syncthreads();
     const int i = cur;
     __syncthreads();
     if (i >= n) break;
     const critmc_item& it = items[i];
     ByteChain a;
+    if (ctl.status) {
+      a.ctl = &ctl;
+      a.poll = &poll;
+    }
     byte_geom_device(it, a.g);
     a.gl = reinterpret_cast<int8_t*>(it.spins);
     a.running = reinterpret_cast<long long*>(it.running);
@@ -466,7 +480,8 @@ __global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_i
   }
 }
 
-int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
+int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+                      cudaStream_t s) {
   if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(byte_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
@@ -476,7 +491,7 @@ int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t s
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
-  byte_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem);
+  byte_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem, ctl);
   if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }

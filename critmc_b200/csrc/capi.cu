@@ -3,8 +3,19 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
+#include "common.cuh"
 #include "host_common.h"
+
+// A bounded-run control: one page of pinned host memory mapped into the
+// device, [0] the cancel word (host writes), [1] the status word (kernels
+// write), plus the per-block time budget of the runs it is passed to.
+struct critmc_control {
+  unsigned* host = nullptr;
+  unsigned* dev = nullptr;
+  unsigned long long budget_ns = 0;
+};
 
 namespace critmc {
 
@@ -104,9 +115,126 @@ int CaptureStream::finish() {
 
 }  // namespace critmc
 
+namespace {
+
+struct CheckReader {
+  const char* file;
+  int (*read)(critmc::CheckRecord*);
+};
+std::vector<CheckReader>& check_readers() {
+  static std::vector<CheckReader> r;
+  return r;
+}
+
+}  // namespace
+
+int critmc::check_register(const char* file, int (*read_and_clear)(CheckRecord*)) {
+  check_readers().push_back(CheckReader{file, read_and_clear});
+  return 0;
+}
+
+extern "C" int64_t critmc_check_report(char* buf, int32_t size) {
+  critmc::clear_error();
+  if (buf && size > 0) buf[0] = 0;
+#ifndef CRITMC_CHECK
+  return -1;  // not a bounds-checked build
+#else
+  int64_t hits = 0;
+  size_t used = 0;
+  for (const CheckReader& r : check_readers()) {
+    critmc::CheckRecord rec;
+    if (r.read(&rec) != 0) return critmc::cuda_fail("read check record");
+    if (!rec.hits) continue;
+    hits += rec.hits;
+    if (buf && size > 0 && used + 1 < (size_t)size) {
+      const char* base = std::strrchr(r.file, '/');
+      used += (size_t)std::snprintf(buf + used, (size_t)size - used, "%s:%d index %llu of %llu (%u bad); ",
+                                    base ? base + 1 : r.file, rec.line, rec.index, rec.extent, rec.hits);
+      if (used >= (size_t)size) used = (size_t)size - 1;
+    }
+  }
+  return hits;
+#endif
+}
+
+critmc::RunCtl critmc::control_device(const critmc_control* ctl) {
+  RunCtl r{nullptr, nullptr, 0ull};
+  if (ctl && ctl->dev) {
+    r.cancel = ctl->dev;
+    r.status = reinterpret_cast<int*>(ctl->dev + 1);
+    r.budget_ns = ctl->budget_ns;
+  }
+  return r;
+}
+
 using namespace critmc;
 
 extern "C" int32_t critmc_version(void) { return 100; }
+
+extern "C" int32_t critmc_control_create(critmc_control** ctl) {
+  clear_error();
+  if (!ctl) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  *ctl = nullptr;
+  critmc_control* c = new critmc_control();
+  void* h = nullptr;
+  if (cudaHostAlloc(&h, 64, cudaHostAllocMapped) != cudaSuccess) {
+    delete c;
+    return cuda_fail("pinned control page");
+  }
+  void* d = nullptr;
+  if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+    cudaFreeHost(h);
+    delete c;
+    return cuda_fail("device view of the control page");
+  }
+  c->host = static_cast<unsigned*>(h);
+  c->dev = static_cast<unsigned*>(d);
+  std::memset(c->host, 0, 64);
+  *ctl = c;
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_control_destroy(critmc_control* ctl) {
+  if (!ctl) return CRITMC_OK;
+  if (ctl->host) cudaFreeHost(ctl->host);
+  delete ctl;
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_control_arm(critmc_control* ctl, int64_t budget_ns) {
+  clear_error();
+  if (!ctl || !ctl->host) return fail(CRITMC_ERR_INVALID, "null control");
+  if (budget_ns < 0) return fail(CRITMC_ERR_INVALID, "budget_ns must not be negative");
+  volatile unsigned* w = ctl->host;
+  w[0] = 0;
+  w[1] = 0;
+  ctl->budget_ns = (unsigned long long)budget_ns;
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_control_cancel(critmc_control* ctl) {
+  clear_error();
+  if (!ctl || !ctl->host) return fail(CRITMC_ERR_INVALID, "null control");
+  volatile unsigned* w = ctl->host;
+  w[0] = 1;
+  return CRITMC_OK;
+}
+
+extern "C" int32_t critmc_control_status(const critmc_control* ctl) {
+  if (!ctl || !ctl->host) return CRITMC_ERR_INVALID;
+  const volatile int* w = reinterpret_cast<const volatile int*>(ctl->host + 1);
+  return *w;
+}
+
+extern "C" int32_t critmc_control_wait(const critmc_control* ctl, void* stream) {
+  clear_error();
+  if (!ctl || !ctl->host) return fail(CRITMC_ERR_INVALID, "null control");
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return cuda_fail("synchronize");
+  const int st = critmc_control_status(ctl);
+  if (st == CRITMC_ERR_TIMEOUT) set_error("a bounded run ran out of its time budget; its outputs are incomplete");
+  if (st == CRITMC_ERR_CANCELLED) set_error("a bounded run was cancelled; its outputs are incomplete");
+  return st;
+}
 
 extern "C" int32_t critmc_graph_cache_set_capacity(int32_t entries) {
   if (entries < 0) return CRITMC_ERR_INVALID;

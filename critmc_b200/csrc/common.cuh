@@ -82,6 +82,95 @@ __device__ __forceinline__ unsigned long long as_ull(long long v) {
 }
 
 // ---------------------------------------------------------------------------
+// Bounds-checked builds (-DCRITMC_CHECK).  CRITMC_IDX(i, n) compares an index
+// with the extent of its array.  An index out of range is recorded (the first
+// one per translation unit: source line, index and extent, plus a count of
+// every bad index) and replaced by 0, so the access stays inside the array and
+// the kernel runs on: a check never traps.  critmc_check_report() reads and
+// clears the records of every translation unit.  Release builds compile the
+// checks away.
+// ---------------------------------------------------------------------------
+struct CheckRecord {
+  int line;
+  unsigned int hits;
+  unsigned long long index, extent;
+};
+// host: adds a translation unit's reader to the report (returns 0)
+int check_register(const char* file, int (*read_and_clear)(CheckRecord*));
+
+#ifdef CRITMC_CHECK
+static __device__ CheckRecord g_check_record;
+__device__ __forceinline__ size_t check_index(size_t i, size_t n, int line) {
+  if (i < n) return i;
+  if (atomicAdd(&g_check_record.hits, 1u) == 0) {
+    g_check_record.line = line;
+    g_check_record.index = i;
+    g_check_record.extent = n;
+  }
+  return 0;
+}
+static int check_read_and_clear(CheckRecord* out) {
+  if (cudaMemcpyFromSymbol(out, g_check_record, sizeof(CheckRecord)) != cudaSuccess) return -1;
+  const CheckRecord zero{0, 0u, 0ull, 0ull};
+  if (cudaMemcpyToSymbol(g_check_record, &zero, sizeof(CheckRecord)) != cudaSuccess) return -1;
+  return 0;
+}
+static const int g_check_registered = check_register(__FILE__, &check_read_and_clear);
+#define CRITMC_IDX(i, n) ::critmc::check_index((size_t)(i), (size_t)(n), __LINE__)
+#else
+#define CRITMC_IDX(i, n) (i)
+#endif
+
+// ---------------------------------------------------------------------------
+// Bounded runs of the persistent kernels (critmc_control).  One thread per
+// block polls: the block's elapsed time against the budget every time, and the
+// host-mapped cancel and status words at most every CTL_POLL_NS (each read
+// crosses the bus).  A block that must stop records why in the status word
+// (first reason wins) and leaves its work; the others see the status word on
+// their next poll.  No wait in here: a poll never blocks.
+// ---------------------------------------------------------------------------
+struct RunCtl {
+  const volatile unsigned* cancel;  // host-mapped; nonzero = cancel (null: unbounded run)
+  int* status;                      // host-mapped; 0, CRITMC_ERR_TIMEOUT or CRITMC_ERR_CANCELLED
+  unsigned long long budget_ns;     // per-block run time budget, 0 = none
+};
+
+constexpr unsigned long long CTL_POLL_NS = 100000ull;
+
+// device view of a critmc_control (all null for an unbounded run); host code
+RunCtl control_device(const critmc_control* ctl);
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+struct CtlPoll {
+  unsigned long long t0, last;
+  __device__ __forceinline__ void start() { t0 = last = global_ns(); }
+  // 0 to go on, else the status that stops the block
+  __device__ __forceinline__ int check(const RunCtl& c) {
+    if (!c.status) return 0;
+    const unsigned long long now = global_ns();
+    if (c.budget_ns && now - t0 > c.budget_ns) {
+      atomicCAS_system(c.status, 0, CRITMC_ERR_TIMEOUT);
+      return CRITMC_ERR_TIMEOUT;
+    }
+    if (now - last >= CTL_POLL_NS) {
+      last = now;
+      if (*c.cancel) {
+        atomicCAS_system(c.status, 0, CRITMC_ERR_CANCELLED);
+        return CRITMC_ERR_CANCELLED;
+      }
+      const int st = *(volatile int*)c.status;
+      if (st) return st;
+    }
+    return 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Error reporting from kernels: the first failing kernel writes its code.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void report_error(int* err, int code) {

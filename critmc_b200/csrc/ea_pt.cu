@@ -169,7 +169,7 @@ inline size_t ea_smem_bytes(const ByteGeom& g, int dim, int lx) {
 // All PT steps of one sample by one thread block.  key[set] = Philox key of replica set.
 template <int Z>
 __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, const uint32_t (&key)[2][2],
-                              unsigned char* smem_raw) {
+                              unsigned char* smem_raw, const RunCtl& ctl, CtlPoll& poll) {
   constexpr int DIM = Z / 2;
   const ByteGeom& g = S.g;
   const uint32_t n_sites = 2 * g.slots;
@@ -186,6 +186,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   __shared__ int conf[2][32], lab[2][32];
   __shared__ double acc_s[32][EA_NOBS];
   __shared__ unsigned long long sw_acc[32], sw_try[32], lhist[32][2], trip[2];
+  __shared__ int s_stop;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m = C.m;
@@ -211,6 +212,11 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   int bin = 0;
   long long next_edge = 1;
   for (int t = 0; t < C.n_steps; ++t) {
+    if (ctl.status) {  // bounded run: stop between steps when the budget or a cancel says so
+      if (tid == 0) s_stop = poll.check(ctl);
+      __syncthreads();
+      if (s_stop) break;
+    }
     if (t >= next_edge) {
       // flush the finished bin (critmc glass.py:114-122)
       if (tid < m)
@@ -470,7 +476,9 @@ __global__ void __launch_bounds__(EA_THREADS) ea_pt_kernel(const __grid_constant
   const int lsample = blockIdx.x;
   const uint32_t key[2][2] = {{P.keys[lsample][0][0], P.keys[lsample][0][1]},
                               {P.keys[lsample][1][0], P.keys[lsample][1][1]}};
-  ea_sample_run<Z>(P.C, P.S, P.sample0 + lsample, key, smem_raw);
+  CtlPoll poll;
+  poll.start();
+  ea_sample_run<Z>(P.C, P.S, P.sample0 + lsample, key, smem_raw, RunCtl{nullptr, nullptr, 0ull}, poll);
 }
 
 // A campaign: samples of several lattice sizes in one persistent launch.  Work
@@ -482,14 +490,17 @@ struct EaCampaignParams {
   const uint32_t* work;
   unsigned* queue;
   int n_work;
+  RunCtl ctl;  // bounded run (null words: unbounded)
 };
 
 template <int Z>
 __global__ void __launch_bounds__(EA_THREADS, 3) ea_campaign_kernel(const __grid_constant__ EaCampaignParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int cur;
+  CtlPoll poll;
+  poll.start();
   for (;;) {
-    if (threadIdx.x == 0) cur = (int)atomicAdd(P.queue, 1u);
+    if (threadIdx.x == 0) cur = poll.check(P.ctl) ? P.n_work : (int)atomicAdd(P.queue, 1u);
     __syncthreads();
     const int w = cur;
     __syncthreads();
@@ -498,7 +509,7 @@ __global__ void __launch_bounds__(EA_THREADS, 3) ea_campaign_kernel(const __grid
     const int sample = (int)(P.work[w] & 0xFFFFFFu);
     const uint32_t* k = S.keys + (size_t)sample * 4;
     const uint32_t key[2][2] = {{k[0], k[1]}, {k[2], k[3]}};
-    ea_sample_run<Z>(P.C, S, sample, key, smem_raw);
+    ea_sample_run<Z>(P.C, S, sample, key, smem_raw, P.ctl, poll);
     __syncthreads();
   }
 }
@@ -686,10 +697,20 @@ extern "C" int32_t critmc_ea_campaign_run(const critmc_ea_size* sizes, int32_t n
                                           const double* betas, const uint32_t* swap_thr, int32_t swap_width,
                                           uint32_t t0, int32_t n_steps, int32_t n_bins, int32_t sweeps_per_step,
                                           void* buffer, int64_t buffer_bytes, void* staging, void* stream) {
+  return critmc_ea_campaign_run_ctl(sizes, n_sizes, dim, m, betas, swap_thr, swap_width, t0, n_steps, n_bins,
+                                    sweeps_per_step, buffer, buffer_bytes, staging, nullptr, stream);
+}
+
+extern "C" int32_t critmc_ea_campaign_run_ctl(const critmc_ea_size* sizes, int32_t n_sizes, int32_t dim,
+                                              int32_t m, const double* betas, const uint32_t* swap_thr,
+                                              int32_t swap_width, uint32_t t0, int32_t n_steps, int32_t n_bins,
+                                              int32_t sweeps_per_step, void* buffer, int64_t buffer_bytes,
+                                              void* staging, critmc_control* ctl, void* stream) {
   clear_error();
   if (!sizes || n_sizes < 1 || n_sizes > 255) return fail(CRITMC_ERR_INVALID, "need 1..255 lattice sizes");
   if (!buffer) return fail(CRITMC_ERR_INVALID, "null pointer argument");
   EaCampaignParams P;
+  P.ctl = control_device(ctl);
   int st = ea_common(P.C, dim, m, betas, swap_thr, swap_width, t0, n_steps, n_bins, sweeps_per_step);
   if (st) return st;
   std::vector<EaSet> sets(n_sizes);

@@ -152,7 +152,14 @@ int family_streams(int dev, FamilyStreams*& out) {
 extern "C" int32_t critmc_run_items(const critmc_item* items, int32_t n_items, void* buffer,
                                     int64_t buffer_bytes, void* staging, int32_t smem_limit,
                                     void* stream) {
+  return critmc_run_items_ctl(items, n_items, buffer, buffer_bytes, staging, smem_limit, nullptr, stream);
+}
+
+extern "C" int32_t critmc_run_items_ctl(const critmc_item* items, int32_t n_items, void* buffer,
+                                        int64_t buffer_bytes, void* staging, int32_t smem_limit,
+                                        critmc_control* ctl, void* stream) {
   clear_error();
+  const RunCtl rc = control_device(ctl);
   if (n_items < 0) return fail(CRITMC_ERR_INVALID, "n_items must not be negative");
   if (n_items == 0) return CRITMC_OK;
   if (!items || !buffer) return fail(CRITMC_ERR_INVALID, "null pointer argument");
@@ -208,9 +215,10 @@ extern "C" int32_t critmc_run_items(const critmc_item* items, int32_t n_items, v
     }
     int st = CRITMC_OK;
     const critmc_item* first = sorted + offset;
-    if (f == 0) st = msc_items_launch(dev_items + offset, count[f], queues + f, smem[f], fstream);
-    else if (f == 1) st = byte_items_launch(dev_items + offset, count[f], queues + f, smem[f], fstream);
-    else st = on_items_launch(dev_items + offset, count[f], first->q_or_n, first->dim, queues + f, smem[f], fstream);
+    if (f == 0) st = msc_items_launch(dev_items + offset, count[f], queues + f, smem[f], rc, fstream);
+    else if (f == 1) st = byte_items_launch(dev_items + offset, count[f], queues + f, smem[f], rc, fstream);
+    else st = on_items_launch(dev_items + offset, count[f], first->q_or_n, first->dim, queues + f, smem[f], rc,
+                              fstream);
     if (st) return st;
     if (fs) {
       if (cudaEventRecord(fs->join[f], fstream) != cudaSuccess) return cuda_fail("event record");

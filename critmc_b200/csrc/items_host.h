@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "common.cuh"
 #include "critmc_b200.h"
 
 namespace critmc {
@@ -11,10 +12,13 @@ constexpr int ITEM_THREADS = 512;
 
 // Each launcher starts a persistent kernel over `n` items at `items` (device)
 // whose blocks pull item indices from *queue (zeroed by the caller).
-int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
-int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s);
+// `ctl` bounds the run (all null: unbounded).
+int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+                     cudaStream_t s);
+int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+                      cudaStream_t s);
 // O(n): all n items share n_comp and dim (one kernel per variant)
 int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem,
-                    cudaStream_t s);
+                    const RunCtl& ctl, cudaStream_t s);
 
 }  // namespace critmc

@@ -70,13 +70,13 @@ __device__ __forceinline__ void msc_fixup(const MscRule<Z, RULE>& rule, const Ms
   uint32_t n[Z];
   msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
   MscWord w;
-  rule.classify(own[f.w], n, w);
+  rule.classify(own[CRITMC_IDX(f.w, g.words)], n, w);
   w.D = f.D;
   w.U = f.U;
   for (int grp = KG; grp < 8 && w.U != 0; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, f.w, sweep, col, grp);
   const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
   msc_obs<Z>((w.s ^ s_new) & f.U, w.s, w.anti, dE, dM, nacc);
-  own[f.w] = s_new;
+  own[CRITMC_IDX(f.w, g.words)] = s_new;
 }
 
 // One colour of one sweep.  grid: x = column/run tiles, y = chain of the launch.
@@ -104,6 +104,14 @@ __global__ void __launch_bounds__(MSC_THREADS, 4)
   const uint32_t lt_mask = (1u << lane) - 1u;
   int nf = 0;  // entries in this warp's list (warp-uniform)
   int dE = 0, dM = 0, nacc = 0;
+  // uniform part of the plane stream and, for the rules with few threshold
+  // classes, the broadcast threshold bits of the inline planes
+  critmc_plane_stream ps;
+  critmc_plane_stream_init(&ps, k0, k1, sweep, col, KG);
+  constexpr int NR = MscRule<Z, RULE>::NR;
+  constexpr bool PRE = NR > 0 && NR <= 2;
+  uint32_t pre[4 * KG][PRE ? NR : 1];
+  if constexpr (PRE) rule.template prepare<KG>(pre);
 
   auto flush = [&]() {
     __syncwarp();
@@ -118,8 +126,8 @@ __global__ void __launch_bounds__(MSC_THREADS, 4)
   if constexpr (Z == 4) {
     if (r0 < g.rows) {
       const int ym = (r0 == 0) ? g.ly - 1 : r0 - 1;
-      o_m = other[(size_t)ym * g.wc + k];
-      o_c = other[(size_t)r0 * g.wc + k];
+      o_m = other[CRITMC_IDX((size_t)ym * g.wc + k, g.words)];
+      o_c = other[CRITMC_IDX((size_t)r0 * g.wc + k, g.words)];
     }
   }
 #pragma unroll 1
@@ -135,10 +143,10 @@ __global__ void __launch_bounds__(MSC_THREADS, 4)
       if constexpr (Z == 4) {
         const int y = r;
         const int yp = (y == g.ly - 1) ? 0 : y + 1;
-        const uint32_t o_p = other[(size_t)yp * g.wc + k];
+        const uint32_t o_p = other[CRITMC_IDX((size_t)yp * g.wc + k, g.words)];
         const int p = (P.col + y) & 1;
         const int ka = p ? ((k == g.wc - 1) ? 0 : k + 1) : ((k == 0) ? g.wc - 1 : k - 1);
-        const uint32_t adj = other[(size_t)y * g.wc + ka];
+        const uint32_t adj = other[CRITMC_IDX((size_t)y * g.wc + ka, g.words)];
         n[0] = o_c;
         n[1] = p ? __funnelshift_r(o_c, adj, 1) : __funnelshift_l(adj, o_c, 1);
         n[2] = o_m;
@@ -150,12 +158,15 @@ __global__ void __launch_bounds__(MSC_THREADS, 4)
         msc_row_coords<Z>(g, widx, y, z, kk);
         msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
       }
-      rule.classify(own[widx], n, w);
+      rule.classify(own[CRITMC_IDX(widx, g.words)], n, w);
+      const critmc_plane_word_t pw = critmc_plane_word(&ps, widx);
 #pragma unroll
-      for (int grp = 0; grp < KG; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, widx, sweep, col, grp);
+      for (int grp = 0; grp < KG; ++grp)
+        msc_resolve<Z, RULE>(rule, w, critmc_plane_group(&ps, pw, grp), grp,
+                             PRE ? &pre[4 * grp][0] : nullptr);
       s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
       msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, dE, dM, nacc);
-      if (w.U == 0) own[widx] = s_new;
+      if (w.U == 0) own[CRITMC_IDX(widx, g.words)] = s_new;
     }
     const uint32_t need = __ballot_sync(0xffffffffu, w.U != 0);
     if (need) {
@@ -811,8 +822,10 @@ __device__ void msci_colour(const MscRule<Z, RULE>& rule, const MscGeom& g, uint
 }
 
 template <int Z>
-__device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[64]) {
+__device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[64], const RunCtl* ctl,
+                           CtlPoll* poll) {
   __shared__ long long red[MSCI_WARPS];
+  __shared__ int s_stop;
   MscGeom g;
   msc_geom_device(it.dim, it.lx, it.ly, it.lz, g);
   uint32_t* gl = reinterpret_cast<uint32_t*>(it.spins);
@@ -822,6 +835,11 @@ __device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[6
   long long e_run = it.running[0], m_run = it.running[1];
   uint32_t sweep = it.sweep0;
   for (int meas = 0; meas < it.n_meas; ++meas) {
+    if (ctl) {  // stop between measurements when the budget or a cancel says so
+      if (tid == 0) s_stop = poll->check(*ctl);
+      __syncthreads();
+      if (s_stop) break;
+    }
     long long dE = 0, dM = 0, nacc = 0;
     for (int row = 0; row < it.n_rows; ++row) {
       const int slot = it.codes[row] == CRITMC_HEATBATH ? 1 : 0;
@@ -878,24 +896,28 @@ __device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[6
 }
 
 __global__ void __launch_bounds__(ITEM_THREADS) msc_items_kernel(const critmc_item* items, int n,
-                                                                 unsigned* queue) {
+                                                                 unsigned* queue, RunCtl ctl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ MscFix fix[MSCI_WARPS][64];
   __shared__ int cur;
   uint32_t* lat = reinterpret_cast<uint32_t*>(smem_raw);
+  CtlPoll poll;
+  poll.start();
+  const RunCtl* pc = ctl.status ? &ctl : nullptr;
   for (;;) {
-    if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+    if (threadIdx.x == 0) cur = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
     __syncthreads();
     const int i = cur;
     __syncthreads();
     if (i >= n) break;
     const critmc_item& it = items[i];
-    if (it.dim == 2) msci_chain<4>(it, lat, fix);
-    else msci_chain<6>(it, lat, fix);
+    if (it.dim == 2) msci_chain<4>(it, lat, fix, pc, &poll);
+    else msci_chain<6>(it, lat, fix, pc, &poll);
   }
 }
 
-int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
+int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+                     cudaStream_t s) {
   if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(msc_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
@@ -905,7 +927,7 @@ int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t sm
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
-  msc_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue);
+  msc_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, ctl);
   if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }

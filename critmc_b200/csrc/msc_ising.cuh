@@ -61,29 +61,28 @@ __device__ __forceinline__ uint32_t mux(uint32_t sel, uint32_t a, uint32_t b) {
 template <int Z>
 __device__ __forceinline__ void msc_neighbours(const uint32_t* __restrict__ other, const MscGeom& g,
                                                int col, int y, int z, int k, uint32_t* n) {
-  const int r = y + g.ly * z;
-  const uint32_t* row = other + (size_t)r * g.wc;
-  const uint32_t same = row[k];
+  const size_t r = (size_t)(y + g.ly * z) * g.wc;
+  const uint32_t same = other[CRITMC_IDX(r + k, g.words)];
   const int p = (col + y + z) & 1;
   uint32_t sh;
   if (p == 0) {
     const int km = (k == 0) ? g.wc - 1 : k - 1;
-    sh = __funnelshift_l(row[km], same, 1);  // site index i-1 lives one bit lower
+    sh = __funnelshift_l(other[CRITMC_IDX(r + km, g.words)], same, 1);  // site index i-1 lives one bit lower
   } else {
     const int kp = (k == g.wc - 1) ? 0 : k + 1;
-    sh = __funnelshift_r(same, row[kp], 1);  // site index i+1 lives one bit higher
+    sh = __funnelshift_r(same, other[CRITMC_IDX(r + kp, g.words)], 1);  // site index i+1 lives one bit higher
   }
   const int ym = (y == 0) ? g.ly - 1 : y - 1;
   const int yp = (y == g.ly - 1) ? 0 : y + 1;
   n[0] = same;
   n[1] = sh;
-  n[2] = other[(size_t)(ym + g.ly * z) * g.wc + k];
-  n[3] = other[(size_t)(yp + g.ly * z) * g.wc + k];
+  n[2] = other[CRITMC_IDX((size_t)(ym + g.ly * z) * g.wc + k, g.words)];
+  n[3] = other[CRITMC_IDX((size_t)(yp + g.ly * z) * g.wc + k, g.words)];
   if constexpr (Z == 6) {
     const int zm = (z == 0) ? g.lz - 1 : z - 1;
     const int zp = (z == g.lz - 1) ? 0 : z + 1;
-    n[4] = other[(size_t)(y + g.ly * zm) * g.wc + k];
-    n[5] = other[(size_t)(y + g.ly * zp) * g.wc + k];
+    n[4] = other[CRITMC_IDX((size_t)(y + g.ly * zm) * g.wc + k, g.words)];
+    n[5] = other[CRITMC_IDX((size_t)(y + g.ly * zp) * g.wc + k, g.words)];
   }
 }
 
@@ -216,6 +215,23 @@ struct MscRule {
     }
   }
 };
+
+// Compare planes 4 g .. 4 g + 3 (random bits r) for the undecided lanes of w.
+template <int Z, int RULE>
+__device__ __forceinline__ void msc_resolve(const MscRule<Z, RULE>& rule, MscWord& w, const critmc_u32x4& r,
+                                            int grp, const uint32_t* pre) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t t;
+    if constexpr (MscRule<Z, RULE>::NR > 0) {
+      t = pre ? rule.tbits_pre(w, pre + q * MscRule<Z, RULE>::NR) : rule.tbits(w, 31 - (4 * grp + q));
+    } else {
+      t = rule.tbits(w, 31 - (4 * grp + q));
+    }
+    w.D |= w.U & t & ~r.v[q];
+    w.U &= ~(r.v[q] ^ t);
+  }
+}
 
 // Resolve plane group `grp` (planes 4 grp .. 4 grp + 3) for the undecided lanes.
 // pre: broadcast threshold bits of these four planes (pre[q * NR + v]) or null.

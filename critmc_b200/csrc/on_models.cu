@@ -147,9 +147,9 @@ __device__ __forceinline__ int on_site(float* lat, const ByteGeom& g, int c, uin
   for (int k = 0; k < N; ++k) {
     float acc = 0.0f;
 #pragma unroll
-    for (int q = 0; q < Z; ++q) acc += oth[k][nb[q]];
+    for (int q = 0; q < Z; ++q) acc += oth[k][CRITMC_IDX(nb[q], g.slots)];
     h[k] = acc;
-    sv[k] = own[k][s];
+    sv[k] = own[k][CRITMC_IDX(s, g.slots)];
   }
   if (code == CRITMC_OVERRELAX) {
     // on.py:141-183: reflect about the local field; keep the spin if h = 0
@@ -326,6 +326,8 @@ __device__ __forceinline__ void on_write_sum(double* e_out, double* m_out, doubl
 
 // Everything one thread block needs to advance one O(n) chain.
 struct OnChain {
+  const RunCtl* ctl = nullptr;  // bounded run (work items), polled between measurements
+  CtlPoll* poll = nullptr;
   float* gl;          // the chain's spins in HBM
   double* e_out;      // [n_meas]
   double* m_out;      // [n_meas][N]
@@ -353,6 +355,7 @@ template <int N, int Z>
 __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
   constexpr int NV = on_nv<N, Z>();
   __shared__ long long red[NV][ON_THREADS / 32];
+  __shared__ int s_stop;
   const ByteGeom& g = P.g;
   const size_t n_sites = 2 * (size_t)g.slots;
   float* gl = P.gl;
@@ -366,6 +369,11 @@ __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
   uint32_t sweep = P.sweep0;
 
   for (int meas = 0; meas < P.n_meas; ++meas) {
+    if (P.ctl) {  // stop between measurements when the budget or a cancel says so
+      if (tid == 0) s_stop = P.poll->check(*P.ctl);
+      __syncthreads();
+      if (s_stop) break;
+    }
     long long nacc = 0;
     for (int row = 0; row < P.n_rows; ++row) {
       const int code = P.codes[row];
@@ -769,17 +777,23 @@ namespace critmc {
 // kernel holding all of them would be held to the largest.
 template <int N, int Z>
 __global__ void __launch_bounds__(ON_THREADS) on_items_kernel(const critmc_item* items, int n,
-                                                              unsigned* queue, size_t smem) {
+                                                              unsigned* queue, size_t smem, RunCtl ctl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int cur;
+  CtlPoll poll;
+  poll.start();
   for (;;) {
-    if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+    if (threadIdx.x == 0) cur = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
     __syncthreads();
     const int i = cur;
     __syncthreads();
     if (i >= n) break;
     const critmc_item& it = items[i];
     OnChain a;
+    if (ctl.status) {
+      a.ctl = &ctl;
+      a.poll = &poll;
+    }
     a.g.dim = it.dim;
     a.g.lx = it.lx;
     a.g.ly = it.dim >= 2 ? it.ly : 1;
@@ -809,7 +823,8 @@ __global__ void __launch_bounds__(ON_THREADS) on_items_kernel(const critmc_item*
 }
 
 template <int N, int Z>
-static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, size_t smem, cudaStream_t s) {
+static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+                              cudaStream_t s) {
   auto kern = on_items_kernel<N, Z>;
   if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -820,20 +835,20 @@ static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, 
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
-  kern<<<grid, ON_THREADS, smem, s>>>(items, n, queue, smem);
+  kern<<<grid, ON_THREADS, smem, s>>>(items, n, queue, smem, ctl);
   if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }
 
 int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem,
-                    cudaStream_t s) {
+                    const RunCtl& ctl, cudaStream_t s) {
   switch (n_comp * 10 + dim) {
-    case 21: return on_items_launch_nz<2, 2>(items, n, queue, smem, s);
-    case 22: return on_items_launch_nz<2, 4>(items, n, queue, smem, s);
-    case 23: return on_items_launch_nz<2, 6>(items, n, queue, smem, s);
-    case 31: return on_items_launch_nz<3, 2>(items, n, queue, smem, s);
-    case 32: return on_items_launch_nz<3, 4>(items, n, queue, smem, s);
-    case 33: return on_items_launch_nz<3, 6>(items, n, queue, smem, s);
+    case 21: return on_items_launch_nz<2, 2>(items, n, queue, smem, ctl, s);
+    case 22: return on_items_launch_nz<2, 4>(items, n, queue, smem, ctl, s);
+    case 23: return on_items_launch_nz<2, 6>(items, n, queue, smem, ctl, s);
+    case 31: return on_items_launch_nz<3, 2>(items, n, queue, smem, ctl, s);
+    case 32: return on_items_launch_nz<3, 4>(items, n, queue, smem, ctl, s);
+    case 33: return on_items_launch_nz<3, 6>(items, n, queue, smem, ctl, s);
     default: return fail(CRITMC_ERR_INVALID, "O(n) items need n = 2 or 3 and dim 1..3");
   }
 }

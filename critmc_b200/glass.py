@@ -283,8 +283,10 @@ class MultiSizeCampaign:
         return sum(c.n_samples * 2 * len(c.temperatures) * c.lattice.n_sites * c.sweeps_per_step
                    for c in self.campaigns)
 
-    def launch(self, n_bins: int, n_steps: int | None = None, stream=None) -> list[dict]:
-        """Enqueue ``n_steps`` PT steps of every sample (no synchronisation); returns the outputs."""
+    def launch(self, n_bins: int, n_steps: int | None = None, stream=None, control=None) -> list[dict]:
+        """Enqueue ``n_steps`` PT steps of every sample (no synchronisation); returns the outputs.
+
+        ``control``: an armed ``RunControl`` bounding the launch (None: runs to completion)."""
         n_steps = (1 << n_bins) - 1 if n_steps is None else int(n_steps)
         c0 = self.campaigns[0]
         outs = [c._outputs(n_bins) for c in self.campaigns]
@@ -297,19 +299,25 @@ class MultiSizeCampaign:
             z.label_hist, z.trips = ptr(o["label_hist"]), ptr(o["trips"])
             z.lx, z.ly, z.lz = dims
             z.n_samples = c.n_samples
-        _lib.call_on(self.device, "critmc_ea_campaign_run", ctypes.cast(sizes, ctypes.c_void_p), len(self.campaigns),
-                     c0.lattice.dim, len(c0.temperatures), c0.betas.ctypes.data, ptr(c0.swap_thr), SWAP_WIDTH,
-                     c0.step, n_steps, n_bins, c0.sweeps_per_step, ptr(self._buffer), self._bytes,
-                     self._staging.data_ptr(), stream if stream is not None else stream_handle(self.device))
+        _lib.call_on(self.device, "critmc_ea_campaign_run_ctl", ctypes.cast(sizes, ctypes.c_void_p),
+                     len(self.campaigns), c0.lattice.dim, len(c0.temperatures), c0.betas.ctypes.data,
+                     ptr(c0.swap_thr), SWAP_WIDTH, c0.step, n_steps, n_bins, c0.sweeps_per_step, ptr(self._buffer),
+                     self._bytes, self._staging.data_ptr(), control.handle if control is not None else None,
+                     stream if stream is not None else stream_handle(self.device))
         for c in self.campaigns:
             c.step += n_steps
         return outs
 
-    def run(self, n_bins: int, n_steps: int | None = None) -> list[list[TemperingRun]]:
-        """Run every size; returns one list of ``TemperingRun`` per campaign."""
+    def run(self, n_bins: int, n_steps: int | None = None, control=None) -> list[list[TemperingRun]]:
+        """Run every size; returns one list of ``TemperingRun`` per campaign.
+
+        With an armed ``control`` the launch is bounded: ``RunStopped`` is raised
+        when it ran out of its budget or was cancelled (outputs incomplete)."""
         t0 = time.perf_counter()
-        outs = self.launch(n_bins, n_steps)
+        outs = self.launch(n_bins, n_steps, control=control)
         torch.cuda.synchronize(self.device)
+        if control is not None:
+            control.wait(raise_on_stop=True)
         wall = time.perf_counter() - t0
         return [c._collect(o, n_bins, wall) for c, o in zip(self.campaigns, outs)]
 

@@ -141,11 +141,12 @@ class ItemRun:
 
 
 def launch_items(items, device, buffer: torch.Tensor | None, *, staging: torch.Tensor | None = None,
-                 smem_limit: int = 0, stream=None) -> torch.Tensor:
+                 smem_limit: int = 0, stream=None, control=None) -> torch.Tensor:
     """Run a ctypes array (or list) of ``CritmcItem``; returns the (grown) descriptor buffer.
 
     ``staging``: pinned host bytes for the asynchronous descriptor copy (see
-    ``critmc_run_items``); ``None`` copies from pageable memory.
+    ``critmc_run_items``); ``None`` copies from pageable memory.  ``control``:
+    an armed ``RunControl`` bounding the launch (None: runs to completion).
     """
     n = len(items)
     if n == 0:
@@ -157,12 +158,16 @@ def launch_items(items, device, buffer: torch.Tensor | None, *, staging: torch.T
     if staging is not None and staging.numel() < n * ctypes.sizeof(CritmcItem):
         raise ValueError("staging buffer too small")
     st = stream if stream is not None else stream_handle(device)
-    _lib.call_on(device, "critmc_run_items", ctypes.cast(arr, ctypes.c_void_p), n, ptr(buffer), int(need),
-                 staging.data_ptr() if staging is not None else None, int(smem_limit), st)
+    _lib.call_on(device, "critmc_run_items_ctl", ctypes.cast(arr, ctypes.c_void_p), n, ptr(buffer), int(need),
+                 staging.data_ptr() if staging is not None else None, int(smem_limit),
+                 control.handle if control is not None else None, st)
     return buffer
 
 
 def run_items(runs: list[ItemRun], device, *, smem_limit: int = 0, buffer: torch.Tensor | None = None,
-              stream=None) -> torch.Tensor:
-    """Launch all ``runs`` in one call; returns the descriptor buffer (reuse it)."""
-    return launch_items([r.item for r in runs], device, buffer, smem_limit=smem_limit, stream=stream)
+              stream=None, control=None) -> torch.Tensor:
+    """Launch all ``runs`` in one call; returns the descriptor buffer (reuse it).
+
+    ``control``: an armed ``RunControl`` bounding the launch (see ``critmc_b200.control``)."""
+    return launch_items([r.item for r in runs], device, buffer, smem_limit=smem_limit, stream=stream,
+                        control=control)

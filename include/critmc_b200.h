@@ -55,6 +55,15 @@ extern "C" {
 /* library version (major*10000 + minor*100 + patch) */
 int32_t critmc_version(void);
 
+/* Bounds-checked builds (compiled with -DCRITMC_CHECK, e.g. python -m
+ * critmc_b200._build --check): the hot kernels compare their lattice indices
+ * with the array extents, record the first bad index of every source file and
+ * access element 0 instead, without trapping.  Returns the number of bad
+ * indices seen since the last call (and clears the records), with one
+ * "file:line index i of n" entry per file in buf; -1 in a release build.
+ * No counterpart in critmc (numba's boundscheck option plays this role).   */
+int64_t critmc_check_report(char* buf, int32_t size);
+
 /* copy the last error message of the calling thread (always NUL-terminated) */
 int32_t critmc_last_error(char* buf, int32_t size);
 
@@ -253,6 +262,41 @@ int32_t critmc_ea_campaign_run(const critmc_ea_size* sizes, int32_t n_sizes, int
                                uint32_t t0, int32_t n_steps, int32_t n_bins, int32_t sweeps_per_step,
                                void* buffer, int64_t buffer_bytes, void* staging, void* stream);
 
+/* ---- bounded runs of the persistent kernels ----------------------------------
+ * A critmc_control is a page of pinned host memory mapped into the device: a
+ * cancel word the host sets and a status word the kernels set.  The _ctl
+ * variants of the persistent entry points take one (NULL = unbounded, the
+ * plain entry points).  One thread of every block polls between steps (EA) or
+ * measurements (items): its block's elapsed time (globaltimer) against the
+ * budget at every poll, the host-mapped words at most every 100 us.  A block
+ * over budget writes CRITMC_ERR_TIMEOUT, a block that sees the cancel word
+ * writes CRITMC_ERR_CANCELLED (the first reason stays); every block then
+ * leaves its work at its next poll, so the kernel returns on its own and the
+ * device stays usable.  The outputs and device state of a run that stopped
+ * are incomplete (samples or items part-way): restore the state saved before
+ * the call.  No counterpart in critmc (its kernels run to completion).
+ * create/destroy: allocate / free the page (not while a run uses it).
+ * arm: clear both words and set the budget in ns (0 = none) for the next
+ *   runs; only while no run using it is in flight.
+ * cancel: set the cancel word (any host thread, while runs are in flight).
+ * status: the status word now (0 while nothing stopped).
+ * wait: synchronise `stream`, then return the status word as the status
+ *   (CRITMC_OK, CRITMC_ERR_TIMEOUT or CRITMC_ERR_CANCELLED).               */
+typedef struct critmc_control critmc_control;
+int32_t critmc_control_create(critmc_control** ctl);
+int32_t critmc_control_destroy(critmc_control* ctl);
+int32_t critmc_control_arm(critmc_control* ctl, int64_t budget_ns);
+int32_t critmc_control_cancel(critmc_control* ctl);
+int32_t critmc_control_status(const critmc_control* ctl);
+int32_t critmc_control_wait(const critmc_control* ctl, void* stream);
+
+/* critmc_ea_campaign_run under a control (the step loop of every sample polls it). */
+int32_t critmc_ea_campaign_run_ctl(const critmc_ea_size* sizes, int32_t n_sizes, int32_t dim, int32_t m,
+                                   const double* betas, const uint32_t* swap_thr, int32_t swap_width,
+                                   uint32_t t0, int32_t n_steps, int32_t n_bins, int32_t sweeps_per_step,
+                                   void* buffer, int64_t buffer_bytes, void* staging, critmc_control* ctl,
+                                   void* stream);
+
 /* ---- heterogeneous work items (continuous batching, serving) --------------
  * One item advances one chain by n_meas schedule applications: any model and
  * lattice size, its own beta, key and sweep counter.  critmc_run_items runs
@@ -310,6 +354,12 @@ int64_t critmc_items_buffer_bytes(int32_t n_items);
  * (larger lattices are updated in HBM); 0 picks 200 KiB.                    */
 int32_t critmc_run_items(const critmc_item* items, int32_t n_items, void* buffer,
                          int64_t buffer_bytes, void* staging, int32_t smem_limit, void* stream);
+
+/* critmc_run_items under a control (see critmc_control): every block polls it
+ * before it takes an item and between the measurements of its item.        */
+int32_t critmc_run_items_ctl(const critmc_item* items, int32_t n_items, void* buffer,
+                             int64_t buffer_bytes, void* staging, int32_t smem_limit, critmc_control* ctl,
+                             void* stream);
 
 /* ---- cluster updates (Swendsen-Wang, Wolff) ----------------------------------
  * One cluster update of n_chains Ising or Potts chains.  bits: 1 for the

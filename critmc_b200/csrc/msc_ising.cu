@@ -60,7 +60,7 @@ __device__ __forceinline__ void msc_row_coords(const MscGeom& g, uint32_t w, int
 
 // Finish one deferred word: continue the MSB-first comparison plane group by
 // plane group until every lane is decided, then store it.
-template <int Z, int RULE, int KG>
+template <int Z, int RULE, int KG, int PR>
 __device__ __forceinline__ void msc_fixup(const MscRule<Z, RULE>& rule, const MscGeom& g,
                                           const MscFix f, uint32_t* own, const uint32_t* other,
                                           uint32_t col, uint32_t k0, uint32_t k1, uint32_t sweep,
@@ -73,15 +73,16 @@ __device__ __forceinline__ void msc_fixup(const MscRule<Z, RULE>& rule, const Ms
   rule.classify(own[CRITMC_IDX(f.w, g.words)], n, w);
   w.D = f.D;
   w.U = f.U;
-  for (int grp = KG; grp < 8 && w.U != 0; ++grp) msc_group<Z, RULE>(rule, w, k0, k1, f.w, sweep, col, grp);
+  for (int grp = KG; grp < 8 && w.U != 0; ++grp) msc_group<Z, RULE, PR>(rule, w, k0, k1, f.w, sweep, col, grp);
   const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
   msc_obs<Z>((w.s ^ s_new) & f.U, w.s, w.anti, dE, dM, nacc);
   own[CRITMC_IDX(f.w, g.words)] = s_new;
 }
 
 // One colour of one sweep.  grid: x = column/run tiles, y = chain of the launch.
-// Thread t walks `run` consecutive rows of column k = t mod wc.
-template <int Z, int RULE, int KG>
+// Thread t walks `run` consecutive rows of column k = t mod wc.  PR: Philox
+// rounds of the acceptance planes (10, or 7 when the caller asks for it).
+template <int Z, int RULE, int KG, int PR>
 __global__ void __launch_bounds__(MSC_THREADS, 4)
     msc_halfsweep_kernel(const __grid_constant__ MscParams P) {
   __shared__ MscFix fix[MSC_WARPS][MSC_FIXCAP];
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(MSC_THREADS, 4)
   auto flush = [&]() {
     __syncwarp();
     for (int e = lane; e < nf; e += 32)
-      msc_fixup<Z, RULE, KG>(rule, g, fix[warp][e], own, other, col, k0, k1, sweep, dE, dM, nacc);
+      msc_fixup<Z, RULE, KG, PR>(rule, g, fix[warp][e], own, other, col, k0, k1, sweep, dE, dM, nacc);
     __syncwarp();
     nf = 0;
   };
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(MSC_THREADS, 4)
       const critmc_plane_word_t pw = critmc_plane_word(&ps, widx);
 #pragma unroll
       for (int grp = 0; grp < KG; ++grp)
-        msc_resolve<Z, RULE>(rule, w, critmc_plane_group(&ps, pw, grp), grp,
+        msc_resolve<Z, RULE>(rule, w, critmc_plane_group_rounds(&ps, pw, grp, PR), grp,
                              PRE ? &pre[4 * grp][0] : nullptr);
       s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
       msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, dE, dM, nacc);
@@ -345,32 +346,38 @@ int msc_pick_rule(const uint32_t* kind, const uint32_t* thr, int z, int algo, in
   return RULE_GEN;
 }
 
-template <int Z, int RULE>
+template <int Z, int RULE, int PR>
 static void launch_half_kg(const MscParams& P, int kg, cudaStream_t st) {
   const long long threads = (long long)P.g.wc * ((P.g.rows + P.run - 1) / P.run);
   const dim3 grid((unsigned)((threads + MSC_THREADS - 1) / MSC_THREADS), P.n_chains - P.chain0 < MSC_PCHAINS ? P.n_chains - P.chain0 : MSC_PCHAINS);
-  if (kg == 1) msc_halfsweep_kernel<Z, RULE, 1><<<grid, MSC_THREADS, 0, st>>>(P);
-  else msc_halfsweep_kernel<Z, RULE, 2><<<grid, MSC_THREADS, 0, st>>>(P);
+  if (kg == 1) msc_halfsweep_kernel<Z, RULE, 1, PR><<<grid, MSC_THREADS, 0, st>>>(P);
+  else msc_halfsweep_kernel<Z, RULE, 2, PR><<<grid, MSC_THREADS, 0, st>>>(P);
 }
 
-template <int Z>
+template <int Z, int PR>
 static void launch_half_z(const MscParams& P, int rule, int kg, cudaStream_t st) {
   switch (rule) {
-    case RULE_METRO0: launch_half_kg<Z, RULE_METRO0>(P, kg, st); break;
-    case RULE_HB0: launch_half_kg<Z, RULE_HB0>(P, kg, st); break;
-    case RULE_GEN: launch_half_kg<Z, RULE_GEN>(P, kg, st); break;
-    default: launch_half_kg<Z, RULE_GENSPIN>(P, kg, st); break;
+    case RULE_METRO0: launch_half_kg<Z, RULE_METRO0, PR>(P, kg, st); break;
+    case RULE_HB0: launch_half_kg<Z, RULE_HB0, PR>(P, kg, st); break;
+    case RULE_GEN: launch_half_kg<Z, RULE_GEN, PR>(P, kg, st); break;
+    default: launch_half_kg<Z, RULE_GENSPIN, PR>(P, kg, st); break;
   }
 }
 
 // One half-sweep of every chain, in launches of at most MSC_PCHAINS chains.
-void msc_launch_half(MscParams& P, const uint32_t* keys, int rule, int kg, cudaStream_t st) {
+// pr: Philox rounds of the acceptance planes (10, or 7 on request).
+void msc_launch_half(MscParams& P, const uint32_t* keys, int rule, int kg, int pr, cudaStream_t st) {
   for (int c0 = 0; c0 < P.n_chains; c0 += MSC_PCHAINS) {
     P.chain0 = c0;
     const int nc = std::min(MSC_PCHAINS, P.n_chains - c0);
     std::memcpy(P.keys, keys + 2 * (size_t)c0, sizeof(uint32_t) * 2 * nc);
-    if (P.g.dim == 2) launch_half_z<4>(P, rule, kg, st);
-    else launch_half_z<6>(P, rule, kg, st);
+    if (pr == 7) {
+      if (P.g.dim == 2) launch_half_z<4, 7>(P, rule, kg, st);
+      else launch_half_z<6, 7>(P, rule, kg, st);
+    } else {
+      if (P.g.dim == 2) launch_half_z<4, CRITMC_PHILOX_ROUNDS>(P, rule, kg, st);
+      else launch_half_z<6, CRITMC_PHILOX_ROUNDS>(P, rule, kg, st);
+    }
   }
 }
 
@@ -410,7 +417,9 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
     sweeps_per_meas += reps;
   }
   const int run_code = (mode >> 8) & 0xF;  // tuning: rows walked per thread, 2^(code-1); 0 = automatic
-  if ((mode & ~0xFFF) || run_code > 6) return fail(CRITMC_ERR_INVALID, "mode: bits 8..11 must be 0..6, no higher bits");
+  if ((mode & ~0x1FFF) || run_code > 6)
+    return fail(CRITMC_ERR_INVALID, "mode: bits 8..11 must be 0..6, bit 12 selects Philox4x32-7, no higher bits");
+  const int pr = (mode & CRITMC_MSC_PHILOX7) ? 7 : CRITMC_PHILOX_ROUNDS;  // a stream choice, not a tuning knob
   mode &= 0xFF;
   if (mode == 0) mode = 3;
   if (mode != 1 && mode != 3) return fail(CRITMC_ERR_UNSUPPORTED, "mode must be 0, 1 or 3");
@@ -471,9 +480,9 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
         q.sweep = sw;
         q.meas = meas_rel;
         q.col = 0;
-        msc_launch_half(q, keys, rule[slot], kg, s);
+        msc_launch_half(q, keys, rule[slot], kg, pr, s);
         q.col = 1;
-        msc_launch_half(q, keys, rule[slot], kg, s);
+        msc_launch_half(q, keys, rule[slot], kg, pr, s);
         ++sw;
       }
     }
@@ -496,7 +505,7 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
       int dev = 0;
       cudaGetDevice(&dev);
       GraphKey key;
-      key.add(0x4d534347u).add(dev).add(G).add(n_rows).add(rule).add(kg);
+      key.add(0x4d534347u).add(dev).add(G).add(n_rows).add(rule).add(kg).add(pr);
       key.add_bytes(schedule, sizeof(int64_t) * 2 * n_rows).add_bytes(keys, sizeof(uint32_t) * 2 * n_chains);
       for (int slot = 0; slot < 2; ++slot) {
         MscParams& q = P[slot];
@@ -734,9 +743,9 @@ extern "C" int32_t critmc_ising_msc_run_noalloc(uint32_t* spins, int32_t dim, in
         P[slot].sweep = sw;
         P[slot].meas = (uint32_t)meas;
         P[slot].col = 0;
-        msc_launch_half(P[slot], keys, rule[slot], k_inline / 4, s);
+        msc_launch_half(P[slot], keys, rule[slot], k_inline / 4, CRITMC_PHILOX_ROUNDS, s);
         P[slot].col = 1;
-        msc_launch_half(P[slot], keys, rule[slot], k_inline / 4, s);
+        msc_launch_half(P[slot], keys, rule[slot], k_inline / 4, CRITMC_PHILOX_ROUNDS, s);
         ++sw;
       }
     }

@@ -235,12 +235,13 @@ __device__ __forceinline__ void msc_resolve(const MscRule<Z, RULE>& rule, MscWor
 
 // Resolve plane group `grp` (planes 4 grp .. 4 grp + 3) for the undecided lanes.
 // pre: broadcast threshold bits of these four planes (pre[q * NR + v]) or null.
-template <int Z, int RULE>
+// PR: Philox rounds of the planes (10; 7 only when a caller asks for it).
+template <int Z, int RULE, int PR = CRITMC_PHILOX_ROUNDS>
 __device__ __forceinline__ void msc_group(const MscRule<Z, RULE>& rule, MscWord& w, uint32_t k0,
                                           uint32_t k1, uint32_t widx, uint32_t sweep, uint32_t col,
                                           int grp, const uint32_t* pre = nullptr) {
-  const critmc_u32x4 r = critmc_philox4x32(
-      widx, sweep, CRITMC_TAG_PLANES | ((uint32_t)grp << 8) | (col << 16), 0u, k0, k1);
+  const critmc_u32x4 r = critmc_philox4x32_rounds(
+      widx, sweep, CRITMC_TAG_PLANES | ((uint32_t)grp << 8) | (col << 16), 0u, k0, k1, PR);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     uint32_t t;

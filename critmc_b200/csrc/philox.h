@@ -50,12 +50,15 @@ typedef struct {
   uint32_t v[4];
 } critmc_u32x4;
 
-CRITMC_HD critmc_u32x4 critmc_philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
-                                         uint32_t k0, uint32_t k1) {
+/* Philox4x32 with `rounds` rounds: 10 is the library's stream everywhere;
+ * 7 (Salmon et al.'s smallest round count that passes BigCrush) is offered
+ * only as an explicit option of the multi-spin-coded acceptance planes. */
+CRITMC_HD critmc_u32x4 critmc_philox4x32_rounds(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                uint32_t k0, uint32_t k1, int rounds) {
 #if defined(__CUDA_ARCH__)
 #pragma unroll
 #endif
-  for (int r = 0; r < CRITMC_PHILOX_ROUNDS; ++r) {
+  for (int r = 0; r < rounds; ++r) {
     /* one 32x32->64 product per lane word: a single wide multiply-add on the GPU */
     const uint64_t p0 = (uint64_t)CRITMC_PHILOX_M0 * c0;
     const uint64_t p1 = (uint64_t)CRITMC_PHILOX_M1 * c2;
@@ -72,6 +75,11 @@ CRITMC_HD critmc_u32x4 critmc_philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, 
   out.v[2] = c2;
   out.v[3] = c3;
   return out;
+}
+
+CRITMC_HD critmc_u32x4 critmc_philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                         uint32_t k0, uint32_t k1) {
+  return critmc_philox4x32_rounds(c0, c1, c2, c3, k0, k1, CRITMC_PHILOX_ROUNDS);
 }
 
 /* ---------------------------------------------------------------------------
@@ -137,8 +145,11 @@ CRITMC_HD critmc_plane_word_t critmc_plane_word(const critmc_plane_stream* ps, u
   return pw;
 }
 
-/* planes 4 g .. 4 g + 3 of a word (word q of the result is plane 4 g + q) */
-CRITMC_HD critmc_u32x4 critmc_plane_group(const critmc_plane_stream* ps, critmc_plane_word_t pw, int g) {
+/* planes 4 g .. 4 g + 3 of a word (word q of the result is plane 4 g + q), for a
+ * Philox of `rounds` rounds (3 .. CRITMC_PHILOX_ROUNDS; the stream object holds
+ * the keys of the longest) */
+CRITMC_HD critmc_u32x4 critmc_plane_group_rounds(const critmc_plane_stream* ps, critmc_plane_word_t pw, int g,
+                                                 int rounds) {
   uint32_t c0 = pw.h1 ^ ps->x1[g]; /* state after round 1 */
   uint32_t c1 = pw.l1;
   uint32_t c2 = pw.v3 ^ ps->x2[g];
@@ -151,7 +162,7 @@ CRITMC_HD critmc_u32x4 critmc_plane_group(const critmc_plane_stream* ps, critmc_
 #if defined(__CUDA_ARCH__)
 #pragma unroll
 #endif
-  for (int r = 0; r < CRITMC_PHILOX_ROUNDS - 3; ++r) {
+  for (int r = 0; r < rounds - 3; ++r) {
     p0 = (uint64_t)CRITMC_PHILOX_M0 * c0;
     p1 = (uint64_t)CRITMC_PHILOX_M1 * c2;
     c0 = (uint32_t)(p1 >> 32) ^ c1 ^ ps->rk0[r];
@@ -165,6 +176,10 @@ CRITMC_HD critmc_u32x4 critmc_plane_group(const critmc_plane_stream* ps, critmc_
   out.v[2] = c2;
   out.v[3] = c3;
   return out;
+}
+
+CRITMC_HD critmc_u32x4 critmc_plane_group(const critmc_plane_stream* ps, critmc_plane_word_t pw, int g) {
+  return critmc_plane_group_rounds(ps, pw, g, CRITMC_PHILOX_ROUNDS);
 }
 
 /* uniform double in [0, 1) with 53 random bits from two words */

@@ -40,7 +40,7 @@ class IsingEnsemble:
 
     def __init__(self, lattice: Lattice | int, betas, chains_per_beta: int, *, h: float = 0.0,
                  seed: int = 0, start: str = "random", device=None, mode: int = 0,
-                 k_inline: int = 8, tune: bool = False):
+                 k_inline: int = 8, tune: bool = False, philox_rounds: int = 10):
         self.lattice = square(lattice) if isinstance(lattice, int) else lattice
         shape = tuple(self.lattice.shape)
         if not (_msc_ok(shape) and self.lattice.bipartite):
@@ -55,6 +55,11 @@ class IsingEnsemble:
         self.shape = shape
         self.dims = shape + (1,) * (3 - len(shape))
         self.mode, self.k_inline = mode, k_inline
+        if philox_rounds not in (10, 7):
+            raise ValueError("philox_rounds is 10 (the library's stream) or 7 (the optional reduced-round planes)")
+        # a different random stream, not a tuning knob: the acceptance planes from Philox4x32-7
+        self.philox_rounds = philox_rounds
+        self._stream_bits = 0x1000 if philox_rounds == 7 else 0
         L = shape[0]
         keys = [philox_key(make_rng(seed, "ising", L, b, c))
                 for b in range(len(self.betas)) for c in range(self.chains_per_beta)]
@@ -119,8 +124,8 @@ class IsingEnsemble:
         lx, ly, lz = self.dims
         _lib.call_on(dev, "critmc_ising_msc_run", ptr(self.words), len(self.shape), lx, ly, lz, n,
                      self.keys.ctypes.data, self.tables.ctypes.data, len(self.betas), self.sweep, sched.ctypes.data,
-                     len(sched), n_meas, ptr(self.running), ptr(e), ptr(m), ptr(aux), ptr(self._scratch), self.mode,
-                     self.k_inline, stream_handle(dev))
+                     len(sched), n_meas, ptr(self.running), ptr(e), ptr(m), ptr(aux), ptr(self._scratch),
+                     self.mode | self._stream_bits, self.k_inline, stream_handle(dev))
         self.sweep += int(sched[:, 1].sum()) * n_meas
         if not host:
             return EnsembleSeries(e, m, aux)

@@ -98,8 +98,14 @@ int32_t critmc_ising_class_table(int32_t algo, int32_t z, double beta, double h,
  * mode: 0 auto, 1 one launch per half-sweep, 3 = 1 replayed as CUDA graphs;
  * plus, in bits 8..11, v = 1..6 for 2^(v-1) rows walked per thread (0 =
  * automatic).  Both are tuning knobs (critmc_b200.autotune picks them).
+ * Bit 12 (CRITMC_MSC_PHILOX7) is not a tuning knob: it draws the acceptance
+ * planes from Philox4x32-7 instead of Philox4x32-10 (same counters), a
+ * different random stream that the CPU oracle replays with rounds = 7.  Off by
+ * default; 7 rounds is the smallest count Salmon et al. (SC'11) report as
+ * passing BigCrush.
  * k_inline: 4 or 8 acceptance planes resolved inline (tuning only; the
  * results do not depend on it).                                            */
+#define CRITMC_MSC_PHILOX7 0x1000
 int64_t critmc_ising_msc_scratch_bytes(int32_t n_chains, int32_t n_meas);
 int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
                              int32_t n_chains, const uint32_t* keys, const uint32_t* tables,

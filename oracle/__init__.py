@@ -57,6 +57,10 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_ising_bond_energy.restype = ctypes.c_int64
     L.oracle_ising_msc_run.argtypes = [_P, _I, _I, _I, _I, _P, _P, _U32, _P, _I, _I, _P, _P, _P, _P]
     L.oracle_ising_msc_run.restype = _I
+    L.oracle_ising_msc_run_rounds.argtypes = [_P, _I, _I, _I, _I, _P, _P, _U32, _P, _I, _I, _P, _P, _P, _P, _I]
+    L.oracle_ising_msc_run_rounds.restype = _I
+    L.oracle_philox_rounds.argtypes = [_P, _P, _P, _I]
+    L.oracle_philox_rounds.restype = None
     L.oracle_ising_byte_run.argtypes = [_P, _I, _I, _I, _I, _P, _P, _U32, _P, _I, _I, _P, _P, _P, _P]
     L.oracle_ising_byte_run.restype = _I
     L.oracle_potts_tables.argtypes = [_I, _D, _P, _P]
@@ -160,6 +164,14 @@ def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
 
+def philox_rounds(ctr, key, rounds: int) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().oracle_philox_rounds(_ptr(c), _ptr(k), _ptr(out), int(rounds))
+    return out
+
+
 def philox(ctr, key) -> np.ndarray:
     c = np.ascontiguousarray(ctr, dtype=np.uint32)
     k = np.ascontiguousarray(key, dtype=np.uint32)
@@ -183,9 +195,10 @@ def ising_bond_energy(s: np.ndarray, shape: tuple[int, ...]) -> int:
     return int(lib().oracle_ising_bond_energy(_ptr(s8), len(shape), *dims))
 
 
-def ising_msc_run(s, shape, key, beta, h, schedule, n_meas, sweep0=0, running=None):
+def ising_msc_run(s, shape, key, beta, h, schedule, n_meas, sweep0=0, running=None, rounds=10):
     """Replay the MSC checkerboard sweeps on ``s`` (int8, reference site order, modified).
 
+    ``rounds``: Philox rounds of the acceptance planes (10, or the optional 7).
     Returns ``(e_b, m, aux, running)``.
     """
     s8 = s if (isinstance(s, np.ndarray) and s.dtype == np.int8 and s.flags["C_CONTIGUOUS"]) else None
@@ -203,9 +216,9 @@ def ising_msc_run(s, shape, key, beta, h, schedule, n_meas, sweep0=0, running=No
     e = np.zeros(n_meas, dtype=np.int64)
     m = np.zeros(n_meas, dtype=np.int64)
     aux = np.zeros((n_meas, 4), dtype=np.int64)
-    rc = lib().oracle_ising_msc_run(
+    rc = lib().oracle_ising_msc_run_rounds(
         _ptr(s8), len(shape), *dims, _ptr(k), _ptr(tables), sweep0, _ptr(sched), len(sched), n_meas,
-        _ptr(running), _ptr(e), _ptr(m), _ptr(aux),
+        _ptr(running), _ptr(e), _ptr(m), _ptr(aux), int(rounds),
     )
     if rc != 0:
         raise ValueError(f"oracle_ising_msc_run failed ({rc})")

@@ -4,12 +4,17 @@
 #include <stdint.h>
 
 void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void oracle_philox_rounds(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4], int rounds);
 int oracle_ising_table(int algo, int z, double beta, double h, uint32_t* kind, uint32_t* thr);
 int64_t oracle_ising_bond_energy(const int8_t* s, int dim, int lx, int ly, int lz);
 int oracle_ising_msc_run(int8_t* s, int dim, int lx, int ly, int lz, const uint32_t key[2],
                          const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
                          int n_rows, int n_meas, int64_t* running, int64_t* e_out, int64_t* m_out,
                          int64_t* aux_out);
+int oracle_ising_msc_run_rounds(int8_t* s, int dim, int lx, int ly, int lz, const uint32_t key[2],
+                                const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
+                                int n_rows, int n_meas, int64_t* running, int64_t* e_out, int64_t* m_out,
+                                int64_t* aux_out, int rounds);
 int oracle_ising_byte_run(int8_t* s, int dim, int lx, int ly, int lz, const uint32_t key[2],
                           const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
                           int n_rows, int n_meas, int64_t* running, int64_t* e_out,

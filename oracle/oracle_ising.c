@@ -18,7 +18,8 @@
  * (x, y, z) has row r = y + ly z, row parity p = (c + y + z) & 1, in-row
  * index i = (x - p) / 2, word w = r * (lx / 64) + i / 32 and lane j = i % 32.
  * Bit (31 - q) of its u is bit j of Philox4x32-10 word (q % 4) of the call
- * with counter (w, sweep, 0x01 | (q / 4) << 8 | c << 16, 0).
+ * with counter (w, sweep, 0x01 | (q / 4) << 8 | c << 16, 0); the optional
+ * reduced-round planes use Philox4x32-7 with the same counters.
  *
  * Philox4x32-10 is implemented here independently of the library header,
  * from Salmon et al. (SC'11), and pinned against the Random123 known-answer
@@ -31,11 +32,11 @@
 
 #include "oracle.h"
 
-/* ---------------- Philox4x32-10 ---------------- */
-void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+/* ---------------- Philox4x32-R (R = 10 everywhere; 7 for the optional planes) ---------------- */
+void oracle_philox_rounds(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4], int rounds) {
   uint32_t x0 = ctr[0], x1 = ctr[1], x2 = ctr[2], x3 = ctr[3];
   uint32_t ka = key[0], kb = key[1];
-  for (int round = 0; round < 10; ++round) {
+  for (int round = 0; round < rounds; ++round) {
     uint64_t p0 = (uint64_t)0xD2511F53u * x0;
     uint64_t p1 = (uint64_t)0xCD9E8D57u * x2;
     uint32_t n0 = (uint32_t)(p1 >> 32) ^ x1 ^ ka;
@@ -51,6 +52,10 @@ void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]
   out[1] = x1;
   out[2] = x2;
   out[3] = x3;
+}
+
+void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  oracle_philox_rounds(ctr, key, out, 10);
 }
 
 /* ---------------- acceptance tables ----------------
@@ -150,6 +155,7 @@ int64_t oracle_ising_bond_energy(const int8_t* s, int dim, int lx, int ly, int l
 /* Planes of one word, computed four at a time on first use. */
 typedef struct {
   uint32_t w, sweep, col;
+  int rounds; /* Philox rounds of the planes: 10, or 7 when asked for */
   const uint32_t* key;
   uint32_t planes[32];
   unsigned have; /* bit g set: planes 4g..4g+3 computed */
@@ -159,7 +165,7 @@ static uint32_t plane(PlaneCache* pc, int q) {
   const unsigned grp = (unsigned)q >> 2;
   if (!(pc->have & (1u << grp))) {
     uint32_t ctr[4] = {pc->w, pc->sweep, 0x01u | (grp << 8) | (pc->col << 16), 0u}, out[4];
-    oracle_philox(ctr, pc->key, out);
+    oracle_philox_rounds(ctr, pc->key, out, pc->rounds);
     for (int k = 0; k < 4; ++k) pc->planes[4 * grp + k] = out[k];
     pc->have |= 1u << grp;
   }
@@ -183,10 +189,11 @@ static int decide(uint32_t kind, uint32_t thr, PlaneCache* pc, int j) {
 
 /* One checkerboard sweep; accumulates (dE_b, dM, changed) through the pointers. */
 static void msc_sweep(int8_t* s, const Geo* g, int algo, const uint32_t* kind, const uint32_t* thr,
-                      const uint32_t key[2], uint32_t sweep, int64_t* d_eb, int64_t* d_m,
+                      const uint32_t key[2], uint32_t sweep, int rounds, int64_t* d_eb, int64_t* d_m,
                       int64_t* changed) {
   const int wc = g->lx / 64;
   PlaneCache pc;
+  pc.rounds = rounds;
   pc.key = key;
   pc.sweep = sweep;
   for (int col = 0; col < 2; ++col) {
@@ -241,7 +248,16 @@ int oracle_ising_msc_run(int8_t* s, int dim, int lx, int ly, int lz, const uint3
                          const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
                          int n_rows, int n_meas, int64_t* running, int64_t* e_out, int64_t* m_out,
                          int64_t* aux_out) {
+  return oracle_ising_msc_run_rounds(s, dim, lx, ly, lz, key, tables, sweep0, schedule, n_rows, n_meas, running,
+                                     e_out, m_out, aux_out, 10);
+}
+
+int oracle_ising_msc_run_rounds(int8_t* s, int dim, int lx, int ly, int lz, const uint32_t key[2],
+                                const uint32_t* tables, uint32_t sweep0, const int64_t* schedule,
+                                int n_rows, int n_meas, int64_t* running, int64_t* e_out, int64_t* m_out,
+                                int64_t* aux_out, int rounds) {
   Geo g;
+  if (rounds < 1 || rounds > 16) return -1;
   if (dim < 2 || dim > 3 || lx % 64) return -1;
   g.dim = dim;
   g.lx = lx;
@@ -260,7 +276,7 @@ int oracle_ising_msc_run(int8_t* s, int dim, int lx, int ly, int lz, const uint3
       const uint32_t* kind = tables + algo_slot * 32;
       const uint32_t* thr = kind + 16;
       for (int64_t rep = 0; rep < schedule[2 * row + 1]; ++rep) {
-        msc_sweep(s, &g, code, kind, thr, key, sweep, &e_b, &m, &acc);
+        msc_sweep(s, &g, code, kind, thr, key, sweep, rounds, &e_b, &m, &acc);
         ++sweep;
       }
     }

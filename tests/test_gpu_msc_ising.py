@@ -105,3 +105,29 @@ def test_msc_measure_matches_host(cuda):
         e_b, mm = to_host(out)[0]
         assert e_b == Ising(lat).bond_energy(s)
         assert mm == int(s.astype(np.int64).sum())
+
+
+@pytest.mark.parametrize("shape,sched,beta", [
+    ((128, 8), [[0, 1], [2, 1]], 0.4406868),
+    ((64, 4, 6), [[0, 1]], 0.2216546),
+])
+@pytest.mark.parametrize("mode,k_inline", [(1, 8), (3, 4)])
+def test_msc_philox7_planes_replay(cuda, shape, sched, beta, mode, k_inline):
+    """The optional Philox4x32-7 acceptance planes (mode bit 12) follow the oracle with
+    rounds = 7, and are a different stream from the default Philox4x32-10."""
+    philox7 = 0x1000
+    rng = np.random.default_rng(77)
+    n = int(np.prod(shape))
+    s0 = (2 * rng.integers(0, 2, n) - 1).astype(np.int8)
+    key = rng.integers(0, 2**32, 2, dtype=np.uint64).astype(np.uint32)
+    raw, s_gpu, running = _run_gpu(cuda, shape, sched, beta, 0.0, s0, key, 12, mode | philox7, k_inline,
+                                   chunks=[5, 7])
+    s_ref = s0.copy()
+    e, m, aux, run = oracle.ising_msc_run(s_ref, shape, key, beta, 0.0, sched, 12, rounds=7)
+    np.testing.assert_array_equal(s_gpu, s_ref)
+    np.testing.assert_array_equal(raw["Eb"], e)
+    np.testing.assert_array_equal(raw["M"], m)
+    np.testing.assert_array_equal(raw["aux"], aux)
+    s10 = s0.copy()
+    e10, _, _, _ = oracle.ising_msc_run(s10, shape, key, beta, 0.0, sched, 12)
+    assert not np.array_equal(e, e10)

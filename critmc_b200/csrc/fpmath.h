@@ -6,10 +6,11 @@
  * atan2 and acos.  Library implementations differ between CUDA and the host
  * C library by an ulp or two, and the over-relaxation dynamics amplify such
  * differences exponentially, so a CPU replay could only follow the GPU for a
- * few sweeps.  These functions use only +, -, *, /, sqrt, rint and exponent
- * bit manipulation, so a translation unit compiled without floating-point
- * contraction (nvcc --fmad=false, gcc -ffp-contract=off) gives bit-identical
- * results on both sides.
+ * few sweeps.  These functions use only +, -, *, /, sqrt, rint, exponent
+ * bit manipulation and explicit fused multiply-adds (CM_FMAF / CM_FMA, one
+ * rounding, the same on both sides), so a translation unit compiled without
+ * implicit floating-point contraction (nvcc --fmad=false, gcc
+ * -ffp-contract=off) gives bit-identical results on both sides.
  *
  * Methods (textbook, e.g. J.-M. Muller, "Elementary Functions"): Cody-Waite
  * argument reduction with a three-part constant, then truncated Taylor
@@ -28,6 +29,17 @@
 #define CM_HD __host__ __device__ __forceinline__
 #else
 #define CM_HD static inline
+#endif
+
+/* Fused multiply-add, rounded once (IEEE fma): the same operation on both
+ * sides, so the Horner steps below cost one instruction each on the GPU and
+ * the host replay (C99 fmaf/fma, correctly rounded) gives the same bits. */
+#if defined(__CUDA_ARCH__)
+#define CM_FMAF(a, b, c) __fmaf_rn((a), (b), (c))
+#define CM_FMA(a, b, c) __fma_rn((a), (b), (c))
+#else
+#define CM_FMAF(a, b, c) fmaf((a), (b), (c))
+#define CM_FMA(a, b, c) fma((a), (b), (c))
 #endif
 
 CM_HD uint32_t cm_f2u(float x) {
@@ -70,19 +82,19 @@ CM_HD float cm_expf(float x) {
   if (x < -103.973f) return 0.0f;
   const float k = rintf(x * 1.44269502f); /* round(x / ln 2) */
   /* ln 2 = 0.693115234375 + 3.1933188e-05 + 1.2996507e-08 (first two: 12 bits) */
-  float r = x - k * 0.693115234375f;
-  r = r - k * 3.193318843841553e-05f;
-  r = r - k * 1.2996506981721723e-08f;
+  float r = CM_FMAF(-k, 0.693115234375f, x);
+  r = CM_FMAF(-k, 3.193318843841553e-05f, r);
+  r = CM_FMAF(-k, 1.2996506981721723e-08f, r);
   /* e^r, |r| <= 0.347: Taylor series to r^8 */
   float p = 2.48015873e-05f; /* 1/8! */
-  p = p * r + 1.98412698e-04f;
-  p = p * r + 1.38888889e-03f;
-  p = p * r + 8.33333333e-03f;
-  p = p * r + 4.16666667e-02f;
-  p = p * r + 1.66666667e-01f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
+  p = CM_FMAF(p, r, 1.98412698e-04f);
+  p = CM_FMAF(p, r, 1.38888889e-03f);
+  p = CM_FMAF(p, r, 8.33333333e-03f);
+  p = CM_FMAF(p, r, 4.16666667e-02f);
+  p = CM_FMAF(p, r, 1.66666667e-01f);
+  p = CM_FMAF(p, r, 0.5f);
+  p = CM_FMAF(p, r, 1.0f);
+  p = CM_FMAF(p, r, 1.0f);
   return cm_scale2(p, (int)k);
 }
 
@@ -115,22 +127,22 @@ CM_HD double cm_exp(double x) {
   if (x > 709.79) return INFINITY;
   if (x < -745.2) return 0.0;
   const double k = rint(x * 1.4426950408889634);
-  double r = x - k * 0x1.62e42fp-1;
-  r = r - k * 0x1.df473de6af279p-26;
+  double r = CM_FMA(-k, 0x1.62e42fp-1, x);
+  r = CM_FMA(-k, 0x1.df473de6af279p-26, r);
   double p = 1.0 / 6227020800.0; /* 1/13! */
-  p = p * r + 1.0 / 479001600.0;
-  p = p * r + 1.0 / 39916800.0;
-  p = p * r + 1.0 / 3628800.0;
-  p = p * r + 1.0 / 362880.0;
-  p = p * r + 1.0 / 40320.0;
-  p = p * r + 1.0 / 5040.0;
-  p = p * r + 1.0 / 720.0;
-  p = p * r + 1.0 / 120.0;
-  p = p * r + 1.0 / 24.0;
-  p = p * r + 1.0 / 6.0;
-  p = p * r + 0.5;
-  p = p * r + 1.0;
-  p = p * r + 1.0;
+  p = CM_FMA(p, r, 1.0 / 479001600.0);
+  p = CM_FMA(p, r, 1.0 / 39916800.0);
+  p = CM_FMA(p, r, 1.0 / 3628800.0);
+  p = CM_FMA(p, r, 1.0 / 362880.0);
+  p = CM_FMA(p, r, 1.0 / 40320.0);
+  p = CM_FMA(p, r, 1.0 / 5040.0);
+  p = CM_FMA(p, r, 1.0 / 720.0);
+  p = CM_FMA(p, r, 1.0 / 120.0);
+  p = CM_FMA(p, r, 1.0 / 24.0);
+  p = CM_FMA(p, r, 1.0 / 6.0);
+  p = CM_FMA(p, r, 0.5);
+  p = CM_FMA(p, r, 1.0);
+  p = CM_FMA(p, r, 1.0);
   return cm_scale2d(p, (int)k);
 }
 
@@ -171,16 +183,16 @@ CM_HD double cm_log(double x) {
   const double s = f / (m + 1.0);
   const double z = s * s;
   double p = 1.0 / 23.0;
-  p = p * z + 1.0 / 21.0;
-  p = p * z + 1.0 / 19.0;
-  p = p * z + 1.0 / 17.0;
-  p = p * z + 1.0 / 15.0;
-  p = p * z + 1.0 / 13.0;
-  p = p * z + 1.0 / 11.0;
-  p = p * z + 1.0 / 9.0;
-  p = p * z + 1.0 / 7.0;
-  p = p * z + 1.0 / 5.0;
-  p = p * z + 1.0 / 3.0;
+  p = CM_FMA(p, z, 1.0 / 21.0);
+  p = CM_FMA(p, z, 1.0 / 19.0);
+  p = CM_FMA(p, z, 1.0 / 17.0);
+  p = CM_FMA(p, z, 1.0 / 15.0);
+  p = CM_FMA(p, z, 1.0 / 13.0);
+  p = CM_FMA(p, z, 1.0 / 11.0);
+  p = CM_FMA(p, z, 1.0 / 9.0);
+  p = CM_FMA(p, z, 1.0 / 7.0);
+  p = CM_FMA(p, z, 1.0 / 5.0);
+  p = CM_FMA(p, z, 1.0 / 3.0);
   /* log m = 2 s + 2 s z p, written as f - (f - 2 s) + ... to keep f's bits:
    * 2 s = f - s f, so log m = f - s (f - 2 z p) */
   const double lm = f - s * (f - 2.0 * z * p);
@@ -208,39 +220,39 @@ CM_HD float cm_logf(float x) {
   const float s = (m - 1.0f) / (m + 1.0f);
   const float s2 = s * s;
   float p = 0.0769230769f; /* 1/13 */
-  p = p * s2 + 0.0909090909f;
-  p = p * s2 + 0.111111111f;
-  p = p * s2 + 0.142857143f;
-  p = p * s2 + 0.2f;
-  p = p * s2 + 0.333333333f;
-  p = p * s2 + 1.0f;
+  p = CM_FMAF(p, s2, 0.0909090909f);
+  p = CM_FMAF(p, s2, 0.111111111f);
+  p = CM_FMAF(p, s2, 0.142857143f);
+  p = CM_FMAF(p, s2, 0.2f);
+  p = CM_FMAF(p, s2, 0.333333333f);
+  p = CM_FMAF(p, s2, 1.0f);
   const float lm = 2.0f * s * p;
   const float fe = (float)e;
-  return fe * 0.693115234375f + (fe * 3.193318843841553e-05f + (fe * 1.2996506981721723e-08f + lm));
+  return CM_FMAF(fe, 0.693115234375f, CM_FMAF(fe, 3.193318843841553e-05f, CM_FMAF(fe, 1.2996506981721723e-08f, lm)));
 }
 
 /* sin and cos of x (|x| up to about 1e4) */
 CM_HD void cm_sincosf(float x, float* sp, float* cp) {
   const float k = rintf(x * 0.636619747f); /* x / (pi/2) */
   /* pi/2 = 1.5703125 + 4.8375130e-04 + 7.5497901e-08 (first two: 12 bits) */
-  float r = x - k * 1.5703125f;
-  r = r - k * 4.837512969970703e-04f;
-  r = r - k * 7.549790126404332e-08f;
+  float r = CM_FMAF(-k, 1.5703125f, x);
+  r = CM_FMAF(-k, 4.837512969970703e-04f, r);
+  r = CM_FMAF(-k, 7.549790126404332e-08f, r);
   const float r2 = r * r;
   /* |r| <= pi/4: Taylor series to r^11 (sin) and r^12 (cos) */
   float ps = -2.50521084e-08f;
-  ps = ps * r2 + 2.75573192e-06f;
-  ps = ps * r2 - 1.98412698e-04f;
-  ps = ps * r2 + 8.33333333e-03f;
-  ps = ps * r2 - 1.66666667e-01f;
-  const float sn = r + r * r2 * ps;
+  ps = CM_FMAF(ps, r2, 2.75573192e-06f);
+  ps = CM_FMAF(ps, r2, -1.98412698e-04f);
+  ps = CM_FMAF(ps, r2, 8.33333333e-03f);
+  ps = CM_FMAF(ps, r2, -1.66666667e-01f);
+  const float sn = CM_FMAF(r * r2, ps, r);
   float pc = 2.08767570e-09f;
-  pc = pc * r2 - 2.75573192e-07f;
-  pc = pc * r2 + 2.48015873e-05f;
-  pc = pc * r2 - 1.38888889e-03f;
-  pc = pc * r2 + 4.16666667e-02f;
-  pc = pc * r2 - 0.5f;
-  const float cs = 1.0f + r2 * pc;
+  pc = CM_FMAF(pc, r2, -2.75573192e-07f);
+  pc = CM_FMAF(pc, r2, 2.48015873e-05f);
+  pc = CM_FMAF(pc, r2, -1.38888889e-03f);
+  pc = CM_FMAF(pc, r2, 4.16666667e-02f);
+  pc = CM_FMAF(pc, r2, -0.5f);
+  const float cs = CM_FMAF(r2, pc, 1.0f);
   const int q = ((int)k) & 3;
   if (q == 0) {
     *sp = sn;
@@ -273,12 +285,12 @@ CM_HD float cm_sinf(float x) {
 CM_HD float cm_atan_small(float t) {
   const float t2 = t * t;
   float p = 0.0769230769f; /* 1/13 */
-  p = p * t2 - 0.0909090909f;
-  p = p * t2 + 0.111111111f;
-  p = p * t2 - 0.142857143f;
-  p = p * t2 + 0.2f;
-  p = p * t2 - 0.333333333f;
-  return t + t * t2 * p;
+  p = CM_FMAF(p, t2, -0.0909090909f);
+  p = CM_FMAF(p, t2, 0.111111111f);
+  p = CM_FMAF(p, t2, -0.142857143f);
+  p = CM_FMAF(p, t2, 0.2f);
+  p = CM_FMAF(p, t2, -0.333333333f);
+  return CM_FMAF(t * t2, p, t);
 }
 
 /* atan2(y, x); returns 0 for x = y = 0 */

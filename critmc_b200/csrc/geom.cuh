@@ -16,14 +16,11 @@ __device__ __forceinline__ void byte_row_index(const ByteGeom& g, uint32_t slot,
   i = (int)slot - r * g.hx;
 }
 
-// slots (in the other colour's plane) of the Z neighbours of slot (r, i) of colour c
+// slots (in the other colour's plane) of the Z neighbours of slot (r, i) of
+// colour c, with the row's y and z given (r = y + ly z)
 template <int Z>
-__device__ __forceinline__ void byte_neighbours(const ByteGeom& g, int c, int r, int i, uint32_t* nb) {
-  int y = r, z = 0;
-  if constexpr (Z == 6) {
-    y = r % g.ly;
-    z = r / g.ly;
-  }
+__device__ __forceinline__ void byte_neighbours_at(const ByteGeom& g, int c, int r, int i, int y, int z,
+                                                   uint32_t* nb) {
   const int p = (c + y + z) & 1;
   const int ia = p ? ((i == g.hx - 1) ? 0 : i + 1) : ((i == 0) ? g.hx - 1 : i - 1);
   nb[0] = (uint32_t)(r * g.hx + i);
@@ -39,6 +36,53 @@ __device__ __forceinline__ void byte_neighbours(const ByteGeom& g, int c, int r,
     nb[5] = (uint32_t)((y + g.ly * zp) * g.hx + i);
   }
 }
+
+template <int Z>
+__device__ __forceinline__ void byte_neighbours(const ByteGeom& g, int c, int r, int i, uint32_t* nb) {
+  int y = r, z = 0;
+  if constexpr (Z == 6) {
+    y = r % g.ly;
+    z = r / g.ly;
+  }
+  byte_neighbours_at<Z>(g, c, r, i, y, z, nb);
+}
+
+// Slot s of a colour plane and its coordinates (r = s / hx, i = s % hx,
+// y = r % ly, z = r / ly), advanced by a fixed stride without a division per
+// step: a thread that walks s, s + stride, ... divides once, at init.
+struct SiteCursor {
+  uint32_t s, stride;
+  int r, i, y, z;
+  int dr, di, dy, dz;
+  __device__ __forceinline__ void init(const ByteGeom& g, uint32_t s0, uint32_t step) {
+    s = s0;
+    stride = step;
+    r = (int)(s0 / (uint32_t)g.hx);
+    i = (int)s0 - r * g.hx;
+    y = r % g.ly;
+    z = r / g.ly;
+    dr = (int)(step / (uint32_t)g.hx);
+    di = (int)step - dr * g.hx;
+    dy = dr % g.ly;
+    dz = dr / g.ly;
+  }
+  __device__ __forceinline__ void next(const ByteGeom& g) {
+    s += stride;
+    i += di;
+    r += dr;
+    y += dy;
+    z += dz;
+    if (i >= g.hx) {  // di < hx: one carry at most
+      i -= g.hx;
+      ++r;
+      ++y;
+    }
+    if (y >= g.ly) {  // y + dy + 1 <= 2 ly - 1: one wrap at most
+      y -= g.ly;
+      ++z;
+    }
+  }
+};
 
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* red) {

@@ -61,20 +61,13 @@ __device__ __forceinline__ void gauss2(uint32_t a, uint32_t b, float& g0, float&
   g1 = rad * sn;
 }
 
-// neighbour slots in critmc's column order (+x, -x, +y, -y, +z, -z)
+// neighbour slots in critmc's column order (+x, -x, +y, -y, +z, -z) of the
+// site at (r, i) of row (y, z)
 template <int Z>
-__device__ __forceinline__ void on_neighbours(const ByteGeom& g, int c, uint32_t s, uint32_t* nb,
-                                              int& y, int& z) {
-  int r, i;
-  byte_row_index(g, s, r, i);
+__device__ __forceinline__ void on_neighbours_at(const ByteGeom& g, int c, int r, int i, int y, int z,
+                                                 uint32_t* nb) {
   uint32_t raw[Z];
-  byte_neighbours<Z>(g, c, r, i, raw);
-  y = r;
-  z = 0;
-  if constexpr (Z == 6) {
-    y = r % g.ly;
-    z = r / g.ly;
-  }
+  byte_neighbours_at<Z>(g, c, r, i, y, z, raw);
   const int p = (c + y + z) & 1;
   nb[0] = p ? raw[1] : raw[0];  // +x
   nb[1] = p ? raw[0] : raw[1];  // -x
@@ -86,6 +79,20 @@ __device__ __forceinline__ void on_neighbours(const ByteGeom& g, int c, uint32_t
     nb[4] = raw[5];  // +z
     nb[5] = raw[4];  // -z
   }
+}
+
+template <int Z>
+__device__ __forceinline__ void on_neighbours(const ByteGeom& g, int c, uint32_t s, uint32_t* nb,
+                                              int& y, int& z) {
+  int r, i;
+  byte_row_index(g, s, r, i);
+  y = r;
+  z = 0;
+  if constexpr (Z == 6) {
+    y = r % g.ly;
+    z = r / g.ly;
+  }
+  on_neighbours_at<Z>(g, c, r, i, y, z, nb);
 }
 
 // Best & Fisher (1979) von Mises sampler, critmc kernels/on.py:187-204, returning
@@ -130,11 +137,9 @@ constexpr int on_nv() { return 2 + N + Z; }
 // One update of site s of colour c (one of the three moves); returns 1 for an
 // accepted Metropolis move.  lat holds comp[n][colour][slot].
 template <int N, int Z>
-__device__ __forceinline__ int on_site(float* lat, const ByteGeom& g, int c, uint32_t s, int code,
-                                       uint32_t sweep, float beta, float step, uint32_t k0, uint32_t k1) {
-  uint32_t nb[Z];
-  int y, z;
-  on_neighbours<Z>(g, c, s, nb, y, z);
+__device__ __forceinline__ int on_site_nb(float* lat, const ByteGeom& g, int c, uint32_t s, const uint32_t* nb,
+                                          int code, uint32_t sweep, float beta, float step, uint32_t k0,
+                                          uint32_t k1) {
   float* own[N];
   const float* oth[N];
 #pragma unroll
@@ -257,6 +262,15 @@ __device__ __forceinline__ int on_site(float* lat, const ByteGeom& g, int c, uin
   return 0;
 }
 
+template <int N, int Z>
+__device__ __forceinline__ int on_site(float* lat, const ByteGeom& g, int c, uint32_t s, int code,
+                                       uint32_t sweep, float beta, float step, uint32_t k0, uint32_t k1) {
+  uint32_t nb[Z];
+  int y, z;
+  on_neighbours<Z>(g, c, s, nb, y, z);
+  return on_site_nb<N, Z>(lat, g, c, s, nb, code, sweep, beta, step, k0, k1);
+}
+
 // on.py:79-87: rescale site j (of 2 slots) to unit length
 template <int N>
 __device__ __forceinline__ void on_normalize_site(float* lat, size_t n_sites, uint32_t j) {
@@ -274,13 +288,9 @@ __device__ __forceinline__ void on_normalize_site(float* lat, size_t n_sites, ui
 // on.py:36-76: add site j's terms (forward bonds) to v[0] energy, v[1..N] M,
 // v[1+N+a] stiffness cos, v[1+N+DIM+a] stiffness sin sums
 template <int N, int Z>
-__device__ __forceinline__ void on_measure_site(const float* lat, const ByteGeom& g, uint32_t j, long long* v) {
+__device__ __forceinline__ void on_measure_site_nb(const float* lat, const ByteGeom& g, int c, uint32_t s,
+                                                   const uint32_t* nb, long long* v) {
   constexpr int DIM = Z / 2;
-  const int c = j >= g.slots;
-  const uint32_t s = j - c * g.slots;
-  uint32_t nb[Z];
-  int y, z;
-  on_neighbours<Z>(g, c, s, nb, y, z);
   double si[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -299,6 +309,16 @@ __device__ __forceinline__ void on_measure_site(const float* lat, const ByteGeom
     v[1 + N + a] += on_fix(si[0] * sj[0] + si[1] * sj[1]);
     v[1 + N + DIM + a] += on_fix(si[0] * sj[1] - si[1] * sj[0]);
   }
+}
+
+template <int N, int Z>
+__device__ __forceinline__ void on_measure_site(const float* lat, const ByteGeom& g, uint32_t j, long long* v) {
+  const int c = j >= g.slots;
+  const uint32_t s = j - c * g.slots;
+  uint32_t nb[Z];
+  int y, z;
+  on_neighbours<Z>(g, c, s, nb, y, z);
+  on_measure_site_nb<N, Z>(lat, g, c, s, nb, v);
 }
 
 // sum q (of on_nv) of measurement meas, converted back to doubles
@@ -379,8 +399,12 @@ __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
       const int code = P.codes[row];
       for (int rep = 0; rep < P.reps[row]; ++rep) {
         for (int c = 0; c < 2; ++c) {
-          for (uint32_t s = t0; s < g.slots; s += nt)
-            nacc += on_site<N, Z>(lat, g, c, s, code, sweep, P.beta, P.step, P.k0, P.k1);
+          SiteCursor cur;
+          for (cur.init(g, t0, (uint32_t)nt); cur.s < g.slots; cur.next(g)) {
+            uint32_t nb[Z];
+            on_neighbours_at<Z>(g, c, cur.r, cur.i, cur.y, cur.z, nb);
+            nacc += on_site_nb<N, Z>(lat, g, c, cur.s, nb, code, sweep, P.beta, P.step, P.k0, P.k1);
+          }
           __syncthreads();
         }
         ++sweep;
@@ -391,7 +415,14 @@ __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
     long long v[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = 0;
-    for (uint32_t j = t0; j < n_sites; j += nt) on_measure_site<N, Z>(lat, g, j, v);
+    for (int c = 0; c < 2; ++c) {
+      SiteCursor cur;
+      for (cur.init(g, t0, (uint32_t)nt); cur.s < g.slots; cur.next(g)) {
+        uint32_t nb[Z];
+        on_neighbours_at<Z>(g, c, cur.r, cur.i, cur.y, cur.z, nb);
+        on_measure_site_nb<N, Z>(lat, g, c, cur.s, nb, v);
+      }
+    }
     v[NV - 1] = nacc;
     const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll

@@ -64,7 +64,8 @@ def profile_traffic() -> dict | None:
 
 class Clocks:
     """Samples the SM clock, its maximum and the clock-event reasons of one GPU
-    every 100 ms from a host thread (NVML queries only; no setting is changed).
+    every 5 ms from a host thread (NVML queries only; no setting is changed), so
+    that a timed region of a few tens of milliseconds still gets several samples.
 
     NVML is read in-process rather than through a piped ``nvidia-smi -lms``:
     that child buffers its output and, stopped by a signal, can lose every
@@ -77,7 +78,7 @@ class Clocks:
                ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
                ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, device, period_s: float = 0.1):
+    def __init__(self, device, period_s: float = 0.005):
         self.device = device
         self.period = period_s
         self.samples: list[tuple[float, float, int]] = []
@@ -147,7 +148,7 @@ class Clocks:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(x[0] for x in self.samples),
                 "sm_max_mhz": max(x[1] for x in self.samples), "reasons": sorted(reasons),
-                "samples": len(self.samples), "source": "NVML, 100 ms period, during the timed steps"}
+                "samples": len(self.samples), "source": f"NVML every {self.period * 1e3:.0f} ms during the timed steps"}
 
 
 def ea_bench(dev, n_bins: int = 16, peak: float = 6650.0) -> dict:

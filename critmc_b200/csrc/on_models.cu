@@ -128,7 +128,15 @@ __device__ __forceinline__ float von_mises_cos(float kappa, const critmc_u32x4& 
 // are split over threads and blocks (the CPU replay gets the same totals).
 constexpr double ON_FIX = 68719476736.0;  // 2^36
 constexpr double ON_UNFIX = 1.0 / 68719476736.0;
-__device__ __forceinline__ long long on_fix(double x) { return __double2ll_rn(x * ON_FIX); }
+// round(x 2^36) to nearest even, as llrint does: for |x 2^36| < 2^51, adding
+// 1.5 2^52 leaves the rounded integer in the low mantissa bits (one add and an
+// integer subtract instead of a conversion instruction).  The terms here are
+// dot products and components of unit vectors, |x| <= 3.
+constexpr double ON_ROUND_MAGIC = 6755399441055744.0;  // 1.5 * 2^52
+__device__ __forceinline__ long long on_fix(double x) {
+  const double t = __dadd_rn(x * ON_FIX, ON_ROUND_MAGIC);
+  return __double_as_longlong(t) - __double_as_longlong(ON_ROUND_MAGIC);
+}
 
 // number of sums per measurement: energy, M[N], stiffness cos/sin [dim], accepted moves
 template <int N, int Z>

@@ -394,17 +394,34 @@ def small_case(dev, case: str) -> dict:
     return {"case": case, "seconds": s, "updates_per_ns": units / s / 1e9}
 
 
+def _critmc_port_state(L_x: int, L_y: int, t: int):
+    """Spins, neighbour table and Generator state of host chain t (critmc's layouts)."""
+    from critmc_b200 import square
+
+    import oracle
+
+    lat = square(L_x, L_y)
+    s = (2 * np.random.default_rng(100 + t).integers(0, 2, lat.n_sites) - 1).astype(np.int8)
+    words = oracle.pcg_words(np.random.PCG64DXSM(200 + t).state)
+    return s, np.ascontiguousarray(lat.nbr, dtype=np.int64), words
+
+
 def cpu_sample(threads: int, sweeps: int = 1, L: int = L_HEAD) -> dict:
-    """The C oracle (a plain-C port of critmc's Ising sweep with the same Philox
-    stream) on `threads` host threads, one L x L chain per thread."""
+    """critmc's own CPU Ising kernel (typewriter Metropolis, float64 table, PCG64DXSM),
+    restated in C and bit-identical to critmc (tests/test_critmc_port_cpu.py), on
+    `threads` host threads, one L x L chain per thread."""
     import oracle
 
     oracle.lib()
+    s0, nbr, _ = _critmc_port_state(L, L, 0)
+    states = [(2 * np.random.default_rng(100 + t).integers(0, 2, L * L) - 1).astype(np.int8) for t in range(threads)]
+    words = [oracle.pcg_words(np.random.PCG64DXSM(200 + t).state) for t in range(threads)]
+    del s0
 
     def one(t: int) -> float:
-        s = (2 * np.random.default_rng(100 + t).integers(0, 2, L * L) - 1).astype(np.int8)
         t0 = time.perf_counter()
-        oracle.ising_msc_run(s, (L, L), (t, 7), BETAS[t % 3], 0.0, [[0, 1]], sweeps)
+        oracle.critmc_ising_run(states[t], nbr, words[t], BETAS[t % 3], 0.0, [[0, 1]], sweeps,
+                                running=np.zeros(2, np.int64))
         return time.perf_counter() - t0
 
     t0 = time.perf_counter()
@@ -413,17 +430,20 @@ def cpu_sample(threads: int, sweeps: int = 1, L: int = L_HEAD) -> dict:
     wall = time.perf_counter() - t0
     upd = threads * sweeps * L * L
     return {"value": upd / wall / 1e9, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"{threads} chains of {L}x{L}, {sweeps} checkerboard Metropolis sweep(s) each, "
-                      f"one host thread per chain, hot start ({wall:.1f} s wall)"}
+            "sample": f"{threads} chains of {L}x{L}, {sweeps} typewriter Metropolis sweep(s) each with critmc's "
+                      f"kernel restated in C (bit-identical to critmc's numba run, same PCG64DXSM stream), one "
+                      f"host thread per chain ({wall:.1f} s wall)"}
 
 
 def run_reference(args) -> None:
-    """CPU arm: the C oracle (port of critmc's sweep) on every host thread.
+    """CPU arm: critmc's own CPU Ising kernel (typewriter Metropolis with its
+    float64 tables and PCG64DXSM stream), restated in C and bit-identical to
+    critmc's numba ``run`` (tests/test_critmc_port_cpu.py), on every host thread.
 
     One step advances, on each host thread, its own 4096 x 64 torus (a strip of
-    the L = 4096 workload, 262,144 sites) by one checkerboard Metropolis sweep,
-    so that `--steps K` stays within minutes; the rate is updates per ns of
-    wall time over the K steps."""
+    the L = 4096 workload, 262,144 sites) by one sweep, so that `--steps K`
+    stays within minutes; the rate is updates per ns of wall time over the K
+    steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -433,30 +453,29 @@ def run_reference(args) -> None:
     threads = os.cpu_count() or 1
     shape = (L_HEAD, 64)
     n = shape[0] * shape[1]
-    states = [(2 * np.random.default_rng(200 + t).integers(0, 2, n) - 1).astype(np.int8)
-              for t in range(threads)]
-    runs = [None] * threads
+    chains = [_critmc_port_state(shape[0], shape[1], t) for t in range(threads)]
+    runs = [np.zeros(2, np.int64) for _ in range(threads)]
 
-    def step(t: int, sweep: int) -> None:
-        _, _, _, runs[t] = oracle.ising_msc_run(states[t], shape, (t, 11), BETAS[t % 3], 0.0,
-                                                [[0, 1]], 1, sweep0=sweep, running=runs[t])
+    def step(t: int) -> None:
+        s, nbr, words = chains[t]
+        oracle.critmc_ising_run(s, nbr, words, BETAS[t % 3], 0.0, [[0, 1]], 1, running=runs[t])
 
     with cf.ThreadPoolExecutor(threads) as ex:
-        for w in range(args.warmup):
-            list(ex.map(lambda t: step(t, w), range(threads)))
+        for _ in range(args.warmup):
+            list(ex.map(step, range(threads)))
         t0 = time.perf_counter()
-        for k in range(args.steps):
-            list(ex.map(lambda t: step(t, args.warmup + k), range(threads)))
+        for _ in range(args.steps):
+            list(ex.map(step, range(threads)))
         wall = time.perf_counter() - t0
     value = threads * n * args.steps / wall / 1e9
-    sample = (f"{threads} host threads, each advancing its own {shape[0]}x{shape[1]} torus by one "
-              f"checkerboard Metropolis sweep per step")
+    sample = (f"{threads} host threads, each advancing its own {shape[0]}x{shape[1]} torus by one typewriter "
+              f"Metropolis sweep per step with critmc's kernel restated in C (bit-identical to critmc)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"2D Ising L={L_HEAD} checkerboard Metropolis (4096x64 strips per thread)",
+        "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": f"2D Ising L={L_HEAD} Metropolis (4096x64 strips per thread)",
                    "parallelism": f"{threads} host threads"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

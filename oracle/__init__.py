@@ -81,6 +81,10 @@ def _declare(L: ctypes.CDLL) -> None:
     L.oracle_ea_pt_run.argtypes = [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _I, _P, _P, _U32, _I, _I, _I,
                                    _P, _P, _P, _P, _P]
     L.oracle_ea_pt_run.restype = _I
+    L.critmc_port_pcg_raw.argtypes = [_P, ctypes.c_int64, _P]
+    L.critmc_port_pcg_raw.restype = None
+    L.critmc_port_ising_run.argtypes = [_P, _P, ctypes.c_int64, _I, _D, _D, _P, _P, _I, _I, _P, _P, _P, _P]
+    L.critmc_port_ising_run.restype = _I
 
 
 def cluster_update(lay: np.ndarray, shape, q: int, key, beta: float, algo: int, sweep: int,
@@ -336,3 +340,45 @@ def ea_pt_run(spins, couplings, shape, keys, betas, swap_thr, perm, labels, n_st
     if rc != 0:
         raise ValueError(f"oracle_ea_pt_run failed ({rc})")
     return acc, sa, stry, lh, tr
+
+
+def pcg_words(state: dict) -> np.ndarray:
+    """numpy PCG64DXSM state dict -> (state hi, state lo, inc hi, inc lo)."""
+    st = state["state"] if "inc" not in state else state
+    s, inc = int(st["state"]), int(st["inc"])
+    m = (1 << 64) - 1
+    return np.array([s >> 64, s & m, inc >> 64, inc & m], dtype=np.uint64)
+
+
+def pcg_raw(words: np.ndarray, n: int) -> np.ndarray:
+    """The next n raw outputs of the C PCG64DXSM (words updated in place)."""
+    out = np.zeros(n, dtype=np.uint64)
+    lib().critmc_port_pcg_raw(_ptr(words), n, _ptr(out))
+    return out
+
+
+def critmc_ising_run(s, nbr, words, beta, h, schedule, n_meas, running=None):
+    """critmc's CPU Ising ``run`` (typewriter Metropolis / heat bath) restated in C.
+
+    ``s`` int8 spins in critmc's site order (updated), ``nbr`` critmc's int64
+    (N, z) neighbour table, ``words`` the Generator state (``pcg_words``,
+    updated).  Returns ``(e_b, m, aux, running)`` like the GPU entry points.
+    """
+    if not (isinstance(s, np.ndarray) and s.dtype == np.int8 and s.flags["C_CONTIGUOUS"]):
+        raise TypeError("s must be a C-contiguous int8 array (it is updated in place)")
+    nb = np.ascontiguousarray(nbr, dtype=np.int64)
+    n, z = nb.shape
+    sched = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
+    if running is None:
+        i = np.arange(n)
+        running = np.array([-int(sum(int(np.dot(s[i].astype(np.int64), s[nb[:, 2 * a]].astype(np.int64)))
+                                     for a in range(z // 2))), int(s.astype(np.int64).sum())], dtype=np.int64)
+    running = np.ascontiguousarray(running, dtype=np.int64).copy()
+    e = np.zeros(n_meas, dtype=np.int64)
+    m = np.zeros(n_meas, dtype=np.int64)
+    aux = np.zeros((n_meas, 4), dtype=np.int64)
+    rc = lib().critmc_port_ising_run(_ptr(s), _ptr(nb), n, z, float(beta), float(h), _ptr(words), _ptr(sched),
+                                     len(sched), n_meas, _ptr(running), _ptr(e), _ptr(m), _ptr(aux))
+    if rc != 0:
+        raise ValueError(f"critmc_port_ising_run failed ({rc})")
+    return e, m, aux, running

@@ -44,4 +44,8 @@ int oracle_ea_pt_run(int8_t* spins, const double* J, int dim, int lx, int ly, in
                      int* perm, int* labels, uint32_t t0, int n_steps, int n_bins,
                      int sweeps_per_step, double* acc, int64_t* swap_acc, int64_t* swap_try,
                      int64_t* label_hist, int64_t* trips);
+void critmc_port_pcg_raw(uint64_t w[4], int64_t n, uint64_t* out);
+int critmc_port_ising_run(int8_t* s, const int64_t* nbr, int64_t n, int z, double beta, double h, uint64_t pcg[4],
+                          const int64_t* schedule, int n_rows, int n_meas, int64_t* running, int64_t* e_out,
+                          int64_t* m_out, int64_t* aux_out);
 #endif

@@ -484,7 +484,7 @@ def run_reference(args) -> None:
 
 
 def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0, world: int = 1,
-                max_grid_lanes: int = 8) -> dict | None:
+                max_grid_lanes: int = 8, grid_after_s: float | None = 1.0) -> dict | None:
     """Continuous-batching server on a seeded Poisson stream of mixed requests.
 
     Workload: ``n_requests`` requests at ``rate``/s, each uniform over 2D Ising
@@ -507,7 +507,7 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0,
 
     # series reduced to sums (stats_lag=0: no host-side error-bar sums inside the timed run)
     srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto", max_grid_lanes=max_grid_lanes,
-                 stats_lag=0)
+                 stats_lag=0, grid_after_s=grid_after_s)
     # warm-up: one short request per (model, size) of the mix builds the
     # lattice cache, the library streams and the kernels' first launches
     shapes = sorted({(r.model, r.L) for r in reqs})
@@ -551,10 +551,14 @@ def main() -> None:
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
     ap.add_argument("--serve-grid-lanes", type=int, default=8, help="requests on multi-block lanes at once")
+    ap.add_argument("--serve-grid-after", type=float, default=1.0,
+                    help="item-lane seconds (cost model) above which a request takes a multi-block lane; "
+                         "negative: every large lattice")
     ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch", "cluster-sw"],
                     help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    grid_after = None if args.serve_grid_after < 0 else args.serve_grid_after
     if args.impl == "reference":
         run_reference(args)
         return
@@ -604,7 +608,8 @@ def main() -> None:
 
     if args.serve_only:
         print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate,
-                                                 max_grid_lanes=args.serve_grid_lanes)}), flush=True)
+                                                 max_grid_lanes=args.serve_grid_lanes,
+                                                 grid_after_s=grid_after)}), flush=True)
         return
 
     # launch shape (rows per thread, inline planes) from the autotuner; results do not depend on it
@@ -679,7 +684,7 @@ def main() -> None:
     serving = None
     if args.serve_requests > 0:  # every rank serves its shard; rank 0 gets the job's numbers
         serving = serve_bench(dev, args.serve_requests, args.serve_rate, rank=rank, world=world,
-                              max_grid_lanes=args.serve_grid_lanes)
+                              max_grid_lanes=args.serve_grid_lanes, grid_after_s=grid_after)
     if rank == 0 and world == 1 and not args.no_extras:
         extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
         extras["on_batched"] = on_bench(dev, peak=peaks()[0])

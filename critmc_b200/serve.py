@@ -280,7 +280,8 @@ class Server:
     """Continuous-batching sampler for a stream of mixed requests on one GPU."""
 
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
-                 tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
+                 tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 12,
+                 grid_after_s: float | None = 1.0,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
                  keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None,
                  stats_lag: int = 64):
@@ -291,6 +292,9 @@ class Server:
         self.tick_s = tick_ms * 1e-3
         self.max_active = max_active
         self.grid_min_sites = grid_min_sites
+        # a request takes a multi-block lane when, on an item lane, it would run longer
+        # than this (cost model); None: every lattice from grid_min_sites sites on
+        self.grid_after_s = grid_after_s
         # the multi-block lanes are launch-bound: they buy latency, the item
         # kernels throughput, so at most this many requests use them at once
         self.max_grid_lanes = max_grid_lanes
@@ -351,6 +355,18 @@ class Server:
         else:
             lat = 4 * n * (2 if req.model == "xy" else 3)
         return lat + 4096
+
+    def _wants_grid(self, req: Request, family: str) -> bool:
+        """Multi-block lanes are few (launch-bound); they go to the requests that an
+        item lane would keep longest: at least grid_min_sites sites and, by the
+        cost model, more than grid_after_s seconds of item-lane time."""
+        if req.n_sites < self.grid_min_sites:
+            return False
+        if self.grid_after_s is None:
+            return True
+        a, b = self.costs[("items", family)]
+        per_meas = int(req.schedule()[:, 1].sum())
+        return req.sweeps * per_meas * (a + b * req.n_sites) > self.grid_after_s
 
     def _grid_free(self) -> bool:
         return sum(1 for lane in self.grid_lanes if lane.jobs) < self.max_grid_lanes
@@ -417,7 +433,7 @@ class Server:
             group = family
             fields = [("Eb", _I8, 1), ("M", _I8, 1), ("aux", _I8, 4)]
             t["running"] = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
-            lane = "grid" if msc and req.n_sites >= self.grid_min_sites and self._grid_free() else "items"
+            lane = "grid" if msc and self._wants_grid(req, "msc") and self._grid_free() else "items"
             kind = ITEM_MSC_ISING if msc else ITEM_BYTE_ISING
             h = model.h
             if lane == "grid":
@@ -428,8 +444,8 @@ class Server:
             t["running"] = torch.tensor([running["energy"]], dtype=torch.int64, device=dev)
             t["counts"] = torch.from_numpy(np.asarray(running["counts"], dtype=np.int64)).to(dev)
         else:
-            if chain.lane == "grid" and not self._grid_free():
-                chain.lane = "block"  # same results on either lane
+            # same results on either lane
+            chain.lane = "grid" if self._wants_grid(req, f"on{model.n}") and self._grid_free() else "block"
             family, lane, kind, h = f"on{model.n}", chain.lane.replace("block", "items"), ITEM_ON, 0.0
             group = f"on{model.n}d{dim}"
             fields = [("E", _F8, 1), ("M", _F8, model.n), ("stiff_c", _F8, dim), ("stiff_s", _F8, dim),

@@ -40,6 +40,7 @@ from .device import empty_bytes, ptr, require_cuda
 from .items import ITEM_BYTE_ISING, ITEM_MSC_ISING, ITEM_ON, ITEM_POTTS, CritmcItem, launch_items
 from .lattice import hypercubic
 from .models import ON, UPDATE_CODES, Ising, Model, Potts, _IsingMscChain, _msc_ok
+from .on_models import GRID_MIN_SITES as ON_GRID_MIN_SITES
 from .rng import make_rng, philox_key
 from .sim import parse_updates
 from .streaming import HostStreamStats
@@ -280,8 +281,8 @@ class Server:
     """Continuous-batching sampler for a stream of mixed requests on one GPU."""
 
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
-                 tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 12,
-                 grid_after_s: float | None = 1.0,
+                 tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
+                 grid_after_s: float | None = None,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
                  keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None,
                  stats_lag: int = 64):
@@ -292,8 +293,9 @@ class Server:
         self.tick_s = tick_ms * 1e-3
         self.max_active = max_active
         self.grid_min_sites = grid_min_sites
-        # a request takes a multi-block lane when, on an item lane, it would run longer
-        # than this (cost model); None: every lattice from grid_min_sites sites on
+        # None: multi-block lanes for multi-spin-coded Ising lattices from grid_min_sites
+        # sites and O(n) lattices from 4096 sites, first come first served; a number:
+        # for the requests that an item lane would keep longer than that (cost model)
         self.grid_after_s = grid_after_s
         # the multi-block lanes are launch-bound: they buy latency, the item
         # kernels throughput, so at most this many requests use them at once
@@ -360,10 +362,10 @@ class Server:
         """Multi-block lanes are few (launch-bound); they go to the requests that an
         item lane would keep longest: at least grid_min_sites sites and, by the
         cost model, more than grid_after_s seconds of item-lane time."""
-        if req.n_sites < self.grid_min_sites:
-            return False
         if self.grid_after_s is None:
-            return True
+            return req.n_sites >= (self.grid_min_sites if family == "msc" else ON_GRID_MIN_SITES)
+        if req.n_sites < ON_GRID_MIN_SITES:
+            return False
         a, b = self.costs[("items", family)]
         per_meas = int(req.schedule()[:, 1].sum())
         return req.sweeps * per_meas * (a + b * req.n_sites) > self.grid_after_s

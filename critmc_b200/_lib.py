@@ -35,6 +35,9 @@ SIGNATURES: dict[str, tuple] = {
         [_P, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32, _U32, _P, _I32, _I32, _P, _P, _P, _P, _P,
          _I32, _I32, _P],
     ),
+    "critmc_ising_msc_batch_scratch_bytes": (_I64, [_I32, _I32]),
+    "critmc_ising_msc_run_batch": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P, _I32, _I32, _P, _I32,
+                                          _P]),
     "critmc_ising_msc_measure": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "critmc_item_prepare": (_I32, [_P, _D, _D, _D]),
     "critmc_items_buffer_bytes": (_I64, [_I32]),
@@ -169,6 +172,7 @@ HOST_ONLY = frozenset({
     "critmc_graph_cache_set_capacity", "critmc_cluster_scratch_bytes", "critmc_stream_state_bytes",
     "critmc_ea_campaign_buffer_bytes", "critmc_graph_cache_size",
     "critmc_control_arm", "critmc_control_cancel", "critmc_control_status",
+    "critmc_ising_msc_batch_scratch_bytes",
 })
 
 

@@ -39,6 +39,13 @@ struct MscParams {
   uint32_t meas;            // measurement slot (or offset when cursor != null)
   uint32_t keys[MSC_PCHAINS][2];
   MscTables tabs;
+  // batches of separately allocated chains (critmc_ising_msc_run_batch): the
+  // lattice and table group of each chain of the launch, and a device array of
+  // their sweep bases; batch_sweep == null for the contiguous chains of
+  // critmc_ising_msc_run
+  const uint32_t* batch_sweep;
+  uint32_t* batch_spins[CRITMC_MSC_BATCH_MAX];
+  uint32_t batch_group[CRITMC_MSC_BATCH_MAX];
 };
 
 struct MscFix {
@@ -102,22 +109,24 @@ __device__ __noinline__ int3 msc_flush(const MscRule<Z, RULE> rule, const MscGeo
 // rounds of the acceptance planes (10, or 7 when the caller asks for it).
 // Three blocks per SM (up to 85 registers a thread): the kernel is issue bound,
 // and fewer rematerialised values beat the fourth block's latency hiding.
-template <int Z, int RULE, int KG, int PR>
+// BATCH: the chains of the launch are separately allocated (batch_* fields).
+template <int Z, int RULE, int KG, int PR, bool BATCH>
 __global__ void __launch_bounds__(MSC_THREADS, 3)
     msc_halfsweep_kernel(const __grid_constant__ MscParams P) {
   __shared__ MscFix fix[MSC_WARPS][MSC_FIXCAP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lchain = blockIdx.y;
   const int chain = P.chain0 + lchain;
-  const int group = chain / P.chains_per_group;
+  const int group = BATCH ? (int)P.batch_group[lchain] : chain / P.chains_per_group;
   const MscGeom& g = P.g;
   const MscRule<Z, RULE> rule{P.tabs.kind[group], P.tabs.thr[group]};
   const uint32_t k0 = P.keys[lchain][0], k1 = P.keys[lchain][1];
-  const uint32_t sweep = P.cursor ? P.cursor[0] + P.sweep : P.sweep;
+  const uint32_t sweep = (P.cursor ? P.cursor[0] + P.sweep : P.sweep) + (BATCH ? P.batch_sweep[chain] : 0u);
   const uint32_t meas = P.cursor ? P.cursor[1] + P.meas : P.meas;
   const uint32_t col = (uint32_t)P.col;
-  uint32_t* own = P.spins + (size_t)chain * 2 * g.words + (size_t)col * g.words;
-  const uint32_t* other = P.spins + (size_t)chain * 2 * g.words + (size_t)(col ^ 1) * g.words;
+  uint32_t* const lat = BATCH ? P.batch_spins[lchain] : P.spins + (size_t)chain * 2 * g.words;
+  uint32_t* own = lat + (size_t)col * g.words;
+  const uint32_t* other = lat + (size_t)(col ^ 1) * g.words;
 
   const uint32_t t = blockIdx.x * MSC_THREADS + threadIdx.x;
   const int k = (int)(t & (g.wc - 1));
@@ -256,6 +265,61 @@ __global__ void msc_finalize_kernel(const long long* __restrict__ acc, long long
   }
 }
 
+// Output pointers of the chains of a batch (critmc_ising_msc_run_batch).
+struct MscBatchOut {
+  long long* running[CRITMC_MSC_BATCH_MAX];
+  long long* e_out[CRITMC_MSC_BATCH_MAX];
+  long long* m_out[CRITMC_MSC_BATCH_MAX];
+  long long* aux_out[CRITMC_MSC_BATCH_MAX];
+};
+
+// msc_finalize_kernel for separately allocated chains: block c scans chain c's
+// increments into its own series and running sums.
+__global__ void msc_finalize_batch_kernel(const long long* __restrict__ acc, const __grid_constant__ MscBatchOut O,
+                                          int n_chains, int n_meas) {
+  const int chain = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int nt = blockDim.x;
+  __shared__ long long se[256], sm[256];
+  const int per = (n_meas + nt - 1) / nt;
+  const int b = tid * per, e = min(n_meas, b + per);
+  long long le = 0, lm = 0;
+  for (int i = b; i < e; ++i) {
+    le += acc[((size_t)i * n_chains + chain) * 3 + 0];
+    lm += acc[((size_t)i * n_chains + chain) * 3 + 1];
+  }
+  se[tid] = le;
+  sm[tid] = lm;
+  __syncthreads();
+  long long* running = O.running[chain];
+  if (tid == 0) {
+    long long ce = running[0], cm = running[1];
+    for (int q = 0; q < nt; ++q) {
+      const long long te = se[q], tm = sm[q];
+      se[q] = ce;
+      sm[q] = cm;
+      ce += te;
+      cm += tm;
+    }
+    running[0] = ce;
+    running[1] = cm;
+  }
+  __syncthreads();
+  long long ce = se[tid], cm = sm[tid];
+  long long *e_out = O.e_out[chain], *m_out = O.m_out[chain], *aux_out = O.aux_out[chain];
+  for (int i = b; i < e; ++i) {
+    const size_t src = ((size_t)i * n_chains + chain) * 3;
+    ce += acc[src + 0];
+    cm += acc[src + 1];
+    e_out[i] = ce;
+    m_out[i] = cm;
+    aux_out[(size_t)i * 4 + 0] = acc[src + 2];
+    aux_out[(size_t)i * 4 + 1] = 0;
+    aux_out[(size_t)i * 4 + 2] = 0;
+    aux_out[(size_t)i * 4 + 3] = 0;
+  }
+}
+
 __global__ void msc_cursor_set(uint32_t* cursor, uint32_t sweep, uint32_t meas) {
   cursor[0] = sweep;
   cursor[1] = meas;
@@ -370,8 +434,14 @@ template <int Z, int RULE, int PR>
 static void launch_half_kg(const MscParams& P, int kg, cudaStream_t st) {
   const long long threads = (long long)P.g.wc * ((P.g.rows + P.run - 1) / P.run);
   const dim3 grid((unsigned)((threads + MSC_THREADS - 1) / MSC_THREADS), P.n_chains - P.chain0 < MSC_PCHAINS ? P.n_chains - P.chain0 : MSC_PCHAINS);
-  if (kg == 1) msc_halfsweep_kernel<Z, RULE, 1, PR><<<grid, MSC_THREADS, 0, st>>>(P);
-  else msc_halfsweep_kernel<Z, RULE, 2, PR><<<grid, MSC_THREADS, 0, st>>>(P);
+  if constexpr (PR == CRITMC_PHILOX_ROUNDS) {
+    if (P.batch_sweep) {  // batches: 8 inline planes, default stream only
+      msc_halfsweep_kernel<Z, RULE, 2, PR, true><<<grid, MSC_THREADS, 0, st>>>(P);
+      return;
+    }
+  }
+  if (kg == 1) msc_halfsweep_kernel<Z, RULE, 1, PR, false><<<grid, MSC_THREADS, 0, st>>>(P);
+  else msc_halfsweep_kernel<Z, RULE, 2, PR, false><<<grid, MSC_THREADS, 0, st>>>(P);
 }
 
 template <int Z, int PR>
@@ -399,6 +469,81 @@ void msc_launch_half(MscParams& P, const uint32_t* keys, int rule, int kg, int p
       else launch_half_z<6, CRITMC_PHILOX_ROUNDS>(P, rule, kg, st);
     }
   }
+}
+
+// Launch the half-sweeps of n_meas schedule applications on stream s: one
+// launch per half-sweep (mode 1), or CUDA graphs of G measurements replayed
+// with a device cursor (mode 3; the graph is cached by its parameters).
+// sweep0 is the first sweep of the call (contiguous chains) or 0 (batches,
+// whose per-chain bases the kernels add).
+static int msc_launch_schedule(MscParams (&P)[2], const int (&rule)[2], const uint32_t* keys, int n_chains,
+                               const int64_t* schedule, int n_rows, long long sweeps_per_meas, int n_meas,
+                               uint32_t sweep0, int mode, int kg, int pr, uint32_t* cursor, cudaStream_t s) {
+  auto launch_meas = [&](uint32_t sweep_rel, uint32_t meas_rel, const uint32_t* cur) {
+    uint32_t sw = sweep_rel;
+    for (int r = 0; r < n_rows; ++r) {
+      const int slot = schedule[2 * r] == CRITMC_HEATBATH ? 1 : 0;
+      MscParams& q = P[slot];
+      q.cursor = cur;
+      for (int64_t rep = 0; rep < schedule[2 * r + 1]; ++rep) {
+        q.sweep = sw;
+        q.meas = meas_rel;
+        q.col = 0;
+        msc_launch_half(q, keys, rule[slot], kg, pr, s);
+        q.col = 1;
+        msc_launch_half(q, keys, rule[slot], kg, pr, s);
+        ++sw;
+      }
+    }
+  };
+
+  if (mode == 1) {
+    uint32_t sw = sweep0;
+    for (int m = 0; m < n_meas; ++m) {
+      launch_meas(sw, (uint32_t)m, nullptr);
+      sw += (uint32_t)sweeps_per_meas;
+    }
+  } else {
+    // a graph of G measurements replayed with a device cursor
+    const int G = (int)std::max<long long>(
+        1, std::min<long long>(n_meas, 256 / std::max<long long>(1, sweeps_per_meas)));
+    msc_cursor_set<<<1, 1, 0, s>>>(cursor, sweep0, 0);
+    const int n_graph = n_meas / G;
+    if (n_graph > 1) {
+      // the graph depends on the parameters below only: reuse it across calls
+      int dev = 0;
+      cudaGetDevice(&dev);
+      GraphKey key;
+      key.add(0x4d534347u).add(dev).add(G).add(n_rows).add(rule).add(kg).add(pr);
+      key.add_bytes(schedule, sizeof(int64_t) * 2 * n_rows).add_bytes(keys, sizeof(uint32_t) * 2 * n_chains);
+      for (int slot = 0; slot < 2; ++slot) {
+        MscParams& q = P[slot];
+        q.cursor = cursor;
+        q.sweep = q.meas = 0;
+        q.col = q.chain0 = 0;
+        std::memset(q.keys, 0, sizeof(q.keys));
+        key.add(q);
+      }
+      cudaGraphExec_t exec = graph_cache_find(key);
+      if (!exec) {
+        cudaGraph_t graph;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+          return cuda_fail("capture");
+        for (int m = 0; m < G; ++m) launch_meas((uint32_t)(m * sweeps_per_meas), (uint32_t)m, cursor);
+        msc_cursor_bump<<<1, 1, 0, s>>>(cursor, (uint32_t)(G * sweeps_per_meas), (uint32_t)G);
+        if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return cuda_fail("end capture");
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return cuda_fail("instantiate");
+        graph_cache_insert(key, exec);
+      }
+      for (int i = 0; i < n_graph; ++i) cudaGraphLaunch(exec, s);
+    }
+    const int done = n_graph > 1 ? n_graph * G : 0;
+    for (int m = done; m < n_meas; ++m)
+      launch_meas((uint32_t)(sweep0 + (uint32_t)(m * sweeps_per_meas)), (uint32_t)m, nullptr);
+  }
+  return CRITMC_OK;
 }
 
 }  // namespace critmc
@@ -482,6 +627,7 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
     MscParams& q = P[slot];
     q.spins = spins;
     q.acc = acc;
+    q.batch_sweep = nullptr;
     q.g = g;
     q.n_chains = n_chains;
     q.chains_per_group = n_chains / n_groups;
@@ -489,74 +635,117 @@ extern "C" int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx
     q.tabs = tabs[slot];
   }
   const int kg = k_inline / 4;
-
-  auto launch_meas = [&](uint32_t sweep_rel, uint32_t meas_rel, const uint32_t* cur) {
-    uint32_t sw = sweep_rel;
-    for (int r = 0; r < n_rows; ++r) {
-      const int slot = schedule[2 * r] == CRITMC_HEATBATH ? 1 : 0;
-      MscParams& q = P[slot];
-      q.cursor = cur;
-      for (int64_t rep = 0; rep < schedule[2 * r + 1]; ++rep) {
-        q.sweep = sw;
-        q.meas = meas_rel;
-        q.col = 0;
-        msc_launch_half(q, keys, rule[slot], kg, pr, s);
-        q.col = 1;
-        msc_launch_half(q, keys, rule[slot], kg, pr, s);
-        ++sw;
-      }
-    }
-  };
-
-  if (mode == 1) {
-    uint32_t sw = sweep0;
-    for (int m = 0; m < n_meas; ++m) {
-      launch_meas(sw, (uint32_t)m, nullptr);
-      sw += (uint32_t)sweeps_per_meas;
-    }
-  } else {
-    // a graph of G measurements replayed with a device cursor
-    const int G = (int)std::max<long long>(
-        1, std::min<long long>(n_meas, 256 / std::max<long long>(1, sweeps_per_meas)));
-    msc_cursor_set<<<1, 1, 0, s>>>(cursor, sweep0, 0);
-    const int n_graph = n_meas / G;
-    if (n_graph > 1) {
-      // the graph depends on the parameters below only: reuse it across calls
-      int dev = 0;
-      cudaGetDevice(&dev);
-      GraphKey key;
-      key.add(0x4d534347u).add(dev).add(G).add(n_rows).add(rule).add(kg).add(pr);
-      key.add_bytes(schedule, sizeof(int64_t) * 2 * n_rows).add_bytes(keys, sizeof(uint32_t) * 2 * n_chains);
-      for (int slot = 0; slot < 2; ++slot) {
-        MscParams& q = P[slot];
-        q.cursor = cursor;
-        q.sweep = q.meas = 0;
-        q.col = q.chain0 = 0;
-        std::memset(q.keys, 0, sizeof(q.keys));
-        key.add(q);
-      }
-      cudaGraphExec_t exec = graph_cache_find(key);
-      if (!exec) {
-        cudaGraph_t graph;
-        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-          return cuda_fail("capture");
-        for (int m = 0; m < G; ++m) launch_meas((uint32_t)(m * sweeps_per_meas), (uint32_t)m, cursor);
-        msc_cursor_bump<<<1, 1, 0, s>>>(cursor, (uint32_t)(G * sweeps_per_meas), (uint32_t)G);
-        if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return cuda_fail("end capture");
-        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ie != cudaSuccess) return cuda_fail("instantiate");
-        graph_cache_insert(key, exec);
-      }
-      for (int i = 0; i < n_graph; ++i) cudaGraphLaunch(exec, s);
-    }
-    const int done = n_graph > 1 ? n_graph * G : 0;
-    for (int m = done; m < n_meas; ++m)
-      launch_meas((uint32_t)(sweep0 + (uint32_t)(m * sweeps_per_meas)), (uint32_t)m, nullptr);
-  }
+  if ((st = msc_launch_schedule(P, rule, keys, n_chains, schedule, n_rows, sweeps_per_meas, n_meas, sweep0, mode, kg,
+                                pr, cursor, s)))
+    return st;
   msc_finalize_kernel<<<n_chains, 256, 0, s>>>((const long long*)acc, (long long*)running,
                                                 (long long*)e_out, (long long*)m_out,
                                                 (long long*)aux_out, n_chains, n_meas);
+  if (int e_ = cuda_check("launch")) return e_;
+  return cs.finish();
+}
+
+extern "C" int64_t critmc_ising_msc_batch_scratch_bytes(int32_t n_chains, int32_t n_meas) {
+  return 256 + (int64_t)n_chains * n_meas * 3 * 8;
+}
+
+extern "C" int32_t critmc_ising_msc_run_batch(const critmc_msc_chain* chains, int32_t n_chains, int32_t dim,
+                                              int32_t lx, int32_t ly, int32_t lz, const uint32_t* tables,
+                                              int32_t n_tables, const int64_t* schedule, int32_t n_rows,
+                                              int32_t n_meas, void* scratch, int32_t mode, void* stream) {
+  clear_error();
+  MscGeom g;
+  int st = msc_geom(dim, lx, ly, lz, g);
+  if (st) return st;
+  if (!chains || !tables || !scratch || !schedule) return fail(CRITMC_ERR_INVALID, "null pointer argument");
+  if (n_chains < 1 || n_chains > CRITMC_MSC_BATCH_MAX)
+    return fail(CRITMC_ERR_INVALID, "a batch holds 1..CRITMC_MSC_BATCH_MAX (16) chains");
+  if (n_tables < 1 || n_tables > MSC_MAX_GROUPS) return fail(CRITMC_ERR_INVALID, "n_tables must be in [1, 16]");
+  if (n_meas < 0) return fail(CRITMC_ERR_INVALID, "n_meas must not be negative");
+  if (n_rows < 1) return fail(CRITMC_ERR_INVALID, "empty schedule");
+  long long sweeps_per_meas = 0;
+  for (int r = 0; r < n_rows; ++r) {
+    const int64_t code = schedule[2 * r], reps = schedule[2 * r + 1];
+    if (code != CRITMC_METROPOLIS && code != CRITMC_HEATBATH)
+      return fail(CRITMC_ERR_UNSUPPORTED, "MSC Ising runs checkerboard metropolis and heatbath rows only");
+    if (reps < 1) return fail(CRITMC_ERR_INVALID, "schedule repetitions must be positive");
+    sweeps_per_meas += reps;
+  }
+  const int run_code = (mode >> 8) & 0xF;
+  if ((mode & ~0xFFF) || run_code > 6) return fail(CRITMC_ERR_INVALID, "mode: bits 8..11 must be 0..6, no higher bits");
+  mode &= 0xFF;
+  if (mode == 0) mode = 3;
+  if (mode != 1 && mode != 3) return fail(CRITMC_ERR_UNSUPPORTED, "mode must be 0, 1 or 3");
+  std::vector<uint32_t> keys(2 * (size_t)n_chains), sweeps(n_chains);
+  for (int c = 0; c < n_chains; ++c) {
+    const critmc_msc_chain& ch = chains[c];
+    if (!ch.spins || !ch.running || !ch.e_out || !ch.m_out || !ch.aux_out)
+      return fail(CRITMC_ERR_INVALID, "batch chain with a null pointer");
+    if (ch.table < 0 || ch.table >= n_tables) return fail(CRITMC_ERR_INVALID, "batch chain table out of range");
+    if ((long long)ch.sweep0 + sweeps_per_meas * (long long)n_meas > 0xFFFFFFFFLL)
+      return fail(CRITMC_ERR_INVALID, "sweep counter would pass 2^32");
+    keys[2 * c] = ch.key[0];
+    keys[2 * c + 1] = ch.key[1];
+    sweeps[c] = ch.sweep0;
+  }
+  if (n_meas == 0) return CRITMC_OK;
+
+  MscTables tabs[2];
+  int rule[2];
+  for (int slot = 0; slot < 2; ++slot) {
+    std::memset(&tabs[slot], 0, sizeof(MscTables));
+    for (int gi = 0; gi < n_tables; ++gi) {
+      const uint32_t* src = tables + (size_t)gi * 4 * CRITMC_NCLS + slot * 2 * CRITMC_NCLS;
+      std::memcpy(tabs[slot].kind[gi], src, CRITMC_NCLS * 4);
+      std::memcpy(tabs[slot].thr[gi], src + CRITMC_NCLS, CRITMC_NCLS * 4);
+    }
+    rule[slot] = msc_pick_rule(&tabs[slot].kind[0][0], &tabs[slot].thr[0][0], 2 * dim,
+                               slot ? CRITMC_HEATBATH : CRITMC_METROPOLIS, n_tables);
+  }
+
+  CaptureStream cs;
+  if ((st = cs.begin(stream))) return st;
+  cudaStream_t s = cs.work;
+  uint32_t* cursor = (uint32_t*)scratch;
+  uint32_t* sweep_dev = (uint32_t*)((char*)scratch + 16);
+  unsigned long long* acc = (unsigned long long*)((char*)scratch + 256);
+  if (cudaMemcpyAsync(sweep_dev, sweeps.data(), 4 * (size_t)n_chains, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return cuda_fail("copy sweep bases");
+  if (cudaMemsetAsync(acc, 0, (size_t)n_chains * n_meas * 3 * 8, s) != cudaSuccess) return cuda_fail("memset");
+
+  const long long col_threads = (long long)n_chains * g.wc * g.rows;
+  int run = 8;
+  while (run > 1 && col_threads / run < 148LL * 1536) run /= 2;
+  if (run_code) run = 1 << (run_code - 1);
+
+  static thread_local MscParams P[2];
+  for (int slot = 0; slot < 2; ++slot) {
+    MscParams& q = P[slot];
+    std::memset(&q, 0, sizeof(MscParams));
+    q.acc = acc;
+    q.batch_sweep = sweep_dev;
+    for (int c = 0; c < n_chains; ++c) {
+      q.batch_spins[c] = chains[c].spins;
+      q.batch_group[c] = (uint32_t)chains[c].table;
+    }
+    q.g = g;
+    q.n_chains = n_chains;
+    q.chains_per_group = 1;
+    q.run = run;
+    q.tabs = tabs[slot];
+  }
+  if ((st = msc_launch_schedule(P, rule, keys.data(), n_chains, schedule, n_rows, sweeps_per_meas, n_meas, 0u, mode,
+                                2, CRITMC_PHILOX_ROUNDS, cursor, s)))
+    return st;
+  MscBatchOut out;
+  std::memset(&out, 0, sizeof(out));
+  for (int c = 0; c < n_chains; ++c) {
+    out.running[c] = (long long*)chains[c].running;
+    out.e_out[c] = (long long*)chains[c].e_out;
+    out.m_out[c] = (long long*)chains[c].m_out;
+    out.aux_out[c] = (long long*)chains[c].aux_out;
+  }
+  msc_finalize_batch_kernel<<<n_chains, 256, 0, s>>>((const long long*)acc, out, n_chains, n_meas);
   if (int e_ = cuda_check("launch")) return e_;
   return cs.finish();
 }
@@ -748,6 +937,7 @@ extern "C" int32_t critmc_ising_msc_run_noalloc(uint32_t* spins, int32_t dim, in
     MscParams& q = P[slot];
     q.spins = spins;
     q.acc = acc;
+    q.batch_sweep = nullptr;
     q.cursor = nullptr;
     q.g = g;
     q.n_chains = n_chains;

@@ -106,6 +106,7 @@ int32_t critmc_ising_class_table(int32_t algo, int32_t z, double beta, double h,
  * k_inline: 4 or 8 acceptance planes resolved inline (tuning only; the
  * results do not depend on it).                                            */
 #define CRITMC_MSC_PHILOX7 0x1000
+#define CRITMC_MSC_BATCH_MAX 16
 int64_t critmc_ising_msc_scratch_bytes(int32_t n_chains, int32_t n_meas);
 int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx, int32_t ly, int32_t lz,
                              int32_t n_chains, const uint32_t* keys, const uint32_t* tables,
@@ -113,6 +114,32 @@ int32_t critmc_ising_msc_run(uint32_t* spins, int32_t dim, int32_t lx, int32_t l
                              int32_t n_rows, int32_t n_meas, int64_t* running, int64_t* e_out,
                              int64_t* m_out, int64_t* aux_out, void* scratch, int32_t mode,
                              int32_t k_inline, void* stream);
+
+/* critmc_ising_msc_run for up to CRITMC_MSC_BATCH_MAX separately allocated
+ * chains of one lattice shape in one call (one launch per half-sweep covers
+ * them all): each chain brings its own lattice, running sums, series outputs
+ * (all DEVICE), Philox key, first sweep and acceptance table (an index into
+ * the HOST tables [n_tables][2][2][16] of critmc_ising_msc_run).  The results
+ * of a chain equal critmc_ising_msc_run's for it alone.  scratch: DEVICE,
+ * critmc_ising_msc_batch_scratch_bytes(n_chains, n_meas) bytes; the call
+ * copies the sweep bases into it.  mode as critmc_ising_msc_run's (no Philox
+ * option; 8 inline planes).  No counterpart in critmc (one chain per
+ * process); the serving loop batches its large lattices with it.          */
+typedef struct {
+  uint32_t* spins;
+  int64_t* running;  /* [2]: E_b, M */
+  int64_t* e_out;    /* [n_meas] */
+  int64_t* m_out;    /* [n_meas] */
+  int64_t* aux_out;  /* [n_meas][4] */
+  uint32_t key[2];
+  uint32_t sweep0;
+  int32_t table;
+} critmc_msc_chain;
+int64_t critmc_ising_msc_batch_scratch_bytes(int32_t n_chains, int32_t n_meas);
+int32_t critmc_ising_msc_run_batch(const critmc_msc_chain* chains, int32_t n_chains, int32_t dim, int32_t lx,
+                                   int32_t ly, int32_t lz, const uint32_t* tables, int32_t n_tables,
+                                   const int64_t* schedule, int32_t n_rows, int32_t n_meas, void* scratch,
+                                   int32_t mode, void* stream);
 
 /* Initial configurations of MSC chains, drawn on the device: start 0 = random
  * (word w of colour c is word 0 of Philox(w, 0, 0x05 | c << 16, 0) with the

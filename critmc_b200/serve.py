@@ -9,10 +9,8 @@ resident on the device, and advances all admitted requests together in ticks:
   per-family kernels (``critmc_run_items``: one thread block per chain,
   blocks pull chains from a queue, the three family kernels side by side);
 * large multi-spin-coded Ising lattices run on the multi-block half-sweep
-  kernel, up to 16 requests of a shape per ``critmc_ising_msc_run_batch``
-  call (one launch per half-sweep covers them all), and large O(n) lattices
-  on the multi-block O(n) kernels (``critmc_on_run_grid``), one library
-  stream per request, next to the item kernels.
+  kernel (``critmc_ising_msc_run``), one library stream per request, next to
+  the item kernels.
 
 Each tick gives every request a slice of sweeps sized so the tick takes about
 ``tick_ms`` of GPU time; requests that arrive meanwhile are admitted at the
@@ -55,15 +53,6 @@ DEFAULT_UPDATES = {"ising": "metropolis", "potts": "metropolis", "xy": "metropol
 _I8, _F8 = np.dtype(np.int64), np.dtype(np.float64)
 _ALIGN = 256
 GRID_MAX_MEAS = 4096  # measurements per grid-lane call (bounds its scratch)
-BATCH_MAX = 16  # requests per batch lane (CRITMC_MSC_BATCH_MAX)
-
-
-class MscChain(ctypes.Structure):
-    """``critmc_msc_chain`` of include/critmc_b200.h (one chain of a batch call)."""
-
-    _fields_ = [("spins", ctypes.c_void_p), ("running", ctypes.c_void_p), ("e_out", ctypes.c_void_p),
-                ("m_out", ctypes.c_void_p), ("aux_out", ctypes.c_void_p), ("key", ctypes.c_uint32 * 2),
-                ("sweep0", ctypes.c_uint32), ("table", ctypes.c_int32)]
 
 # Seconds per sweep of one chain, a + b * sites, by (lane, family): starting
 # values for the tick planner (B200 measurements of one chain alone); the
@@ -75,7 +64,6 @@ COSTS = {
     ("items", "on2"): (3.0e-6, 2.5e-9),
     ("items", "on3"): (4.0e-6, 4.0e-9),
     ("grid", "msc"): (8.7e-6, 2.0e-13),
-    ("batch", "msc"): (8.7e-6, 4.0e-13),  # per request of a batch; the lane's scale absorbs the rest
     ("grid", "on2"): (1.0e-5, 2.0e-10),
     ("grid", "on3"): (1.2e-5, 3.0e-10),
 }
@@ -241,9 +229,7 @@ class _Lane:
 
     An item lane holds the requests of one persistent-kernel group (their
     ticks are one ``critmc_run_items`` call); a grid lane holds one request
-    on the multi-block kernels; a batch lane holds up to 16 large
-    multi-spin-coded Ising requests of one lattice shape, advanced together by
-    one ``critmc_ising_msc_run_batch`` call per tick.  Lanes tick independently, two ticks in
+    on the multi-block kernels.  Lanes tick independently, two ticks in
     flight each, so a lane of short sweeps never waits for a lane of long ones.
     """
 
@@ -255,8 +241,6 @@ class _Lane:
         self.staging = [None, None]
         self.n_ticks = 0
         self.item_buffer = None
-        self.scratch = None  # batch lanes: critmc_ising_msc_run_batch scratch
-        self.shape = None
 
 
 class _Arena:
@@ -330,7 +314,6 @@ class Server:
         self.item_lanes: dict[str, _Lane] = {}
         self.grid_pool = [torch.cuda.Stream(self.device) for _ in range(grid_streams)]
         self.grid_lanes: list[_Lane] = []
-        self.batch_lanes: list[_Lane] = []  # large MSC Ising lattices, by shape, <= 16 requests each
         self._next_grid = 0
         self.arena = _Arena(int(arena_bytes), self.device)
         self.grid_scratch: dict[int, torch.Tensor] = {}
@@ -393,7 +376,6 @@ class Server:
     def _lanes(self):
         yield from self.item_lanes.values()
         yield from self.grid_lanes
-        yield from self.batch_lanes
 
     # ---- admission -------------------------------------------------------
     def _admit(self) -> bool:
@@ -431,16 +413,6 @@ class Server:
             lane = self.item_lanes.get(key)
             if lane is None:
                 lane = self.item_lanes[key] = _Lane("items", job.family, torch.cuda.Stream(self.device))
-        elif job.lane == "batch":
-            # one call shares the lattice shape and the schedule
-            shape = (job.chain.shape, job.sched.tobytes())
-            lane = next((ln for ln in self.batch_lanes if ln.shape == shape and len(ln.jobs) < BATCH_MAX), None)
-            if lane is None:
-                stream = self.grid_pool[self._next_grid % len(self.grid_pool)]
-                self._next_grid += 1
-                lane = _Lane("batch", job.family, stream)
-                lane.shape = shape
-                self.batch_lanes.append(lane)
         else:
             stream = self.grid_pool[self._next_grid % len(self.grid_pool)]
             self._next_grid += 1
@@ -463,11 +435,10 @@ class Server:
             group = family
             fields = [("Eb", _I8, 1), ("M", _I8, 1), ("aux", _I8, 4)]
             t["running"] = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
-            # large lattices: batched multi-block lanes (no cap: one call per tick for up to 16)
-            lane = "batch" if msc and self._wants_grid(req, "msc") else "items"
+            lane = "grid" if msc and self._wants_grid(req, "msc") and self._grid_free() else "items"
             kind = ITEM_MSC_ISING if msc else ITEM_BYTE_ISING
             h = model.h
-            if lane != "items":
+            if lane == "grid":
                 tables = np.ascontiguousarray(model.tables(req.beta)[0])
         elif isinstance(model, Potts):
             family, group, lane, kind, h = "potts", "byte", "items", ITEM_POTTS, 0.0
@@ -528,14 +499,11 @@ class Server:
                 continue
             per = self._sweep_seconds(j) * lane.scale
             n = min(left, max(1, int(self.tick_s / per)))
-            if lane.kind != "items":
+            if lane.kind == "grid":
                 n = min(n, GRID_MAX_MEAS)
             plan.append([j, n])
         if not plan:
             return [], 0.0
-        if lane.kind == "batch":  # one call: every request of the lane gets the same slice
-            n = min(n for _, n in plan)
-            plan = [[j, n] for j, _ in plan]
         predicted = max(self._sweep_seconds(j) * lane.scale * n for j, n in plan)
         return plan, predicted
 
@@ -557,7 +525,6 @@ class Server:
         entries = []
         off = seg
         items = []
-        batch = []
         for j, n in plan:
             entries.append((j, n, off))
             ptrs = []
@@ -573,8 +540,6 @@ class Server:
                 if j.family.startswith("on"):
                     it.sc_out, it.ss_out = ptrs[2], ptrs[3]
                 items.append(it)
-            elif lane.kind == "batch":
-                batch.append((j, ptrs))
             else:
                 self._grid_call(lane, j, n, ptrs)
             off = _round_up(off + j.meas_bytes * n)
@@ -588,8 +553,6 @@ class Server:
                 lane.item_buffer = empty_bytes(_lib.lib().critmc_items_buffer_bytes(2 * len(items) + 64), self.device)
             arr = (CritmcItem * len(items))(*items)
             launch_items(arr, self.device, lane.item_buffer, staging=lane.staging[slot], stream=s.cuda_stream)
-        if batch:
-            self._batch_call(lane, batch, plan[0][1])
         end.record(s)
         with torch.cuda.stream(s):
             self.arena.host[seg:seg + size].copy_(self.arena.dev[seg:seg + size], non_blocking=True)
@@ -618,28 +581,6 @@ class Server:
                          c.key.ctypes.data, betas.ctypes.data, steps.ctypes.data, 1, c.sweep, j.sched.ctypes.data,
                          len(j.sched), n, ptrs[0], ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptr(scratch),
                          c.blocks_per_chain, s.cuda_stream)
-
-    def _batch_call(self, lane: _Lane, batch: list, n: int) -> None:
-        """One critmc_ising_msc_run_batch call for the lane's requests (same slice n)."""
-        j0 = batch[0][0]
-        c0 = j0.chain
-        lx, ly, lz = c0.dims
-        arr = (MscChain * len(batch))()
-        tables = np.ascontiguousarray(np.stack([j.tables for j, _ in batch]))
-        for i, (j, ptrs) in enumerate(batch):
-            c = j.chain
-            arr[i].spins, arr[i].running = ptr(c.words), ptr(j.tensors["running"])
-            arr[i].e_out, arr[i].m_out, arr[i].aux_out = ptrs[0], ptrs[1], ptrs[2]
-            k = c.key.ravel()
-            arr[i].key[0], arr[i].key[1] = int(k[0]), int(k[1])
-            arr[i].sweep0 = c.sweep
-            arr[i].table = i
-        if lane.scratch is None:
-            lane.scratch = empty_bytes(_lib.lib().critmc_ising_msc_batch_scratch_bytes(BATCH_MAX, GRID_MAX_MEAS),
-                                       self.device)
-        _lib.call_on(self.device, "critmc_ising_msc_run_batch", ctypes.cast(arr, ctypes.c_void_p), len(batch),
-                     len(c0.shape), lx, ly, lz, tables.ctypes.data, len(batch), j0.sched.ctypes.data,
-                     len(j0.sched), n, ptr(lane.scratch), 0, lane.stream.cuda_stream)
 
     def _grid_scratch(self, stream: torch.cuda.Stream) -> torch.Tensor:
         key = stream.cuda_stream
@@ -681,8 +622,6 @@ class Server:
         self.arena.release(tick.offset, tick.size)
         if lane.kind == "grid" and not lane.jobs and not lane.inflight:
             self.grid_lanes.remove(lane)
-        if lane.kind == "batch" and not lane.jobs and not lane.inflight:
-            self.batch_lanes.remove(lane)
 
     def _finish(self, j: _Job, now: float) -> None:
         req = j.req

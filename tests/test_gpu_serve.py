@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 REQUESTS = [
     Request("ising", 16, 0.44, 900, seed=1),  # byte lattice item
     Request("ising", 64, 0.4406868, 1200, seed=2),  # multi-spin-coded item
-    Request("ising", 512, 0.45, 300, seed=3),  # multi-block batch lane
+    Request("ising", 512, 0.45, 300, seed=3),  # multi-block lane
     Request("ising", 128, 0.3, 700, seed=4, h=0.2, updates="heatbath"),
     Request("ising", 8, 0.2216546, 500, seed=5, dim=3, updates="2*metropolis+heatbath"),
     Request("potts", 32, 1.42, 800, seed=6, q=10),
@@ -23,9 +23,6 @@ REQUESTS = [
     Request("heisenberg", 16, 0.7, 300, seed=9, updates="metropolis+overrelax"),
     Request("xy", 64, 1.0, 250, seed=10),
     Request("ising", 256, 0.46, 400, seed=11),
-    Request("ising", 512, 0.40, 260, seed=12),  # joins the first 512 request's batch lane
-    Request("ising", 512, 0.47, 180, seed=13, updates="heatbath"),  # another schedule: its own batch lane
-    Request("ising", 512, 0.43, 90, seed=14),
 ]
 
 

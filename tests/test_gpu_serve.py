@@ -23,6 +23,9 @@ REQUESTS = [
     Request("heisenberg", 16, 0.7, 300, seed=9, updates="metropolis+overrelax"),
     Request("xy", 64, 1.0, 250, seed=10),
     Request("ising", 256, 0.46, 400, seed=11),
+    Request("ising", 512, 0.40, 260, seed=12),
+    Request("ising", 512, 0.47, 180, seed=13, updates="heatbath"),
+    Request("ising", 512, 0.43, 90, seed=14),
 ]
 
 

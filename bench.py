@@ -484,7 +484,7 @@ def run_reference(args) -> None:
 
 
 def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0, world: int = 1,
-                max_grid_lanes: int = 8, grid_after_s: float | None = None) -> dict | None:
+                max_grid_lanes: int = 8, grid_after_s: float | None = 1.0) -> dict | None:
     """Continuous-batching server on a seeded Poisson stream of mixed requests.
 
     Workload: ``n_requests`` requests at ``rate``/s, each uniform over 2D Ising
@@ -551,9 +551,9 @@ def main() -> None:
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-only", action="store_true", help="print only the serving run")
     ap.add_argument("--serve-grid-lanes", type=int, default=8, help="requests on multi-block lanes at once")
-    ap.add_argument("--serve-grid-after", type=float, default=-1.0,
-                    help="item-lane seconds (cost model) above which a request takes a multi-block lane; "
-                         "negative (default): every large lattice, first come first served")
+    ap.add_argument("--serve-grid-after", type=float, default=1.0,
+                    help="item-lane seconds (cost model) above which a request takes a multi-block lane "
+                         "(negative: every large lattice, first come first served)")
     ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch", "cluster-sw"],
                     help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()

@@ -201,12 +201,18 @@ _SERVE_PROBES = {
     ("grid", "on2"): ("xy", (64, 128)),
     ("grid", "on3"): ("heisenberg", (64, 128)),
 }
+# teams: (lane, family) -> probe, for every team size
+_TEAM_PROBES = {"msc": ("ising", (256, 1024)), "byte": ("ising", (32, 128)), "potts": ("potts", (64, 128)),
+                "on2": ("xy", (64, 128)), "on3": ("heisenberg", (32, 64))}
+for _t in (2, 4, 8, 16):
+    for _fam, _probe in _TEAM_PROBES.items():
+        _SERVE_PROBES[(f"team{_t}", _fam)] = _probe
 
 
 def calibrate_serving(device=None, *, n_meas: int = 200, force: bool = False) -> dict:
     """Per-lane cost model (a, b): seconds per sweep = a + b * sites, from two sizes each."""
     dev = require_cuda(device)
-    key = cache_key(dev, "serve-costs", (0,), 1, "metropolis", "mixed")
+    key = cache_key(dev, "serve-costs", (1,), 1, "metropolis", "mixed")  # (1,): with team lanes
     if not force:
         hit = _load().get(key)
         if hit:
@@ -221,9 +227,11 @@ def calibrate_serving(device=None, *, n_meas: int = 200, force: bool = False) ->
             req = Request(kind, L, 0.44 if kind == "ising" else (1.4 if kind == "potts" else 1.1), n_meas)
             model, chain, running = open_chain(req, dev)
             sched = req.schedule()
-            if lane == "items":
+            if lane == "items" or lane.startswith("team"):
+                team = int(lane[4:]) if lane.startswith("team") else 1
+
                 def fn():
-                    run_items([ItemRun(model, chain, running, req.beta, sched, n_meas)], dev)
+                    run_items([ItemRun(model, chain, running, req.beta, sched, n_meas, team=team)], dev)
             else:
                 if hasattr(chain, "lane"):
                     chain.lane = "grid"

@@ -67,32 +67,60 @@ struct ByteChain {
   const unsigned long long* weight;  // [8] (Potts)
 };
 
-template <int MODEL, int Z>
+// CL == 1: one block, the lattice in shared memory when a.resident.  CL > 1: a
+// cluster of CL blocks splits every site loop over the lattice in global
+// memory, the cluster barrier separates the colours, and block 0 adds the
+// blocks' per-measurement sums (and, for Potts, their running count changes,
+// snapshotted at each measurement) from distributed shared memory.  A
+// colour's sites are independent and the sums are integers, so every CL
+// gives the same spins and series.  Block 0's thread 0 alone polls the
+// control and passes its answer to all blocks before the barrier that ends a
+// measurement, so the whole team stops at the same measurement.
+template <int MODEL, int Z, int CL = 1>
 __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
+  using T = Team<CL>;
   __shared__ long long red[16];
-  __shared__ int cnt[128];
-  __shared__ int s_stop;
+  __shared__ int cnt[128];  // Potts: counts (CL == 1), this block's count changes (CL > 1)
+  __shared__ int s_stop[2];
+  __shared__ long long part[CL > 1 ? 2 : 1][CL][3];
+  __shared__ int snap[CL > 1 ? 2 : 1][CL > 1 ? 128 : 1];
+  __shared__ long long cnt0[CL > 1 ? 128 : 1];
   const ByteGeom& g = a.g;
   const uint32_t k0 = a.k0, k1 = a.k1;
   const size_t n_sites = 2 * (size_t)g.slots;
   int8_t* gl = a.gl;
-  int8_t* lat = a.resident ? reinterpret_cast<int8_t*>(smem_raw) : gl;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  if (a.resident)
-    for (size_t j = tid; j < n_sites; j += nt) lat[j] = gl[j];
+  const bool resident = CL == 1 && a.resident;
+  int8_t* lat = resident ? reinterpret_cast<int8_t*>(smem_raw) : gl;
+  const unsigned rank = T::rank();
+  const int tid = threadIdx.x, nb_threads = blockDim.x;
+  const uint32_t t0 = rank * blockDim.x + tid, nt = CL * blockDim.x;
+  if (resident)
+    for (size_t j = tid; j < n_sites; j += nb_threads) lat[j] = gl[j];
   const int q = a.q;
   if (MODEL == MODEL_POTTS)
-    for (int k = tid; k < q; k += nt) cnt[k] = (int)a.counts[k];
-  __syncthreads();
+    for (int k = tid; k < q; k += nb_threads) {
+      if constexpr (CL == 1) {
+        cnt[k] = (int)a.counts[k];
+      } else {
+        cnt[k] = 0;
+        cnt0[k] = a.counts[k];
+      }
+    }
+  if (CL > 1 && tid == 0) s_stop[0] = 0;
+  T::sync();
 
   long long e_run = a.running[0];
   long long m_run = (MODEL == MODEL_ISING) ? a.running[1] : 0;
   uint32_t sweep = a.sweep0;
   for (int meas = 0; meas < a.n_meas; ++meas) {
-    if (a.ctl) {  // stop between measurements when the budget or a cancel says so
-      if (tid == 0) s_stop = a.poll->check(*a.ctl);
-      __syncthreads();
-      if (s_stop) break;
+    if constexpr (CL == 1) {
+      if (a.ctl) {  // stop between measurements when the budget or a cancel says so
+        if (tid == 0) s_stop[0] = a.poll->check(*a.ctl);
+        __syncthreads();
+        if (s_stop[0]) break;
+      }
+    } else {
+      if (s_stop[meas & 1]) break;  // block 0's answer, written before the last barrier
     }
     long long dE = 0, dM = 0, nacc = 0;
     for (int row = 0; row < a.n_rows; ++row) {
@@ -102,7 +130,7 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
         for (int c = 0; c < 2; ++c) {
           int8_t* own = lat + (size_t)c * g.slots;
           const int8_t* other = lat + (size_t)(c ^ 1) * g.slots;
-          for (uint32_t s = tid; s < g.slots; s += nt) {
+          for (uint32_t s = t0; s < g.slots; s += nt) {
             int r, i;
             byte_row_index(g, s, r, i);
             uint32_t nb[Z];
@@ -192,7 +220,7 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
               }
             }
           }
-          __syncthreads();
+          T::sync();
         }
         ++sweep;
       }
@@ -200,9 +228,33 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
     dE = block_sum(dE, red);
     dM = block_sum(dM, red);
     nacc = block_sum(nacc, red);
+    if constexpr (CL > 1) {
+      if (tid == 0) {
+        long long* p = T::at(&part[meas & 1][rank][0], 0);
+        p[0] = dE;
+        p[1] = dM;
+        p[2] = nacc;
+      }
+      if (MODEL == MODEL_POTTS)
+        for (int k = tid; k < q; k += nb_threads) snap[meas & 1][k] = cnt[k];
+      if (rank == 0 && tid == 0) {
+        const int stop = a.ctl ? a.poll->check(*a.ctl) : 0;
+        for (int r = 0; r < CL; ++r) *T::at(&s_stop[(meas + 1) & 1], (unsigned)r) = stop;
+      }
+      T::sync();
+      // block 0 adds the blocks' sums; part and snap of this parity are next
+      // written two measurements on, after barriers block 0 passes once done here
+      dE = dM = nacc = 0;
+      if (rank == 0 && tid == 0)
+        for (int r = 0; r < CL; ++r) {
+          dE += part[meas & 1][r][0];
+          dM += part[meas & 1][r][1];
+          nacc += part[meas & 1][r][2];
+        }
+    }
     e_run += dE;
     m_run += dM;
-    if (tid == 0) {
+    if (rank == 0 && tid == 0) {
       a.e_out[meas] = e_run;
       if (MODEL == MODEL_ISING) a.m_out[meas] = m_run;
       a.aux_out[4 * meas + 0] = nacc;
@@ -210,19 +262,37 @@ __device__ void byte_chain_run(const ByteChain& a, unsigned char* smem_raw) {
       a.aux_out[4 * meas + 2] = 0;
       a.aux_out[4 * meas + 3] = 0;
     }
-    if (MODEL == MODEL_POTTS)
-      for (int k = tid; k < q; k += nt) a.counts_out[(size_t)meas * q + k] = cnt[k];
+    if (MODEL == MODEL_POTTS && rank == 0)
+      for (int k = tid; k < q; k += nb_threads) {
+        long long c;
+        if constexpr (CL == 1) {
+          c = cnt[k];
+        } else {
+          c = cnt0[k];
+          for (int r = 0; r < CL; ++r) c += *T::at(&snap[meas & 1][k], (unsigned)r);
+        }
+        a.counts_out[(size_t)meas * q + k] = c;
+      }
   }
-  __syncthreads();
-  if (a.resident)
-    for (size_t j = tid; j < n_sites; j += nt) gl[j] = lat[j];
-  if (tid == 0) {
+  T::sync();
+  if (resident)
+    for (size_t j = tid; j < n_sites; j += nb_threads) gl[j] = lat[j];
+  if (rank == 0 && tid == 0) {
     a.running[0] = e_run;
     if (MODEL == MODEL_ISING) a.running[1] = m_run;
   }
-  if (MODEL == MODEL_POTTS)
-    for (int k = tid; k < q; k += nt) a.counts[k] = cnt[k];
-  __syncthreads();
+  if (MODEL == MODEL_POTTS && rank == 0)
+    for (int k = tid; k < q; k += nb_threads) {
+      long long c;
+      if constexpr (CL == 1) {
+        c = cnt[k];
+      } else {
+        c = cnt0[k];
+        for (int r = 0; r < CL; ++r) c += *T::at(&cnt[k], (unsigned)r);
+      }
+      a.counts[k] = c;
+    }
+  T::sync();
 }
 
 template <int MODEL, int Z>
@@ -429,17 +499,25 @@ __device__ __forceinline__ int byte_geom_device(const critmc_item& it, ByteGeom&
   return 0;
 }
 
+// CL > 1: each item is advanced by a cluster of CL blocks (block 0 takes the
+// item from the queue and hands its index to the others).
+template <int CL>
 __global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_item* items, int n,
                                                                   unsigned* queue, size_t smem, RunCtl ctl) {
+  using T = Team<CL>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int cur;
   CtlPoll poll;
   poll.start();
+  const unsigned rank = T::rank();
   for (;;) {
-    if (threadIdx.x == 0) cur = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
-    __syncthreads();
+    if (rank == 0 && threadIdx.x == 0) {
+      const int v = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
+      for (int r = 0; r < CL; ++r) *T::at(&cur, (unsigned)r) = v;
+    }
+    T::sync();
     const int i = cur;
-    __syncthreads();
+    T::sync();
     if (i >= n) break;
     const critmc_item& it = items[i];
     ByteChain a;
@@ -469,29 +547,37 @@ __global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_i
     a.boltz = reinterpret_cast<const unsigned long long*>(it.boltz);
     a.weight = reinterpret_cast<const unsigned long long*>(it.weight);
     if (it.kind == CRITMC_ITEM_POTTS) {
-      if (it.dim == 1) byte_chain_run<MODEL_POTTS, 2>(a, smem_raw);
-      else if (it.dim == 2) byte_chain_run<MODEL_POTTS, 4>(a, smem_raw);
-      else byte_chain_run<MODEL_POTTS, 6>(a, smem_raw);
+      if (it.dim == 1) byte_chain_run<MODEL_POTTS, 2, CL>(a, smem_raw);
+      else if (it.dim == 2) byte_chain_run<MODEL_POTTS, 4, CL>(a, smem_raw);
+      else byte_chain_run<MODEL_POTTS, 6, CL>(a, smem_raw);
     } else {
-      if (it.dim == 1) byte_chain_run<MODEL_ISING, 2>(a, smem_raw);
-      else if (it.dim == 2) byte_chain_run<MODEL_ISING, 4>(a, smem_raw);
-      else byte_chain_run<MODEL_ISING, 6>(a, smem_raw);
+      if (it.dim == 1) byte_chain_run<MODEL_ISING, 2, CL>(a, smem_raw);
+      else if (it.dim == 2) byte_chain_run<MODEL_ISING, 4, CL>(a, smem_raw);
+      else byte_chain_run<MODEL_ISING, 6, CL>(a, smem_raw);
     }
   }
 }
 
-int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, int team, const RunCtl& ctl,
                       cudaStream_t s) {
+  switch (team) {
+    case 2: return launch_team(byte_items_kernel<2>, 2, ITEM_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    case 4: return launch_team(byte_items_kernel<4>, 4, ITEM_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    case 8: return launch_team(byte_items_kernel<8>, 8, ITEM_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    case 16: return launch_team(byte_items_kernel<16>, 16, ITEM_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    default: break;
+  }
+  auto kern = byte_items_kernel<1>;
   if (smem > 0 &&  // static + dynamic may pass 48 KiB
-      cudaFuncSetAttribute(byte_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, byte_items_kernel, ITEM_THREADS, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ITEM_THREADS, smem);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
-  byte_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem, ctl);
+  kern<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, smem, ctl);
   if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }

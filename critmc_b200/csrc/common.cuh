@@ -1,5 +1,6 @@
 // Device helpers shared by every sampler kernel of the library.
 #pragma once
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -167,6 +168,36 @@ struct CtlPoll {
       if (st) return st;
     }
     return 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Teams: the thread blocks that advance one work item together.  CL == 1 is
+// one block; CL > 1 a thread-block cluster of CL blocks on CL SMs of one GPC
+// (the hardware schedules a cluster's blocks together).  sync() is the block
+// barrier, or the cluster barrier (barrier.cluster.arrive has release and
+// barrier.cluster.wait acquire semantics at cluster scope): what any thread of
+// the team wrote before it, to shared or global memory, every thread of the
+// team sees after it.  Every thread of every block of a team must reach the
+// same sequence of sync() calls, so all control flow around them depends only
+// on values that are the same in the whole team.  at(p, r) is block r's copy
+// of the shared variable p (distributed shared memory).
+// ---------------------------------------------------------------------------
+template <int CL>
+struct Team {
+  static_assert(CL == 1 || CL == 2 || CL == 4 || CL == 8 || CL == 16, "team sizes: 1, 2, 4, 8 or 16 blocks");
+  __device__ static __forceinline__ unsigned rank() {
+    if constexpr (CL == 1) return 0;
+    else return cooperative_groups::this_cluster().block_rank();
+  }
+  __device__ static __forceinline__ void sync() {
+    if constexpr (CL == 1) __syncthreads();
+    else cooperative_groups::this_cluster().sync();
+  }
+  template <typename T>
+  __device__ static __forceinline__ T* at(T* p, unsigned r) {
+    if constexpr (CL == 1) return p;
+    else return cooperative_groups::this_cluster().map_shared_rank(p, r);
   }
 };
 

@@ -14,7 +14,7 @@ using namespace critmc;
 
 namespace {
 
-constexpr size_t ITEMS_HEADER = 64;  // queue counters of the families
+constexpr size_t ITEMS_HEADER = 256;  // queue counters of the launch groups
 constexpr int ITEMS_SMEM_DEFAULT = 200 * 1024;
 
 int family_of(int kind) {
@@ -27,13 +27,28 @@ int family_of(int kind) {
   }
 }
 
-// Launch groups: one persistent kernel each.  0 multi-spin-coded Ising,
-// 1 byte lattices, 2..7 O(n) by (n, dim) (a kernel per variant).
-constexpr int N_GROUPS = 8;
+// Kernel groups: 0 multi-spin-coded Ising, 1 byte lattices, 2..7 O(n) by
+// (n, dim) (a kernel per variant).  Launch groups: kernel group x team size,
+// one persistent kernel each.
+constexpr int N_KGROUPS = 8;
+constexpr int N_TEAMS = 5;  // 1, 2, 4, 8, 16 blocks per item
+constexpr int N_GROUPS = N_KGROUPS * N_TEAMS;
+static_assert(N_GROUPS * sizeof(unsigned) <= ITEMS_HEADER, "queue counters");
+int team_slot(int team) {
+  switch (team) {
+    case 0:
+    case 1: return 0;
+    case 2: return 1;
+    case 4: return 2;
+    case 8: return 3;
+    case 16: return 4;
+    default: return -1;
+  }
+}
 int group_of(const critmc_item& it) {
   const int fam = family_of(it.kind);
-  if (fam < 2) return fam;
-  return 2 + (it.q_or_n - 2) * 3 + (it.dim - 1);
+  const int kg = fam < 2 ? fam : 2 + (it.q_or_n - 2) * 3 + (it.dim - 1);
+  return kg * N_TEAMS + team_slot(it.team);
 }
 
 int check_schedule(const critmc_item& it) {
@@ -51,6 +66,7 @@ int check_schedule(const critmc_item& it) {
 int check_item(const critmc_item& it) {
   const int fam = family_of(it.kind);
   if (fam < 0) return fail(CRITMC_ERR_INVALID, "unknown item kind");
+  if (team_slot(it.team) < 0) return fail(CRITMC_ERR_INVALID, "item team must be 0, 1, 2, 4, 8 or 16 blocks");
   if (!it.spins || !it.e_out || !it.vec_out || !it.aux_out) return fail(CRITMC_ERR_INVALID, "item with a null pointer");
   if (it.n_meas < 0) return fail(CRITMC_ERR_INVALID, "item n_meas must not be negative");
   int st = check_schedule(it);
@@ -61,7 +77,8 @@ int check_item(const critmc_item& it) {
   if (fam == 0) {
     MscGeom g;
     if ((st = msc_geom(it.dim, it.lx, it.ly, it.lz, g))) return st;
-    if (2 * (size_t)g.words * 4 > 128 * 1024) return fail(CRITMC_ERR_UNSUPPORTED, "MSC items hold at most 2^20 sites (128 KiB)");
+    if (it.team <= 1 && 2 * (size_t)g.words * 4 > 128 * 1024)
+      return fail(CRITMC_ERR_UNSUPPORTED, "one-block MSC items hold at most 2^20 sites (128 KiB)");
     if (!it.running) return fail(CRITMC_ERR_INVALID, "item with a null pointer");
   } else {
     ByteGeom g;
@@ -76,6 +93,7 @@ int check_item(const critmc_item& it) {
 }
 
 size_t item_smem(const critmc_item& it, int fam, size_t limit) {
+  if (it.team > 1) return 0;  // teams update the lattice in global memory
   if (fam == 0) {
     MscGeom g;
     msc_geom(it.dim, it.lx, it.ly, it.lz, g);
@@ -125,23 +143,21 @@ namespace {
 // sequence is serialised per process so the fork/join events are never
 // re-recorded while a wait on them is being enqueued.
 struct FamilyStreams {
-  bool ready = false;
   cudaStream_t aux[N_GROUPS] = {};
   cudaEvent_t fork = nullptr, join[N_GROUPS] = {};
 };
 std::mutex g_family_mutex;
 FamilyStreams g_family[64];
 
-int family_streams(int dev, FamilyStreams*& out) {
+// the fork event and, made on first use, the streams of the launch groups in `used`
+int family_streams(int dev, const int (&used)[N_GROUPS], FamilyStreams*& out) {
   if (dev < 0 || dev >= 64) return fail(CRITMC_ERR_UNSUPPORTED, "device ordinal above 63");
   FamilyStreams& f = g_family[dev];
-  if (!f.ready) {
-    for (int k = 0; k < N_GROUPS; ++k) {
-      if (cudaStreamCreateWithFlags(&f.aux[k], cudaStreamNonBlocking) != cudaSuccess) return cuda_fail("stream");
-      if (cudaEventCreateWithFlags(&f.join[k], cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
-    }
-    if (cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
-    f.ready = true;
+  if (!f.fork && cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
+  for (int k = 0; k < N_GROUPS; ++k) {
+    if (!used[k] || f.aux[k]) continue;
+    if (cudaStreamCreateWithFlags(&f.aux[k], cudaStreamNonBlocking) != cudaSuccess) return cuda_fail("stream");
+    if (cudaEventCreateWithFlags(&f.join[k], cudaEventDisableTiming) != cudaSuccess) return cuda_fail("event");
   }
   out = &f;
   return CRITMC_OK;
@@ -184,7 +200,7 @@ extern "C" int32_t critmc_run_items_ctl(const critmc_item* items, int32_t n_item
       if (group_of(items[i]) != f) continue;
       sorted[fill++] = items[i];
       ++count[f];
-      smem[f] = std::max(smem[f], item_smem(items[i], family_of(items[i].kind), limit));
+      smem[f] = std::max(smem[f], item_smem(items[i], family_of(items[i].kind), limit));  // per launch group
     }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail("device");
@@ -201,7 +217,7 @@ extern "C" int32_t critmc_run_items_ctl(const critmc_item* items, int32_t n_item
   FamilyStreams* fs = nullptr;
   if (groups > 1) {
     lock.lock();
-    int st = family_streams(dev, fs);
+    int st = family_streams(dev, count, fs);
     if (st) return st;
     if (cudaEventRecord(fs->fork, s) != cudaSuccess) return cuda_fail("event record");
   }
@@ -215,9 +231,10 @@ extern "C" int32_t critmc_run_items_ctl(const critmc_item* items, int32_t n_item
     }
     int st = CRITMC_OK;
     const critmc_item* first = sorted + offset;
-    if (f == 0) st = msc_items_launch(dev_items + offset, count[f], queues + f, smem[f], rc, fstream);
-    else if (f == 1) st = byte_items_launch(dev_items + offset, count[f], queues + f, smem[f], rc, fstream);
-    else st = on_items_launch(dev_items + offset, count[f], first->q_or_n, first->dim, queues + f, smem[f], rc,
+    const int kg = f / N_TEAMS, team = 1 << (f % N_TEAMS);
+    if (kg == 0) st = msc_items_launch(dev_items + offset, count[f], queues + f, smem[f], team, rc, fstream);
+    else if (kg == 1) st = byte_items_launch(dev_items + offset, count[f], queues + f, smem[f], team, rc, fstream);
+    else st = on_items_launch(dev_items + offset, count[f], first->q_or_n, first->dim, queues + f, smem[f], team, rc,
                               fstream);
     if (st) return st;
     if (fs) {

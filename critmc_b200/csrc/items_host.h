@@ -11,14 +11,17 @@ namespace critmc {
 constexpr int ITEM_THREADS = 512;
 
 // Each launcher starts a persistent kernel over `n` items at `items` (device)
-// whose blocks pull item indices from *queue (zeroed by the caller).
-// `ctl` bounds the run (all null: unbounded).
-int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+// whose blocks pull item indices from *queue (zeroed by the caller).  team 1:
+// one block per item (`smem` bytes of dynamic shared memory for resident
+// lattices); team 2, 4, 8 or 16: a thread-block cluster of that many blocks
+// per item, the lattice in global memory.  `ctl` bounds the run (all null:
+// unbounded).
+int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, int team, const RunCtl& ctl,
                      cudaStream_t s);
-int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, int team, const RunCtl& ctl,
                       cudaStream_t s);
 // O(n): all n items share n_comp and dim (one kernel per variant)
-int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem,
+int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem, int team,
                     const RunCtl& ctl, cudaStream_t s);
 
 }  // namespace critmc

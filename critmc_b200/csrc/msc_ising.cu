@@ -107,11 +107,14 @@ __device__ __noinline__ int3 msc_flush(const MscRule<Z, RULE> rule, const MscGeo
 // One colour of one sweep.  grid: x = column/run tiles, y = chain of the launch.
 // Thread t walks `run` consecutive rows of column k = t mod wc.  PR: Philox
 // rounds of the acceptance planes (10, or 7 when the caller asks for it).
-// Three blocks per SM (up to 85 registers a thread): the kernel is issue bound,
-// and fewer rematerialised values beat the fourth block's latency hiding.
 // BATCH: the chains of the launch are separately allocated (batch_* fields).
+// The kernel is issue bound.  2D: each loop step updates two rows, whose
+// loads, Philox evaluations and comparisons are independent and interleave,
+// at two blocks per SM (up to 128 registers a thread, nothing rematerialised):
+// +5 % over one row per step at three blocks per SM (85 registers).  3D: one
+// row per step, three blocks per SM.
 template <int Z, int RULE, int KG, int PR, bool BATCH>
-__global__ void __launch_bounds__(MSC_THREADS, 3)
+__global__ void __launch_bounds__(MSC_THREADS, Z == 4 ? 2 : 3)
     msc_halfsweep_kernel(const __grid_constant__ MscParams P) {
   __shared__ MscFix fix[MSC_WARPS][MSC_FIXCAP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -151,59 +154,106 @@ __global__ void __launch_bounds__(MSC_THREADS, 3)
     nf = 0;
   };
 
-  // 2D: sliding window down the column over the other colour
-  uint32_t o_m = 0, o_c = 0;
-  if constexpr (Z == 4) {
-    if (r0 < g.rows) {
-      const int ym = (r0 == 0) ? g.ly - 1 : r0 - 1;
-      o_m = other[CRITMC_IDX((size_t)ym * g.wc + k, g.words)];
-      o_c = other[CRITMC_IDX((size_t)r0 * g.wc + k, g.words)];
-    }
-  }
-#pragma unroll 1
-  for (int i = 0; i < P.run; ++i) {
-    const int r = r0 + i;
-    const bool valid = r < g.rows;
-    const uint32_t widx = (uint32_t)r * g.wc + k;
-    MscWord w;
-    w.U = 0;
-    uint32_t s_new = 0;
-    if (valid) {
-      uint32_t n[Z];
-      if constexpr (Z == 4) {
-        const int y = r;
-        const int yp = (y == g.ly - 1) ? 0 : y + 1;
-        const uint32_t o_p = other[CRITMC_IDX((size_t)yp * g.wc + k, g.words)];
-        const int p = (P.col + y) & 1;
-        const int ka = p ? ((k == g.wc - 1) ? 0 : k + 1) : ((k == 0) ? g.wc - 1 : k - 1);
-        const uint32_t adj = other[CRITMC_IDX((size_t)y * g.wc + ka, g.words)];
-        n[0] = o_c;
-        n[1] = p ? __funnelshift_r(o_c, adj, 1) : __funnelshift_l(adj, o_c, 1);
-        n[2] = o_m;
-        n[3] = o_p;
-        o_m = o_c;
-        o_c = o_p;
-      } else {
-        int y, z, kk;
-        msc_row_coords<Z>(g, widx, y, z, kk);
-        msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
-      }
-      rule.classify(own[CRITMC_IDX(widx, g.words)], n, w);
-      const critmc_plane_word_t pw = critmc_plane_word(&ps, widx);
-#pragma unroll
-      for (int grp = 0; grp < KG; ++grp)
-        msc_resolve<Z, RULE>(rule, w, critmc_plane_group_rounds(&ps, pw, grp, PR), grp,
-                             PRE ? &pre[4 * grp][0] : nullptr);
-      s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
-      msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, dE, dM, nacc);
-      if (w.U == 0) own[CRITMC_IDX(widx, g.words)] = s_new;
-    }
+  auto defer = [&](const MscWord& w, uint32_t widx) {  // a word with undecided lanes goes on the list
     const uint32_t need = __ballot_sync(0xffffffffu, w.U != 0);
     if (need) {
       const int cnt = __popc(need);
       if (nf + cnt > MSC_FIXCAP) flush();
       if (w.U != 0) fix[warp][nf + __popc(need & lt_mask)] = MscFix{widx, w.U, w.D};
       nf += cnt;
+    }
+  };
+
+  if constexpr (Z == 4) {
+    // sliding window down the column over the other colour: rows r-1 (o_m) and r (o_c)
+    uint32_t o_m = 0, o_c = 0;
+    if (r0 < g.rows) {
+      const int ym = (r0 == 0) ? g.ly - 1 : r0 - 1;
+      o_m = other[CRITMC_IDX((size_t)ym * g.wc + k, g.words)];
+      o_c = other[CRITMC_IDX((size_t)r0 * g.wc + k, g.words)];
+    }
+    const int kplus = (k == g.wc - 1) ? 0 : k + 1, kminus = (k == 0) ? g.wc - 1 : k - 1;
+#pragma unroll 1
+    for (int i = 0; i < P.run; i += 2) {  // rows a = r0 + i and b = a + 1
+      const int ra = r0 + i, rb = ra + 1;
+      const bool va = ra < g.rows, vb = (i + 1 < P.run) && (rb < g.rows);
+      const uint32_t wa = (uint32_t)ra * g.wc + k, wb = (uint32_t)rb * g.wc + k;
+      const int pa = (P.col + ra) & 1, pb = pa ^ 1;
+      uint32_t o_p1 = 0, o_p2 = 0, adjA = 0, adjB = 0, ownA = 0, ownB = 0;
+      if (va) {
+        const int yp = (ra == g.ly - 1) ? 0 : ra + 1;
+        o_p1 = other[CRITMC_IDX((size_t)yp * g.wc + k, g.words)];
+        adjA = other[CRITMC_IDX((size_t)ra * g.wc + (pa ? kplus : kminus), g.words)];
+        ownA = own[CRITMC_IDX(wa, g.words)];
+      }
+      if (vb) {
+        const int yp = (rb == g.ly - 1) ? 0 : rb + 1;
+        o_p2 = other[CRITMC_IDX((size_t)yp * g.wc + k, g.words)];
+        adjB = other[CRITMC_IDX((size_t)rb * g.wc + (pb ? kplus : kminus), g.words)];
+        ownB = own[CRITMC_IDX(wb, g.words)];
+      }
+      uint32_t nA[4], nB[4];
+      nA[0] = o_c;
+      nA[1] = pa ? __funnelshift_r(o_c, adjA, 1) : __funnelshift_l(adjA, o_c, 1);
+      nA[2] = o_m;
+      nA[3] = o_p1;
+      nB[0] = o_p1;
+      nB[1] = pb ? __funnelshift_r(o_p1, adjB, 1) : __funnelshift_l(adjB, o_p1, 1);
+      nB[2] = o_c;
+      nB[3] = o_p2;
+      o_m = o_p1;
+      o_c = o_p2;
+      MscWord A, B;
+      rule.classify(ownA, nA, A);
+      rule.classify(ownB, nB, B);
+      const critmc_plane_word_t pwa = critmc_plane_word(&ps, wa);
+      const critmc_plane_word_t pwb = critmc_plane_word(&ps, wb);
+#pragma unroll
+      for (int grp = 0; grp < KG; ++grp) {
+        const critmc_u32x4 xa = critmc_plane_group_rounds(&ps, pwa, grp, PR);
+        const critmc_u32x4 xb = critmc_plane_group_rounds(&ps, pwb, grp, PR);
+        msc_resolve<Z, RULE>(rule, A, xa, grp, PRE ? &pre[4 * grp][0] : nullptr);
+        msc_resolve<Z, RULE>(rule, B, xb, grp, PRE ? &pre[4 * grp][0] : nullptr);
+      }
+      if (!va) A.U = 0;
+      if (!vb) B.U = 0;
+      const uint32_t sa = (RULE == RULE_HB0) ? A.D : (A.s ^ A.D);
+      const uint32_t sb = (RULE == RULE_HB0) ? B.D : (B.s ^ B.D);
+      if (va) {
+        msc_obs<Z>((A.s ^ sa) & ~A.U, A.s, A.anti, dE, dM, nacc);
+        if (A.U == 0) own[CRITMC_IDX(wa, g.words)] = sa;
+      }
+      if (vb) {
+        msc_obs<Z>((B.s ^ sb) & ~B.U, B.s, B.anti, dE, dM, nacc);
+        if (B.U == 0) own[CRITMC_IDX(wb, g.words)] = sb;
+      }
+      defer(A, wa);
+      defer(B, wb);
+    }
+  } else {
+#pragma unroll 1
+    for (int i = 0; i < P.run; ++i) {
+      const int r = r0 + i;
+      const bool valid = r < g.rows;
+      const uint32_t widx = (uint32_t)r * g.wc + k;
+      MscWord w;
+      w.U = 0;
+      if (valid) {
+        uint32_t n[Z];
+        int y, z, kk;
+        msc_row_coords<Z>(g, widx, y, z, kk);
+        msc_neighbours<Z>(other, g, (int)col, y, z, k, n);
+        rule.classify(own[CRITMC_IDX(widx, g.words)], n, w);
+        const critmc_plane_word_t pw = critmc_plane_word(&ps, widx);
+#pragma unroll
+        for (int grp = 0; grp < KG; ++grp)
+          msc_resolve<Z, RULE>(rule, w, critmc_plane_group_rounds(&ps, pw, grp, PR), grp,
+                               PRE ? &pre[4 * grp][0] : nullptr);
+        const uint32_t s_new = (RULE == RULE_HB0) ? w.D : (w.s ^ w.D);
+        msc_obs<Z>((w.s ^ s_new) & ~w.U, w.s, w.anti, dE, dM, nacc);
+        if (w.U == 0) own[CRITMC_IDX(widx, g.words)] = s_new;
+      }
+      defer(w, widx);
     }
   }
   if (nf) flush();
@@ -977,8 +1027,8 @@ namespace critmc {
 
 constexpr int MSCI_WARPS = ITEM_THREADS / 32;
 
-// one colour of one sweep over the resident lattice
-template <int Z, int RULE>
+// one colour of one sweep (CL > 1: the words are split over the team's blocks)
+template <int Z, int RULE, int CL>
 __device__ void msci_colour(const MscRule<Z, RULE>& rule, const MscGeom& g, uint32_t* lat, int c,
                             uint32_t sweep, uint32_t k0, uint32_t k1, MscFix (*fix)[64],
                             long long& dE, long long& dM, long long& nacc) {
@@ -1008,9 +1058,11 @@ __device__ void msci_colour(const MscRule<Z, RULE>& rule, const MscGeom& g, uint
     __syncwarp();
     nf = 0;
   };
-  const uint32_t rounds = (g.words + ITEM_THREADS - 1) / ITEM_THREADS;
+  constexpr uint32_t stride = (uint32_t)CL * ITEM_THREADS;
+  const uint32_t t0 = Team<CL>::rank() * ITEM_THREADS + threadIdx.x;
+  const uint32_t rounds = (g.words + stride - 1) / stride;  // the same for the whole team
   for (uint32_t it = 0; it < rounds; ++it) {
-    const uint32_t widx = it * ITEM_THREADS + threadIdx.x;
+    const uint32_t widx = it * stride + t0;
     MscWord w;
     w.U = 0;
     if (widx < g.words) {
@@ -1037,27 +1089,46 @@ __device__ void msci_colour(const MscRule<Z, RULE>& rule, const MscGeom& g, uint
   dE += idE;
   dM += idM;
   nacc += inacc;
-  __syncthreads();
+  Team<CL>::sync();
 }
 
-template <int Z>
+// CL == 1: one block, the lattice copied into shared memory (`lat`).  CL > 1:
+// a cluster of CL blocks updates the lattice in global memory, the cluster
+// barrier separating the colours, and block 0 adds the blocks' sums from
+// distributed shared memory; the same spins and series for every CL (a
+// colour's words are independent, the sums are integers).  Block 0's thread 0
+// alone polls the control and passes its answer to all blocks before the
+// barrier that ends a measurement.
+template <int Z, int CL>
 __device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[64], const RunCtl* ctl,
                            CtlPoll* poll) {
+  using T = Team<CL>;
   __shared__ long long red[MSCI_WARPS];
-  __shared__ int s_stop;
+  __shared__ int s_stop[2];
+  __shared__ long long part[CL > 1 ? 2 : 1][CL][3];
   MscGeom g;
   msc_geom_device(it.dim, it.lx, it.ly, it.lz, g);
   uint32_t* gl = reinterpret_cast<uint32_t*>(it.spins);
   const int tid = threadIdx.x;
-  for (uint32_t j = tid; j < 2 * g.words; j += ITEM_THREADS) lat[j] = gl[j];
-  __syncthreads();
+  const unsigned rank = T::rank();
+  if constexpr (CL == 1) {
+    for (uint32_t j = tid; j < 2 * g.words; j += ITEM_THREADS) lat[j] = gl[j];
+  } else {
+    lat = gl;
+    if (tid == 0) s_stop[0] = 0;
+  }
+  T::sync();
   long long e_run = it.running[0], m_run = it.running[1];
   uint32_t sweep = it.sweep0;
   for (int meas = 0; meas < it.n_meas; ++meas) {
-    if (ctl) {  // stop between measurements when the budget or a cancel says so
-      if (tid == 0) s_stop = poll->check(*ctl);
-      __syncthreads();
-      if (s_stop) break;
+    if constexpr (CL == 1) {
+      if (ctl) {  // stop between measurements when the budget or a cancel says so
+        if (tid == 0) s_stop[0] = poll->check(*ctl);
+        __syncthreads();
+        if (s_stop[0]) break;
+      }
+    } else {
+      if (s_stop[meas & 1]) break;  // block 0's answer, written before the last barrier
     }
     long long dE = 0, dM = 0, nacc = 0;
     for (int row = 0; row < it.n_rows; ++row) {
@@ -1068,16 +1139,16 @@ __device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[6
         for (int c = 0; c < 2; ++c) {
           switch (it.rule[slot]) {
             case RULE_METRO0:
-              msci_colour<Z, RULE_METRO0>(MscRule<Z, RULE_METRO0>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              msci_colour<Z, RULE_METRO0, CL>(MscRule<Z, RULE_METRO0>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
               break;
             case RULE_HB0:
-              msci_colour<Z, RULE_HB0>(MscRule<Z, RULE_HB0>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              msci_colour<Z, RULE_HB0, CL>(MscRule<Z, RULE_HB0>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
               break;
             case RULE_GEN:
-              msci_colour<Z, RULE_GEN>(MscRule<Z, RULE_GEN>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              msci_colour<Z, RULE_GEN, CL>(MscRule<Z, RULE_GEN>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
               break;
             default:
-              msci_colour<Z, RULE_GENSPIN>(MscRule<Z, RULE_GENSPIN>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
+              msci_colour<Z, RULE_GENSPIN, CL>(MscRule<Z, RULE_GENSPIN>{kd, th}, g, lat, c, sweep, it.key[0], it.key[1], fix, dE, dM, nacc);
               break;
           }
         }
@@ -1095,9 +1166,28 @@ __device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[6
       for (int w = 0; w < MSCI_WARPS; ++w) tot[q] += red[w];
       __syncthreads();
     }
+    if constexpr (CL > 1) {
+      if (tid == 0) {
+        long long* p = T::at(&part[meas & 1][rank][0], 0);
+        p[0] = tot[0];
+        p[1] = tot[1];
+        p[2] = tot[2];
+      }
+      if (rank == 0 && tid == 0) {
+        const int stop = ctl ? poll->check(*ctl) : 0;
+        for (int r = 0; r < CL; ++r) *T::at(&s_stop[(meas + 1) & 1], (unsigned)r) = stop;
+      }
+      T::sync();
+      // part of this parity is next written two measurements on, after
+      // barriers that block 0 passes once it is done here
+      tot[0] = tot[1] = tot[2] = 0;
+      if (rank == 0 && tid == 0)
+        for (int r = 0; r < CL; ++r)
+          for (int q = 0; q < 3; ++q) tot[q] += part[meas & 1][r][q];
+    }
     e_run += tot[0];
     m_run += tot[1];
-    if (tid == 0) {
+    if (rank == 0 && tid == 0) {
       reinterpret_cast<long long*>(it.e_out)[meas] = e_run;
       reinterpret_cast<long long*>(it.vec_out)[meas] = m_run;
       it.aux_out[4 * meas + 0] = tot[2];
@@ -1106,16 +1196,21 @@ __device__ void msci_chain(const critmc_item& it, uint32_t* lat, MscFix (*fix)[6
       it.aux_out[4 * meas + 3] = 0;
     }
   }
-  for (uint32_t j = tid; j < 2 * g.words; j += ITEM_THREADS) gl[j] = lat[j];
-  if (tid == 0) {
+  if constexpr (CL == 1)
+    for (uint32_t j = tid; j < 2 * g.words; j += ITEM_THREADS) gl[j] = lat[j];
+  if (rank == 0 && tid == 0) {
     it.running[0] = e_run;
     it.running[1] = m_run;
   }
-  __syncthreads();
+  T::sync();
 }
 
+// CL > 1: each item is advanced by a cluster of CL blocks (block 0 takes the
+// item from the queue and hands its index to the others).
+template <int CL>
 __global__ void __launch_bounds__(ITEM_THREADS) msc_items_kernel(const critmc_item* items, int n,
                                                                  unsigned* queue, RunCtl ctl) {
+  using T = Team<CL>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ MscFix fix[MSCI_WARPS][64];
   __shared__ int cur;
@@ -1123,30 +1218,42 @@ __global__ void __launch_bounds__(ITEM_THREADS) msc_items_kernel(const critmc_it
   CtlPoll poll;
   poll.start();
   const RunCtl* pc = ctl.status ? &ctl : nullptr;
+  const unsigned rank = T::rank();
   for (;;) {
-    if (threadIdx.x == 0) cur = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
-    __syncthreads();
+    if (rank == 0 && threadIdx.x == 0) {
+      const int v = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
+      for (int r = 0; r < CL; ++r) *T::at(&cur, (unsigned)r) = v;
+    }
+    T::sync();
     const int i = cur;
-    __syncthreads();
+    T::sync();
     if (i >= n) break;
     const critmc_item& it = items[i];
-    if (it.dim == 2) msci_chain<4>(it, lat, fix, pc, &poll);
-    else msci_chain<6>(it, lat, fix, pc, &poll);
+    if (it.dim == 2) msci_chain<4, CL>(it, lat, fix, pc, &poll);
+    else msci_chain<6, CL>(it, lat, fix, pc, &poll);
   }
 }
 
-int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
+int msc_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, int team, const RunCtl& ctl,
                      cudaStream_t s) {
+  switch (team) {
+    case 2: return launch_team(msc_items_kernel<2>, 2, ITEM_THREADS, n, s, items, n, queue, ctl);
+    case 4: return launch_team(msc_items_kernel<4>, 4, ITEM_THREADS, n, s, items, n, queue, ctl);
+    case 8: return launch_team(msc_items_kernel<8>, 8, ITEM_THREADS, n, s, items, n, queue, ctl);
+    case 16: return launch_team(msc_items_kernel<16>, 16, ITEM_THREADS, n, s, items, n, queue, ctl);
+    default: break;
+  }
+  auto kern = msc_items_kernel<1>;
   if (smem > 0 &&  // static + dynamic may pass 48 KiB
-      cudaFuncSetAttribute(msc_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, msc_items_kernel, ITEM_THREADS, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ITEM_THREADS, smem);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
-  msc_items_kernel<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, ctl);
+  kern<<<grid, ITEM_THREADS, smem, s>>>(items, n, queue, ctl);
   if (int e_ = cuda_check("launch")) return e_;
   return CRITMC_OK;
 }

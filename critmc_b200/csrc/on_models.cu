@@ -379,28 +379,48 @@ __host__ __device__ inline int on_site_threads(uint32_t slots) {
   return (int)(t < 32 ? 32 : (t > (uint32_t)ON_THREADS ? (uint32_t)ON_THREADS : t));
 }
 
-template <int N, int Z>
+// CL == 1: one block, the lattice in shared memory when P.resident.  CL > 1: a
+// cluster of CL blocks splits every site loop, the lattice stays in global
+// memory (L2-resident at the sizes that use teams), the cluster barrier
+// separates the colours, and the blocks' partial sums meet in block 0's
+// shared memory.  The site order within a colour does not matter (a colour's
+// sites are independent) and the sums are integers, so every CL gives the
+// same spins and series.  Block 0's thread 0 alone polls the control and
+// passes its answer to all blocks before the barrier that ends a
+// measurement, so the whole team stops at the same measurement.
+template <int N, int Z, int CL = 1>
 __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
+  using T = Team<CL>;
   constexpr int NV = on_nv<N, Z>();
   __shared__ long long red[NV][ON_THREADS / 32];
-  __shared__ int s_stop;
+  __shared__ long long part[CL > 1 ? 2 : 1][CL][NV];  // team: block totals by measurement parity
+  __shared__ int s_stop[2];
   const ByteGeom& g = P.g;
   const size_t n_sites = 2 * (size_t)g.slots;
   float* gl = P.gl;
-  float* lat = P.resident ? reinterpret_cast<float*>(smem_raw) : gl;
-  // idle threads (tid >= nt) start every site loop past its end but take part in the barriers
-  const int tid = threadIdx.x, nt = P.nt;
-  const uint32_t t0 = tid < nt ? (uint32_t)tid : 0x7fffffffu;
-  if (P.resident)
+  const bool resident = CL == 1 && P.resident;
+  float* lat = resident ? reinterpret_cast<float*>(smem_raw) : gl;
+  const int tid = threadIdx.x;
+  const unsigned rank = T::rank();
+  // one block: idle threads (tid >= nt) start every site loop past its end but
+  // take part in the barriers; a team: every thread owns sites
+  const uint32_t nt = CL == 1 ? (uint32_t)P.nt : (uint32_t)(CL * blockDim.x);
+  const uint32_t t0 = CL == 1 ? (tid < P.nt ? (uint32_t)tid : 0x7fffffffu) : rank * blockDim.x + tid;
+  if (resident)
     for (size_t j = t0; j < N * n_sites; j += nt) lat[j] = gl[j];
-  __syncthreads();
+  if (CL > 1 && tid == 0) s_stop[0] = 0;
+  T::sync();
   uint32_t sweep = P.sweep0;
 
   for (int meas = 0; meas < P.n_meas; ++meas) {
-    if (P.ctl) {  // stop between measurements when the budget or a cancel says so
-      if (tid == 0) s_stop = P.poll->check(*P.ctl);
-      __syncthreads();
-      if (s_stop) break;
+    if constexpr (CL == 1) {
+      if (P.ctl) {  // stop between measurements when the budget or a cancel says so
+        if (tid == 0) s_stop[0] = P.poll->check(*P.ctl);
+        __syncthreads();
+        if (s_stop[0]) break;
+      }
+    } else {
+      if (s_stop[meas & 1]) break;  // block 0's answer, written before the last barrier
     }
     long long nacc = 0;
     for (int row = 0; row < P.n_rows; ++row) {
@@ -408,24 +428,24 @@ __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
       for (int rep = 0; rep < P.reps[row]; ++rep) {
         for (int c = 0; c < 2; ++c) {
           SiteCursor cur;
-          for (cur.init(g, t0, (uint32_t)nt); cur.s < g.slots; cur.next(g)) {
+          for (cur.init(g, t0, nt); cur.s < g.slots; cur.next(g)) {
             uint32_t nb[Z];
             on_neighbours_at<Z>(g, c, cur.r, cur.i, cur.y, cur.z, nb);
             nacc += on_site_nb<N, Z>(lat, g, c, cur.s, nb, code, sweep, P.beta, P.step, P.k0, P.k1);
           }
-          __syncthreads();
+          T::sync();
         }
         ++sweep;
       }
     }
     for (uint32_t j = t0; j < n_sites; j += nt) on_normalize_site<N>(lat, n_sites, j);
-    __syncthreads();
+    T::sync();
     long long v[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = 0;
     for (int c = 0; c < 2; ++c) {
       SiteCursor cur;
-      for (cur.init(g, t0, (uint32_t)nt); cur.s < g.slots; cur.next(g)) {
+      for (cur.init(g, t0, nt); cur.s < g.slots; cur.next(g)) {
         uint32_t nb[Z];
         on_neighbours_at<Z>(g, c, cur.r, cur.i, cur.y, cur.z, nb);
         on_measure_site_nb<N, Z>(lat, g, c, cur.s, nb, v);
@@ -439,16 +459,32 @@ __device__ void on_chain_run(const OnChain& P, unsigned char* smem_raw) {
       if (lane == 0) red[q][warp] = w;
     }
     __syncthreads();
-    if (tid < NV) {
-      long long total = 0;
+    long long total = 0;
+    if (tid < NV)
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += red[tid][w];
-      on_write_sum<N, Z>(P.e_out, P.m_out, P.sc_out, P.ss_out, P.aux_out, meas, tid, total);
+    if constexpr (CL == 1) {
+      if (tid < NV) on_write_sum<N, Z>(P.e_out, P.m_out, P.sc_out, P.ss_out, P.aux_out, meas, tid, total);
+    } else {
+      if (tid < NV) *T::at(&part[meas & 1][rank][tid], 0) = total;
+      if (rank == 0 && tid == 0) {
+        const int stop = P.ctl ? P.poll->check(*P.ctl) : 0;
+        for (int r = 0; r < CL; ++r) *T::at(&s_stop[(meas + 1) & 1], (unsigned)r) = stop;
+      }
     }
-    __syncthreads();
+    T::sync();
+    if constexpr (CL > 1) {
+      // block 0 adds the totals; part[meas & 1] is next written two measurements
+      // on, after barriers that block 0 only passes once it is done here
+      if (rank == 0 && tid < NV) {
+        long long sum = 0;
+        for (int r = 0; r < CL; ++r) sum += part[meas & 1][r][tid];
+        on_write_sum<N, Z>(P.e_out, P.m_out, P.sc_out, P.ss_out, P.aux_out, meas, tid, sum);
+      }
+    }
   }
-  if (P.resident)
+  if (resident)
     for (size_t j = t0; j < N * n_sites; j += nt) gl[j] = lat[j];
-  __syncthreads();
+  T::sync();
 }
 
 template <int N, int Z>
@@ -813,19 +849,26 @@ extern "C" int32_t critmc_on_run_grid(float* spins, int32_t dim, int32_t lx, int
 namespace critmc {
 
 // One kernel per (n, dimension): the variants' register needs differ, and a
-// kernel holding all of them would be held to the largest.
-template <int N, int Z>
+// kernel holding all of them would be held to the largest.  CL > 1: each item
+// is advanced by a cluster of CL blocks (block 0 takes the item from the queue
+// and hands its index to the others).
+template <int N, int Z, int CL>
 __global__ void __launch_bounds__(ON_THREADS) on_items_kernel(const critmc_item* items, int n,
                                                               unsigned* queue, size_t smem, RunCtl ctl) {
+  using T = Team<CL>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int cur;
   CtlPoll poll;
   poll.start();
+  const unsigned rank = T::rank();
   for (;;) {
-    if (threadIdx.x == 0) cur = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
-    __syncthreads();
+    if (rank == 0 && threadIdx.x == 0) {
+      const int v = poll.check(ctl) ? n : (int)atomicAdd(queue, 1u);
+      for (int r = 0; r < CL; ++r) *T::at(&cur, (unsigned)r) = v;
+    }
+    T::sync();
     const int i = cur;
-    __syncthreads();
+    T::sync();
     if (i >= n) break;
     const critmc_item& it = items[i];
     OnChain a;
@@ -857,14 +900,21 @@ __global__ void __launch_bounds__(ON_THREADS) on_items_kernel(const critmc_item*
     a.k1 = it.key[1];
     a.beta = it.beta;
     a.step = it.step;
-    on_chain_run<N, Z>(a, smem_raw);
+    on_chain_run<N, Z, CL>(a, smem_raw);
   }
 }
 
 template <int N, int Z>
-static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, size_t smem, const RunCtl& ctl,
-                              cudaStream_t s) {
-  auto kern = on_items_kernel<N, Z>;
+static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, size_t smem, int team,
+                              const RunCtl& ctl, cudaStream_t s) {
+  switch (team) {
+    case 2: return launch_team(on_items_kernel<N, Z, 2>, 2, ON_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    case 4: return launch_team(on_items_kernel<N, Z, 4>, 4, ON_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    case 8: return launch_team(on_items_kernel<N, Z, 8>, 8, ON_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    case 16: return launch_team(on_items_kernel<N, Z, 16>, 16, ON_THREADS, n, s, items, n, queue, (size_t)0, ctl);
+    default: break;
+  }
+  auto kern = on_items_kernel<N, Z, 1>;
   if (smem > 0 &&  // static + dynamic may pass 48 KiB
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cuda_fail("shared memory attribute");
@@ -879,15 +929,15 @@ static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, 
   return CRITMC_OK;
 }
 
-int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem,
+int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem, int team,
                     const RunCtl& ctl, cudaStream_t s) {
   switch (n_comp * 10 + dim) {
-    case 21: return on_items_launch_nz<2, 2>(items, n, queue, smem, ctl, s);
-    case 22: return on_items_launch_nz<2, 4>(items, n, queue, smem, ctl, s);
-    case 23: return on_items_launch_nz<2, 6>(items, n, queue, smem, ctl, s);
-    case 31: return on_items_launch_nz<3, 2>(items, n, queue, smem, ctl, s);
-    case 32: return on_items_launch_nz<3, 4>(items, n, queue, smem, ctl, s);
-    case 33: return on_items_launch_nz<3, 6>(items, n, queue, smem, ctl, s);
+    case 21: return on_items_launch_nz<2, 2>(items, n, queue, smem, team, ctl, s);
+    case 22: return on_items_launch_nz<2, 4>(items, n, queue, smem, team, ctl, s);
+    case 23: return on_items_launch_nz<2, 6>(items, n, queue, smem, team, ctl, s);
+    case 31: return on_items_launch_nz<3, 2>(items, n, queue, smem, team, ctl, s);
+    case 32: return on_items_launch_nz<3, 4>(items, n, queue, smem, team, ctl, s);
+    case 33: return on_items_launch_nz<3, 6>(items, n, queue, smem, team, ctl, s);
     default: return fail(CRITMC_ERR_INVALID, "O(n) items need n = 2 or 3 and dim 1..3");
   }
 }

@@ -57,13 +57,25 @@ class CritmcItem(ctypes.Structure):
         ("thr_tab", (ctypes.c_uint32 * 16) * 2),
         ("boltz", ctypes.c_uint64 * 8),
         ("weight", ctypes.c_uint64 * 8),
+        ("team", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
-class ItemRun:
-    """One slice of work for one chain: ``n_meas`` applications of ``schedule``."""
+TEAM_SIZES = (1, 2, 4, 8, 16)
 
-    def __init__(self, model, chain, running: dict, beta: float, schedule: np.ndarray, n_meas: int):
+
+class ItemRun:
+    """One slice of work for one chain: ``n_meas`` applications of ``schedule``.
+
+    ``team``: thread blocks advancing the chain together (1; or 2, 4, 8, 16 as a
+    thread-block cluster, for large lattices); the results do not depend on it.
+    """
+
+    def __init__(self, model, chain, running: dict, beta: float, schedule: np.ndarray, n_meas: int,
+                 team: int = 1):
+        if team not in TEAM_SIZES:
+            raise ValueError(f"team must be one of {TEAM_SIZES}, got {team}")
         self.model, self.chain, self.running = model, chain, running
         self.beta = float(beta)
         self.schedule = np.ascontiguousarray(schedule, dtype=np.int64).reshape(-1, 2)
@@ -77,6 +89,7 @@ class ItemRun:
         it.key[0], it.key[1] = int(chain.key.ravel()[0]), int(chain.key.ravel()[1])
         it.sweep0 = chain.sweep
         it.n_meas = self.n_meas
+        it.team = int(team)
         it.n_rows = len(self.schedule)
         if it.n_rows > 4:
             raise ValueError("work items take at most 4 schedule rows")

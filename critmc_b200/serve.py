@@ -67,6 +67,13 @@ COSTS = {
     ("grid", "on2"): (1.0e-5, 2.0e-10),
     ("grid", "on3"): (1.2e-5, 3.0e-10),
 }
+TEAMS = (2, 4, 8, 16)
+# teams (thread-block clusters per item): about 1/T of one block's per-site
+# time plus the cluster barriers
+for _fam in ("msc", "byte", "potts", "on2", "on3"):
+    _a, _b = COSTS[("items", _fam)]
+    for _t in TEAMS:
+        COSTS[(f"team{_t}", _fam)] = (2.0 * _a, 1.2 * _b / _t)
 
 
 @dataclass
@@ -203,6 +210,7 @@ class _Job:
     launched: int = 0
     harvested: int = 0
     group: str = ""
+    team: int = 1  # thread blocks per item on an item lane
     home: object = None  # the lane that advances it
     stream: dict = field(default_factory=dict)  # summary mode: streaming statistics per scalar field
 
@@ -282,7 +290,7 @@ class Server:
 
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
                  tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
-                 grid_after_s: float | None = None,
+                 grid_after_s: float | None = None, team_after_s: float | None = None,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
                  keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None,
                  stats_lag: int = 64):
@@ -300,6 +308,12 @@ class Server:
         # the multi-block lanes are launch-bound: they buy latency, the item
         # kernels throughput, so at most this many requests use them at once
         self.max_grid_lanes = max_grid_lanes
+        # None: one block per item.  A number: a request that one block would
+        # keep longer than that (cost model) gets a team, the smallest thread-
+        # block cluster predicted to finish it within that time (else the
+        # fastest); teams replace the multi-block lanes for the families they serve
+        self.team_after_s = team_after_s
+        self.team_sizes_used: set[int] = set()
         self.keep_series, self.keep_state = keep_series, keep_state
         self.stats_lag = int(stats_lag)
         self.on_result = on_result
@@ -370,6 +384,25 @@ class Server:
         per_meas = int(req.schedule()[:, 1].sum())
         return req.sweeps * per_meas * (a + b * req.n_sites) > self.grid_after_s
 
+    def _team_for(self, req: Request, family: str) -> int:
+        """Blocks per item for a request on an item lane (1 = one block): the
+        smallest team predicted to finish within team_after_s, else the fastest."""
+        if self.team_after_s is None:
+            return 1
+        per = req.sweeps * int(req.schedule()[:, 1].sum())
+        a, b = self.costs[("items", family)]
+        best, best_t = per * (a + b * req.n_sites), 1
+        if best <= self.team_after_s:
+            return 1
+        for t in TEAMS:
+            a, b = self.costs[(f"team{t}", family)]
+            pred = per * (a + b * req.n_sites)
+            if pred <= self.team_after_s:
+                return t
+            if pred < best:
+                best, best_t = pred, t
+        return best_t
+
     def _grid_free(self) -> bool:
         return sum(1 for lane in self.grid_lanes if lane.jobs) < self.max_grid_lanes
 
@@ -435,19 +468,26 @@ class Server:
             group = family
             fields = [("Eb", _I8, 1), ("M", _I8, 1), ("aux", _I8, 4)]
             t["running"] = torch.tensor([[running["e_b"], running["m"]]], dtype=torch.int64, device=dev)
-            lane = "grid" if msc and self._wants_grid(req, "msc") and self._grid_free() else "items"
+            team = self._team_for(req, family)
+            if self.team_after_s is not None:
+                lane = "items" if (team > 1 or not msc or req.n_sites <= 1 << 20) else "grid"
+            else:
+                lane = "grid" if msc and self._wants_grid(req, "msc") and self._grid_free() else "items"
             kind = ITEM_MSC_ISING if msc else ITEM_BYTE_ISING
             h = model.h
             if lane == "grid":
                 tables = np.ascontiguousarray(model.tables(req.beta)[0])
         elif isinstance(model, Potts):
             family, group, lane, kind, h = "potts", "byte", "items", ITEM_POTTS, 0.0
+            team = self._team_for(req, family)
             fields = [("E", _I8, 1), ("counts", _I8, model.q), ("aux", _I8, 4)]
             t["running"] = torch.tensor([running["energy"]], dtype=torch.int64, device=dev)
             t["counts"] = torch.from_numpy(np.asarray(running["counts"], dtype=np.int64)).to(dev)
         else:
             # same results on either lane
-            chain.lane = "grid" if self._wants_grid(req, f"on{model.n}") and self._grid_free() else "block"
+            team = self._team_for(req, f"on{model.n}")
+            grid = self.team_after_s is None and self._wants_grid(req, f"on{model.n}") and self._grid_free()
+            chain.lane = "grid" if grid else "block"
             family, lane, kind, h = f"on{model.n}", chain.lane.replace("block", "items"), ITEM_ON, 0.0
             group = f"on{model.n}d{dim}"
             fields = [("E", _F8, 1), ("M", _F8, model.n), ("stiff_c", _F8, dim), ("stiff_s", _F8, dim),
@@ -461,6 +501,7 @@ class Server:
             item.dim = dim
             item.lx, item.ly, item.lz = chain.dims
             item.q_or_n = model.q if family == "potts" else (model.n if kind == ITEM_ON else 0)
+            item.team = team
             item.key[0], item.key[1] = int(chain.key.ravel()[0]), int(chain.key.ravel()[1])
             if len(sched) > 4:
                 raise ValueError("served schedules have at most 4 rows")
@@ -473,9 +514,11 @@ class Server:
                       float(running.get("step", 1.0)))
         job = _Job(req, model, chain, running, lane, family, sched, int(sched[:, 1].sum()), fields, item, t,
                    need, self.now(), tables=tables)
-        # item lanes by kernel group and lattice size class (a call's blocks get the largest
-        # lattice's shared memory, so small lattices do not share a lane with large ones)
-        job.group = f"{group}-{(need - 4096).bit_length()}"
+        # item lanes by kernel group, team size and lattice size class (a call's blocks get
+        # the largest lattice's shared memory, so small lattices do not share a lane with large ones)
+        job.team = team if lane == "items" else 1
+        self.team_sizes_used.add(job.team)
+        job.group = f"{group}-t{job.team}-{(need - 4096).bit_length()}"
         if self.keep_series:
             job.series = {name: np.empty((req.sweeps, w) if w > 1 else req.sweeps, dtype=dt)
                           for name, dt, w in fields}
@@ -488,7 +531,7 @@ class Server:
 
     # ---- ticks -----------------------------------------------------------
     def _sweep_seconds(self, job: _Job) -> float:
-        a, b = self.costs[(job.lane, job.family)]
+        a, b = self.costs[(job.lane, job.family) if job.team == 1 else (f"team{job.team}", job.family)]
         return job.sweeps_per_meas * (a + b * job.req.n_sites)
 
     def _plan(self, lane: _Lane):

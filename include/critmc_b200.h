@@ -367,6 +367,11 @@ typedef struct {
   float beta, step;  /* O(n) */
   uint32_t kind_tab[2][16], thr_tab[2][16]; /* Ising acceptance classes (metropolis, heat bath) */
   uint64_t boltz[8], weight[8];             /* Potts tables */
+  int32_t team;      /* thread blocks per item: 0 or 1 = one block (lattice in shared
+                        memory when it fits); 2, 4, 8 or 16 = a thread-block cluster of
+                        that many blocks on one GPC, the lattice in global memory (large
+                        lattices: about team times less time per sweep) */
+  int32_t reserved;  /* 0 */
 } critmc_item;
 
 /* Fill the acceptance tables of an item for inverse temperature beta (and
@@ -376,9 +381,10 @@ int32_t critmc_item_prepare(critmc_item* item, double beta, double h, double ste
 /* Device bytes needed to run n_items items (descriptors + queue counters).  */
 int64_t critmc_items_buffer_bytes(int32_t n_items);
 
-/* Copy the HOST items to the DEVICE buffer (grouped by family) and run them;
- * the three family kernels run side by side on library-owned streams forked
- * from and joined into `stream` (CUDA-graph capturable).
+/* Copy the HOST items to the DEVICE buffer (grouped by family and team size)
+ * and run them; the kernels of the groups run side by side on library-owned
+ * streams forked from and joined into `stream` (CUDA-graph capturable).  A
+ * team size the GPU cannot schedule fails with CRITMC_ERR_UNSUPPORTED.
  * staging: NULL, or PINNED host memory of n_items * sizeof(critmc_item)
  *   bytes that the call fills and copies from asynchronously (do not reuse it
  *   before `stream` has passed this call).  With NULL the copy comes from

@@ -124,3 +124,21 @@ def test_item_struct_matches_the_header():
     it.kind = 9
     assert _lib.lib().critmc_item_prepare(ctypes.byref(it), 1.0, 0.0, 1.0) != 0
     assert _lib.lib().critmc_run_items(None, 0, None, 0, None, 0, None) == 0
+
+
+def test_item_team_sizes_are_checked_before_any_device_work():
+    """A team of 2, 4, 8 or 16 blocks is a thread-block cluster; other sizes are refused."""
+    from critmc_b200.items import TEAM_SIZES, CritmcItem, ItemRun
+
+    assert TEAM_SIZES == (1, 2, 4, 8, 16)
+    lib = _lib.lib()
+    it = CritmcItem()
+    it.kind, it.dim, it.lx, it.ly, it.n_rows = 0, 2, 64, 64, 1
+    it.codes[0], it.reps[0] = 0, 1
+    it.team = 3
+    buf = ctypes.create_string_buffer(int(lib.critmc_items_buffer_bytes(1)))
+    st = lib.critmc_run_items(ctypes.byref(it), 1, ctypes.cast(buf, ctypes.c_void_p), len(buf), None, 0, None)
+    assert st == -1  # CRITMC_ERR_INVALID
+    assert "team" in _lib.last_error()
+    with pytest.raises(ValueError, match="team"):
+        ItemRun(None, None, {}, 0.4, np.array([[0, 1]]), 1, team=5)

@@ -42,8 +42,10 @@ def _check(res, cuda):
     np.testing.assert_array_equal(res.state, state)
 
 
-def test_served_results_equal_alone(cuda):
-    srv = Server(cuda, tick_ms=0.5, keep_state=True)
+@pytest.mark.parametrize("team_after_s", [None, 2e-3])
+def test_served_results_equal_alone(cuda, team_after_s):
+    """team_after_s 2 ms: the longer requests run as thread-block-cluster teams."""
+    srv = Server(cuda, tick_ms=0.5, keep_state=True, team_after_s=team_after_s)
     reqs = []
     for i, r in enumerate(REQUESTS):
         reqs.append(Request(**{**r.__dict__, "arrival": 0.004 * i, "rid": i}))
@@ -51,6 +53,8 @@ def test_served_results_equal_alone(cuda):
     assert len(results) == len(REQUESTS)
     st = srv.stats()
     assert st["ticks"] > 3  # the requests were sliced and overlapped
+    if team_after_s is not None:
+        assert len(srv.team_sizes_used) > 1, srv.team_sizes_used
     for res in results:
         assert res.finished >= res.admitted >= res.arrival
         _check(res, cuda)

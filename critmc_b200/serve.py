@@ -68,12 +68,14 @@ COSTS = {
     ("grid", "on3"): (1.2e-5, 3.0e-10),
 }
 TEAMS = (2, 4, 8, 16)
-# teams (thread-block clusters per item): about 1/T of one block's per-site
-# time plus the cluster barriers
+# teams (thread-block clusters per item), measured on B200 for T = 2..16: about
+# 1/T of one block's per-site time, and 2-3 times its fixed time per sweep
+# (cluster barriers, the lattice in global memory)
 for _fam in ("msc", "byte", "potts", "on2", "on3"):
     _a, _b = COSTS[("items", _fam)]
     for _t in TEAMS:
-        COSTS[(f"team{_t}", _fam)] = (2.0 * _a, 1.2 * _b / _t)
+        COSTS[(f"team{_t}", _fam)] = (2.5 * _a, 1.1 * _b / _t)
+TEAM_SLACK = 1.15  # a smaller team within this factor of the fastest saves SMs
 
 
 @dataclass
@@ -290,7 +292,7 @@ class Server:
 
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
                  tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
-                 grid_after_s: float | None = None, team_after_s: float | None = None,
+                 grid_after_s: float | None = None, team_after_s: float | None = None, max_team: int = 16,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
                  keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None,
                  stats_lag: int = 64):
@@ -313,6 +315,7 @@ class Server:
         # block cluster predicted to finish it within that time (else the
         # fastest); teams replace the multi-block lanes for the families they serve
         self.team_after_s = team_after_s
+        self.teams = tuple(t for t in TEAMS if t <= max_team)
         self.team_sizes_used: set[int] = set()
         self.keep_series, self.keep_state = keep_series, keep_state
         self.stats_lag = int(stats_lag)
@@ -386,22 +389,23 @@ class Server:
 
     def _team_for(self, req: Request, family: str) -> int:
         """Blocks per item for a request on an item lane (1 = one block): the
-        smallest team predicted to finish within team_after_s, else the fastest."""
+        smallest team predicted to finish within team_after_s; else the smallest
+        team within TEAM_SLACK of the fastest (larger teams buy little there and
+        hold more SMs)."""
         if self.team_after_s is None:
             return 1
         per = req.sweeps * int(req.schedule()[:, 1].sum())
         a, b = self.costs[("items", family)]
-        best, best_t = per * (a + b * req.n_sites), 1
-        if best <= self.team_after_s:
+        pred = {1: per * (a + b * req.n_sites)}
+        if pred[1] <= self.team_after_s:
             return 1
-        for t in TEAMS:
+        for t in self.teams:
             a, b = self.costs[(f"team{t}", family)]
-            pred = per * (a + b * req.n_sites)
-            if pred <= self.team_after_s:
+            pred[t] = per * (a + b * req.n_sites)
+            if pred[t] <= self.team_after_s:
                 return t
-            if pred < best:
-                best, best_t = pred, t
-        return best_t
+        fastest = min(pred.values())
+        return min(t for t, p in pred.items() if p <= TEAM_SLACK * fastest)
 
     def _grid_free(self) -> bool:
         return sum(1 for lane in self.grid_lanes if lane.jobs) < self.max_grid_lanes

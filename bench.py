@@ -485,7 +485,7 @@ def run_reference(args) -> None:
 
 def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0, world: int = 1,
                 max_grid_lanes: int = 8, grid_after_s: float | None = 1.0,
-                team_after_s: float | None = None) -> dict | None:
+                team_after_s: float | None = 1.0, max_team: int = 8) -> dict | None:
     """Continuous-batching server on a seeded Poisson stream of mixed requests.
 
     Workload: ``n_requests`` requests at ``rate``/s, each uniform over 2D Ising
@@ -508,7 +508,7 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0,
 
     # series reduced to sums (stats_lag=0: no host-side error-bar sums inside the timed run)
     srv = Server(dev, keep_series=False, on_result=lambda r: None, costs="auto", max_grid_lanes=max_grid_lanes,
-                 stats_lag=0, grid_after_s=grid_after_s, team_after_s=team_after_s)
+                 stats_lag=0, grid_after_s=grid_after_s, team_after_s=team_after_s, max_team=max_team)
     # warm-up: one short request per (model, size) of the mix builds the
     # lattice cache, the library streams and the kernels' first launches
     shapes = sorted({(r.model, r.L) for r in reqs})
@@ -535,7 +535,8 @@ def serve_bench(dev, n_requests: int, rate: float, seed: int = 0, rank: int = 0,
             "mean_latency_s": float(lat_a.mean()), "max_latency_s": float(lat_a.max()),
             "updates_per_ns": upd[0] / wall / 1e9, "gpu_busy_frac": st["gpu_seconds"] / wall,
             "ticks": st["ticks"], "peak_hbm_bytes": st["peak_hbm_bytes"], "max_queued": st["max_queued"],
-            "team_after_s": team_after_s, "grid_after_s": grid_after_s if team_after_s is None else None,
+            "team_after_s": team_after_s, "max_team": max_team if team_after_s is not None else None,
+            "grid_after_s": grid_after_s if team_after_s is None else None,
             "workload": "Poisson arrivals; Ising L 16..1024 / Potts q=10 L 16..128 / XY L 32..128, "
                         "sweeps log-uniform 1e3..1e5, checkerboard Metropolis (critmc's default update)"}
 
@@ -556,7 +557,9 @@ def main() -> None:
     ap.add_argument("--serve-grid-after", type=float, default=1.0,
                     help="item-lane seconds (cost model) above which a request takes a multi-block lane "
                          "(negative: every large lattice, first come first served)")
-    ap.add_argument("--serve-team-after", type=float, default=-1.0,
+    ap.add_argument("--serve-max-team", type=int, default=8, choices=[2, 4, 8, 16],
+                    help="largest thread-block cluster per request")
+    ap.add_argument("--serve-team-after", type=float, default=1.0,
                     help="one-block seconds (cost model) above which a request runs as a thread-block-cluster "
                          "team (negative: no teams, multi-block lanes as --serve-grid-after says)")
     ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch", "cluster-sw"],
@@ -615,7 +618,8 @@ def main() -> None:
     if args.serve_only:
         print(json.dumps({"serving": serve_bench(dev, args.serve_requests, args.serve_rate,
                                                  max_grid_lanes=args.serve_grid_lanes,
-                                                 grid_after_s=grid_after, team_after_s=team_after)}), flush=True)
+                                                 grid_after_s=grid_after, team_after_s=team_after,
+                                                 max_team=args.serve_max_team)}), flush=True)
         return
 
     # launch shape (rows per thread, inline planes) from the autotuner; results do not depend on it
@@ -691,7 +695,7 @@ def main() -> None:
     if args.serve_requests > 0:  # every rank serves its shard; rank 0 gets the job's numbers
         serving = serve_bench(dev, args.serve_requests, args.serve_rate, rank=rank, world=world,
                               max_grid_lanes=args.serve_grid_lanes, grid_after_s=grid_after,
-                              team_after_s=team_after)
+                              team_after_s=team_after, max_team=args.serve_max_team)
     if rank == 0 and world == 1 and not args.no_extras:
         extras["ea_campaign"] = ea_bench(dev, peak=peaks()[0])
         extras["on_batched"] = on_bench(dev, peak=peaks()[0])

@@ -63,9 +63,11 @@ def profile_traffic() -> dict | None:
 
 
 class Clocks:
-    """Samples the SM clock, its maximum and the clock-event reasons of one GPU
-    every 5 ms from a host thread (NVML queries only; no setting is changed), so
-    that a timed region of a few tens of milliseconds still gets several samples.
+    """Samples the SM clock and the clock-event reasons of one GPU every 1 ms
+    from a host thread (NVML queries only; no setting is changed), so that a
+    timed region of a few tens of milliseconds still gets several samples.  NVML
+    set-up, the maximum clock and a first (discarded) sample come before the
+    region starts.
 
     NVML is read in-process rather than through a piped ``nvidia-smi -lms``:
     that child buffers its output and, stopped by a signal, can lose every
@@ -78,7 +80,7 @@ class Clocks:
                ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
                ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, device, period_s: float = 0.005):
+    def __init__(self, device, period_s: float = 0.001):
         self.device = device
         self.period = period_s
         self.samples: list[tuple[float, float, int]] = []
@@ -107,6 +109,12 @@ class Clocks:
             self.error = f"NVML unavailable: {exc}"
             return self
         self._stop = threading.Event()
+        ready = threading.Event()
+        try:
+            mx = float(nvml.nvmlDeviceGetMaxClockInfo(h, nvml.NVML_CLOCK_SM))
+        except Exception as exc:
+            self.error = f"NVML max clock: {exc}"
+            return self
 
         def loop():
             get_reasons = getattr(nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
@@ -114,14 +122,16 @@ class Clocks:
             while not self._stop.is_set():
                 try:
                     sm = nvml.nvmlDeviceGetClockInfo(h, nvml.NVML_CLOCK_SM)
-                    mx = nvml.nvmlDeviceGetMaxClockInfo(h, nvml.NVML_CLOCK_SM)
-                    self.samples.append((float(sm), float(mx), int(get_reasons(h))))
+                    self.samples.append((float(sm), mx, int(get_reasons(h))))
                 except Exception as exc:
                     self.error = str(exc)
+                ready.set()
                 self._stop.wait(self.period)
 
         self._thread = threading.Thread(target=loop, daemon=True)
         self._thread.start()
+        ready.wait(2.0)
+        self.samples = []  # the warm-up sample precedes the timed region
         return self
 
     def __exit__(self, *exc):

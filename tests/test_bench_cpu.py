@@ -35,3 +35,41 @@ def test_reference_arm_prints_the_contract_line():
 
 def test_reference_arm_prints_only_on_rank_0():
     assert _run({"RANK": "1", "WORLD_SIZE": "2"}).strip() == ""
+
+
+def test_clock_sampler_records_only_inside_the_region(monkeypatch):
+    """The sampler reads NVML (faked here) from a thread: set-up and a warm-up
+    sample come before the region, samples are taken every millisecond inside
+    it, and throttle reasons are decoded from the event-reason mask."""
+    import time
+    import types
+
+    import bench
+
+    calls = {"max": 0, "clock": 0}
+
+    def max_clock(h, kind):
+        calls["max"] += 1
+        return 1965
+
+    def clock(h, kind):
+        calls["clock"] += 1
+        return 1900 + calls["clock"] % 3
+
+    fake = types.SimpleNamespace(
+        nvmlInit=lambda: None, nvmlDeviceGetHandleByIndex=lambda i: "h", nvmlDeviceGetHandleByPciBusId=None,
+        NVML_CLOCK_SM=0, nvmlDeviceGetMaxClockInfo=max_clock, nvmlDeviceGetClockInfo=clock,
+        nvmlDeviceGetCurrentClocksEventReasons=lambda h: 0x4 | 0x8,
+        nvmlClocksEventReasonHwSlowdown=0x8, nvmlClocksEventReasonHwThermalSlowdown=0x40,
+        nvmlClocksEventReasonSwThermalSlowdown=0x20, nvmlClocksEventReasonSwPowerCap=0x4,
+        nvmlClocksEventReasonHwPowerBrakeSlowdown=0x80)
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    clk = bench.Clocks(types.SimpleNamespace(index=0))
+    monkeypatch.setattr(clk, "_handle", lambda nvml: "h")
+    with clk:
+        before = calls["clock"]
+        time.sleep(0.03)
+    s = clk.summary()
+    assert before >= 1 and calls["max"] == 1
+    assert s["samples"] >= 5 and s["sm_max_mhz"] == 1965 and 1900 <= s["sm_mhz"] <= 1902
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]

@@ -328,7 +328,9 @@ def small_case(dev, case: str) -> dict:
     moves) or of 18944 walkers (128 per SM, 200,000 moves each) on the q = 10 Potts
     8 x 8 torus, energy window [-1.95, -0.6] per site.  cluster-sw: Swendsen-Wang
     updates of one 2D Ising chain of 1024 x 1024 (bit layout) at beta_c, two
-    warm-up updates and one timed.
+    warm-up updates and one timed.  team-xy128: one XY 128 x 128 chain as a work
+    item of an 8-block thread-block cluster, 400 Metropolis sweeps with a
+    measurement after each (the served form of a large XY request).
     """
     import torch
 
@@ -372,6 +374,25 @@ def small_case(dev, case: str) -> dict:
         W.run(0, lng, moves, ln_f=lnf, n_levels=lnf, one_over_t=off, t_base=W.trials.clone())
         e1.record()
         units = nw * moves
+    elif case == "team-xy128":
+        from critmc_b200 import ON, square
+        from critmc_b200.items import ItemRun, run_items
+
+        model = ON(square(128), 2)
+        s0 = model.initial_state("random", np.random.default_rng(1))
+        ch = model.to_device(s0, np.random.default_rng(2), dev)
+        run = model.begin(s0)
+        sched = np.array([[0, 1]])
+        warm = ItemRun(model, ch, run, 1.1, sched, 20, team=8)
+        run_items([warm], dev)
+        warm.finish()
+        it = ItemRun(model, ch, run, 1.1, sched, 400, team=8)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        run_items([it], dev)
+        e1.record()
+        it.finish()
+        units = model.lattice.n_sites * 400
     elif case == "ea-small":
         from critmc_b200 import cubic
         from critmc_b200.glass import EdwardsAnderson, MultiSizeCampaign, SpinGlassCampaign, geometric_temperatures
@@ -572,7 +593,7 @@ def main() -> None:
     ap.add_argument("--serve-team-after", type=float, default=1.0,
                     help="one-block seconds (cost model) above which a request runs as a thread-block-cluster "
                          "team (negative: no teams, multi-block lanes as --serve-grid-after says)")
-    ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch", "cluster-sw"],
+    ap.add_argument("--case", choices=["ea-small", "on-small", "fh-single", "fh-batch", "cluster-sw", "team-xy128"],
                     help="run one small case of a secondary kernel (for profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -161,13 +161,30 @@ __device__ __forceinline__ void ea_planes(const EaCommon& C, const Count3& cnt, 
   }
 }
 
+// Threads per block for a sample of this geometry (64, 128 or 256): every
+// thread may hold at most 63 / z sites of one colour, the capacity of the
+// 6-plane vertical counters of the energy and link-overlap sums.  Fewer
+// threads per small sample let more samples share an SM (registers bound the
+// blocks per SM), which pays on small lattices, where a step is dominated by
+// its serial phases (swap walk, measurement) rather than by the sweep.
+inline int ea_threads_for(const ByteGeom& g, int z) {
+  // measured per size alone (3D, 512 samples): 64 threads gave +29 % at L = 6 and
+  // +10 % at L = 8 but -9 % at L = 10, where the sweep outweighs the serial phases
+  if (g.slots <= 256u && (g.slots + 63u) / 64u * (uint32_t)z <= 63u) return 64;
+  if ((g.slots + 127u) / 128u * (uint32_t)z <= 63u) return 128;
+  return EA_THREADS;
+}
+
 // Dynamic shared memory of one sample's block.
 inline size_t ea_smem_bytes(const ByteGeom& g, int dim, int lx) {
   return (size_t)(2 * g.slots) * (2 * 4 + 4 + 1) + (size_t)dim * lx * 32 * 4;
 }
 
-// All PT steps of one sample by one thread block.  key[set] = Philox key of replica set.
-template <int Z>
+// All PT steps of one sample by one thread block of T threads (64, 128 or 256;
+// the vertical counters of a thread hold at most 63, so T must give every
+// thread at most 63 / z sites of a colour: ea_threads_for).  key[set] =
+// Philox key of replica set.
+template <int Z, int T = EA_THREADS>
 __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, const uint32_t (&key)[2][2],
                               unsigned char* smem_raw, const RunCtl& ctl, CtlPoll& poll) {
   constexpr int DIM = Z / 2;
@@ -177,7 +194,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   uint32_t* qw = lat + 2 * n_sites;                      // overlap words [2][slots]
   int* splane = reinterpret_cast<int*>(qw + n_sites);    // [DIM][L][32] overlap per plane and lane
   uint8_t* jn = reinterpret_cast<uint8_t*>(splane + DIM * S.ext[0] * 32);  // [2][slots]
-  __shared__ EaFix fix[EA_WARPS][EA_FIXCAP];
+  __shared__ EaFix fix[(T / 32)][EA_FIXCAP];
   __shared__ int ecnt[2][32];  // unsatisfied bonds per set and temperature
   __shared__ int qlcnt[32];    // agreeing bonds of the overlap field
   __shared__ int sigma[2][32];
@@ -187,12 +204,13 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   __shared__ double acc_s[32][EA_NOBS];
   __shared__ unsigned long long sw_acc[32], sw_try[32], lhist[32][2], trip[2];
   __shared__ int s_stop;
+  __shared__ uint32_t s_acc_mask[2];  // swaps accepted in the step's walk, by set
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m = C.m;
   uint32_t* gw = S.words + (size_t)sample * 2 * n_sites;
-  for (uint32_t j = tid; j < 2 * n_sites; j += EA_THREADS) lat[j] = gw[j];
-  for (uint32_t j = tid; j < n_sites; j += EA_THREADS) jn[j] = S.jneg[(size_t)sample * n_sites + j];
+  for (uint32_t j = tid; j < 2 * n_sites; j += T) lat[j] = gw[j];
+  for (uint32_t j = tid; j < n_sites; j += T) jn[j] = S.jneg[(size_t)sample * n_sites + j];
   if (tid < 64) {
     const int r = tid >> 5, k = tid & 31;
     if (k < m) {
@@ -234,9 +252,9 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
       for (int c = 0; c < 2; ++c) {
         int nf = 0;
         const uint32_t work = 2 * g.slots;  // both sets, one colour
-        const uint32_t rounds = (work + EA_THREADS - 1) / EA_THREADS;
+        const uint32_t rounds = (work + T - 1) / T;
         for (uint32_t it = 0; it < rounds; ++it) {
-          const uint32_t j = it * EA_THREADS + tid;
+          const uint32_t j = it * T + tid;
           uint32_t U = 0, D = 0, idx = 0;
           if (j < work) {
             const int set = j >= g.slots;
@@ -297,9 +315,9 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     if (tid < 64) ecnt[tid >> 5][tid & 31] = 0;
     __syncthreads();
     {
-      // colour-0 sites see every bond once; at most 8 sites per thread x z <= 6 bonds < 64
+      // colour-0 sites see every bond once; at most 63 / z sites per thread (ea_threads_for)
       uint32_t va[6] = {0, 0, 0, 0, 0, 0}, vb[6] = {0, 0, 0, 0, 0, 0};
-      for (uint32_t s = tid; s < g.slots; s += EA_THREADS) {
+      for (uint32_t s = tid; s < g.slots; s += T) {
         uint32_t w_s;
         Count3 cnt;
         ea_site<Z>(g, lat, jn, 0, 0, s, w_s, cnt);
@@ -323,32 +341,45 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
       if (lane < m - 1)
         swu[r][lane] = critmc_philox4x32((uint32_t)lane, step, CRITMC_TAG_SWAP | ((uint32_t)r << 16), 0u,
                                          key[r][0], key[r][1]).v[0];
+      if (lane < m - 1) atomicAdd(&sw_try[lane], 1ULL);  // every pair is tried once per set and step
       __syncwarp();
       if (lane == 0) {
+        // The walk swaps positions k and k+1 in order k = 0 .. m-2, so position k
+        // is final after step k and position k+1 is still untouched: carry the
+        // entry moving up (energy, configuration, permutation) in registers and
+        // write each position once.  Accepted pairs go to a bit mask that the
+        // lanes count afterwards, off the serial chain.
+        int cur_e = es[r][0], cur_c = conf[r][0], cur_s = sigma[r][0];
+        uint32_t accm = 0;
         for (int k = 0; k < m - 1; ++k) {
+          const int ne = es[r][k + 1], nc = conf[r][k + 1], ns = sigma[r][k + 1];
           // betas ascend hot -> cold, so x = (b_k - b_k+1)(E_k - E_k+1) >= 0 iff E_k <= E_k+1
-          const int de = es[r][k] - es[r][k + 1];
+          const int de = cur_e - ne;
           bool ok = de <= 0;
           if (!ok) {
             int j = de / 4;
             if (j > C.swap_width - 1) j = C.swap_width - 1;
             ok = swu[r][k] < C.swap_thr[(size_t)k * C.swap_width + j];
           }
-          atomicAdd(&sw_try[k], 1ULL);
-          if (ok) {
-            atomicAdd(&sw_acc[k], 1ULL);
-            const int te = es[r][k];
-            es[r][k] = es[r][k + 1];
-            es[r][k + 1] = te;
-            const int tc = conf[r][k];
-            conf[r][k] = conf[r][k + 1];
-            conf[r][k + 1] = tc;
-            const int ts = sigma[r][k];
-            sigma[r][k] = sigma[r][k + 1];
-            sigma[r][k + 1] = ts;
+          if (ok) {  // the carried entry moves on to k+1
+            accm |= 1u << k;
+            es[r][k] = ne;
+            conf[r][k] = nc;
+            sigma[r][k] = ns;
+          } else {
+            es[r][k] = cur_e;
+            conf[r][k] = cur_c;
+            sigma[r][k] = cur_s;
+            cur_e = ne;
+            cur_c = nc;
+            cur_s = ns;
           }
         }
-        const int hot = conf[r][0], cold = conf[r][m - 1];
+        es[r][m - 1] = cur_e;
+        conf[r][m - 1] = cur_c;
+        sigma[r][m - 1] = cur_s;
+        s_acc_mask[r] = accm;
+        const int hot = conf[r][0], cold = cur_c;
         // labels are indexed by configuration: lab[r][c] for configuration c
         if (lab[r][hot] == 2) atomicAdd(&trip[r], 1ULL);
         lab[r][hot] = 1;
@@ -356,6 +387,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
         lab[r][cold] = 2;
       }
       __syncwarp();
+      if (lane < m - 1 && ((s_acc_mask[r] >> lane) & 1u)) atomicAdd(&sw_acc[lane], 1ULL);
       if (lane < m) {
         ecnt[r][lane] = (es[r][lane] + n_bonds) / 2;  // permuted counts
         const int l = lab[r][conf[r][lane]];
@@ -368,7 +400,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     // (32 words per warp: transpose, take row sigma[k] into row k, transpose back)
     for (int r = 0; r < 2; ++r) {
       const int src = lane < m ? sigma[r][lane] : lane;
-      for (uint32_t base = (uint32_t)warp * 32; base < n_sites; base += EA_WARPS * 32) {
+      for (uint32_t base = (uint32_t)warp * 32; base < n_sites; base += T) {
         const uint32_t i = base + (uint32_t)lane;
         uint32_t x = i < n_sites ? lat[(size_t)r * n_sites + i] : 0u;
         x = transpose32(x, lane);
@@ -379,12 +411,12 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     }
     __syncthreads();
     // ---- measurement (critmc glass.py:57-77, :153-163) -----------------------
-    for (uint32_t j = tid; j < n_sites; j += EA_THREADS) qw[j] = ~(lat[j] ^ lat[n_sites + j]);
+    for (uint32_t j = tid; j < n_sites; j += T) qw[j] = ~(lat[j] ^ lat[n_sites + j]);
     if (tid < 32) qlcnt[tid] = 0;
     __syncthreads();
     {
-      uint32_t vq[6] = {0, 0, 0, 0, 0, 0};  // agreeing bonds, at most 8 sites x z <= 6 per thread
-      for (uint32_t s = tid; s < g.slots; s += EA_THREADS) {
+      uint32_t vq[6] = {0, 0, 0, 0, 0, 0};  // agreeing bonds, at most 63 per lane (ea_threads_for)
+      for (uint32_t s = tid; s < g.slots; s += T) {
         int r, i;
         byte_row_index(g, s, r, i);
         uint32_t nb[Z];
@@ -399,7 +431,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     }
     // per-plane overlap counts: warp w handles planes (d, x) = w, w + WARPS, ...;
     // its lanes split the plane's sites (at most 256 / 32 = 8 each)
-    for (int pl = warp; pl < DIM * S.ext[0]; pl += EA_WARPS) {
+    for (int pl = warp; pl < DIM * S.ext[0]; pl += (T / 32)) {
       const int d = pl / S.ext[0], x0 = pl % S.ext[0];
       const int e1 = S.ext[d == 0 ? 1 : 0], e2 = DIM == 3 ? S.ext[d == 2 ? 1 : 2] : 1;
       uint32_t vp[4] = {0, 0, 0, 0};
@@ -450,7 +482,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   if (tid < m)
     for (int o = 0; o < EA_NOBS; ++o)
       S.acc[(((size_t)sample * C.n_bins + bin) * m + tid) * EA_NOBS + o] = acc_s[tid][o];
-  for (uint32_t j = tid; j < 2 * n_sites; j += EA_THREADS) gw[j] = lat[j];
+  for (uint32_t j = tid; j < 2 * n_sites; j += T) gw[j] = lat[j];
   if (tid < 64) {
     const int r = tid >> 5, k = tid & 31;
     if (k < m) {
@@ -493,8 +525,11 @@ struct EaCampaignParams {
   RunCtl ctl;  // bounded run (null words: unbounded)
 };
 
-template <int Z>
-__global__ void __launch_bounds__(EA_THREADS, 3) ea_campaign_kernel(const __grid_constant__ EaCampaignParams P) {
+// T threads per block (ea_threads_for: the largest need of the campaign's sizes);
+// 80 registers a thread allow 3 blocks of 256, 6 of 128 or 12 of 64 per SM.
+template <int Z, int T>
+__global__ void __launch_bounds__(T, T == 256 ? 3 : (T == 128 ? 6 : 12))
+    ea_campaign_kernel(const __grid_constant__ EaCampaignParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int cur;
   CtlPoll poll;
@@ -509,7 +544,7 @@ __global__ void __launch_bounds__(EA_THREADS, 3) ea_campaign_kernel(const __grid
     const int sample = (int)(P.work[w] & 0xFFFFFFu);
     const uint32_t* k = S.keys + (size_t)sample * 4;
     const uint32_t key[2][2] = {{k[0], k[1]}, {k[2], k[3]}};
-    ea_sample_run<Z>(P.C, S, sample, key, smem_raw, P.ctl, poll);
+    ea_sample_run<Z, T>(P.C, S, sample, key, smem_raw, P.ctl, poll);
     __syncthreads();
   }
 }
@@ -716,6 +751,7 @@ extern "C" int32_t critmc_ea_campaign_run_ctl(const critmc_ea_size* sizes, int32
   std::vector<EaSet> sets(n_sizes);
   long long total = 0;
   size_t smem = 0;
+  int threads = 64;
   for (int i = 0; i < n_sizes; ++i) {
     const critmc_ea_size& z = sizes[i];
     if (!z.keys) return fail(CRITMC_ERR_INVALID, "null pointer argument");
@@ -725,6 +761,7 @@ extern "C" int32_t critmc_ea_campaign_run_ctl(const critmc_ea_size* sizes, int32
     sets[i].keys = z.keys;
     total += z.n_samples;
     smem = std::max(smem, ea_smem_bytes(sets[i].g, dim, z.lx));
+    threads = std::max(threads, ea_threads_for(sets[i].g, 2 * dim));
   }
   if (buffer_bytes < critmc_ea_campaign_buffer_bytes(n_sizes, total))
     return fail(CRITMC_ERR_INVALID, "campaign buffer too small");
@@ -754,16 +791,23 @@ extern "C" int32_t critmc_ea_campaign_run_ctl(const critmc_ea_size* sizes, int32
   P.sets = reinterpret_cast<const EaSet*>(dev + sets_off);
   P.work = reinterpret_cast<const uint32_t*>(dev + work_off);
   P.n_work = (int)total;
-  auto launch = [&](auto kern) -> int {
+  auto launch = [&](auto kern, int nthreads) -> int {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return cuda_fail("shared memory attribute");
     int per_sm = 0, dev_id = 0, sms = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, EA_THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nthreads, smem);
     cudaGetDevice(&dev_id);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
     const long long grid = std::max(1LL, std::min<long long>(total, (long long)std::max(1, per_sm) * sms));
-    kern<<<(unsigned)grid, EA_THREADS, smem, s>>>(P);
+    kern<<<(unsigned)grid, nthreads, smem, s>>>(P);
     return cuda_check("launch");
   };
-  return dim == 2 ? launch(ea_campaign_kernel<4>) : launch(ea_campaign_kernel<6>);
+  if (dim == 2) {
+    if (threads == 64) return launch(ea_campaign_kernel<4, 64>, 64);
+    if (threads == 128) return launch(ea_campaign_kernel<4, 128>, 128);
+    return launch(ea_campaign_kernel<4, 256>, 256);
+  }
+  if (threads == 64) return launch(ea_campaign_kernel<6, 64>, 64);
+  if (threads == 128) return launch(ea_campaign_kernel<6, 128>, 128);
+  return launch(ea_campaign_kernel<6, 256>, 256);
 }

@@ -24,7 +24,6 @@
 namespace critmc {
 
 constexpr int EA_THREADS = 256;
-constexpr int EA_WARPS = EA_THREADS / 32;
 constexpr int EA_MAX_SITES = 4096;
 constexpr int EA_MAX_L = 64;
 constexpr int EA_NOBS = 7;  // e, q_l, |q|, q^2, q^4, |q(kmin)|^2, count (critmc glass.py:24-31)
@@ -205,9 +204,17 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
   __shared__ unsigned long long sw_acc[32], sw_try[32], lhist[32][2], trip[2];
   __shared__ int s_stop;
   __shared__ uint32_t s_acc_mask[2];  // swaps accepted in the step's walk, by set
+  __shared__ uint32_t thr_s[31][32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m = C.m;
+  const int ext = S.ext[0];  // every extent (equal extents are required)
+  // the first 32 swap thresholds of each pair (energy gaps below 128, the common
+  // case) in shared memory; the walk reads wider gaps from global memory
+  for (int i = tid; i < (m - 1) * 32; i += T) {
+    const int k = i >> 5, j = i & 31;
+    thr_s[k][j] = j < C.swap_width ? C.swap_thr[(size_t)k * C.swap_width + j] : 0u;
+  }
   uint32_t* gw = S.words + (size_t)sample * 2 * n_sites;
   for (uint32_t j = tid; j < 2 * n_sites; j += T) lat[j] = gw[j];
   for (uint32_t j = tid; j < n_sites; j += T) jn[j] = S.jneg[(size_t)sample * n_sites + j];
@@ -359,7 +366,7 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
           if (!ok) {
             int j = de / 4;
             if (j > C.swap_width - 1) j = C.swap_width - 1;
-            ok = swu[r][k] < C.swap_thr[(size_t)k * C.swap_width + j];
+            ok = swu[r][k] < (j < 32 ? thr_s[k][j] : C.swap_thr[(size_t)k * C.swap_width + j]);
           }
           if (ok) {  // the carried entry moves on to k+1
             accm |= 1u << k;
@@ -431,20 +438,21 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
     }
     // per-plane overlap counts: warp w handles planes (d, x) = w, w + WARPS, ...;
     // its lanes split the plane's sites (at most 256 / 32 = 8 each)
-    for (int pl = warp; pl < DIM * S.ext[0]; pl += (T / 32)) {
-      const int d = pl / S.ext[0], x0 = pl % S.ext[0];
-      const int e1 = S.ext[d == 0 ? 1 : 0], e2 = DIM == 3 ? S.ext[d == 2 ? 1 : 2] : 1;
+    // (equal extents: ext = lx for every direction; coordinates in registers)
+    for (int pl = warp; pl < DIM * ext; pl += (T / 32)) {
+      const int d = pl / ext, x0 = pl - d * ext;
+      const int n_pl = DIM == 3 ? ext * ext : ext;
       uint32_t vp[4] = {0, 0, 0, 0};
-      for (int idx = lane; idx < e1 * e2; idx += 32) {
-        int xyz[3] = {0, 0, 0};
-        xyz[d] = x0;
-        xyz[d == 0 ? 1 : 0] = idx % e1;
-        if (DIM == 3) xyz[d == 2 ? 1 : 2] = idx / e1;
-        const int col = (xyz[0] + xyz[1] + xyz[2]) & 1;
-        const uint32_t slot = (uint32_t)((xyz[1] + g.ly * xyz[2]) * g.hx + xyz[0] / 2);
+      for (int idx = lane; idx < n_pl; idx += 32) {
+        const int a = idx % ext, b = DIM == 3 ? idx / ext : 0;
+        const int x = d == 0 ? x0 : a;
+        const int y = d == 0 ? a : (d == 1 ? x0 : b);
+        const int z = d == 2 ? x0 : b;
+        const int col = (x + y + z) & 1;
+        const uint32_t slot = (uint32_t)((y + g.ly * z) * g.hx + x / 2);
         vadd1(vp, qw[(size_t)col * g.slots + slot]);
       }
-      splane[(d * S.ext[0] + x0) * 32 + lane] = vreduce(vp, lane);
+      splane[(d * ext + x0) * 32 + lane] = vreduce(vp, lane);
     }
     __syncthreads();
     if (tid < m) {
@@ -452,15 +460,15 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
       const double n = (double)n_sites;
       const double nb = n * DIM;
       int qs = 0;
-      for (int x = 0; x < S.ext[0]; ++x) qs += splane[x * 32 + k];
+      for (int x = 0; x < ext; ++x) qs += splane[x * 32 + k];
       const double q = (2.0 * qs - n) / n;
       const double ql = (2.0 * qlcnt[k] - nb) / nb;
       double qk2 = 0.0;
       for (int d = 0; d < DIM; ++d) {
-        const double per = n / S.ext[d];
+        const double per = n / ext;
         double re = 0.0, im = 0.0;
-        for (int x = 0; x < S.ext[d]; ++x) {
-          const double sx = 2.0 * splane[(d * S.ext[0] + x) * 32 + k] - per;
+        for (int x = 0; x < ext; ++x) {
+          const double sx = 2.0 * splane[(d * ext + x) * 32 + k] - per;
           re += S.cosx[x] * sx;
           im += S.sinx[x] * sx;
         }

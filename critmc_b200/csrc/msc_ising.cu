@@ -112,9 +112,10 @@ __device__ __noinline__ int3 msc_flush(const MscRule<Z, RULE> rule, const MscGeo
 // loads, Philox evaluations and comparisons are independent and interleave,
 // at two blocks per SM (up to 128 registers a thread, nothing rematerialised):
 // +5 % over one row per step at three blocks per SM (85 registers).  3D: one
-// row per step, three blocks per SM.
+// row per step, three blocks per SM, except for the general (field) rules,
+// which spilled at 85 registers: two blocks per SM, +3 % measured.
 template <int Z, int RULE, int KG, int PR, bool BATCH>
-__global__ void __launch_bounds__(MSC_THREADS, Z == 4 ? 2 : 3)
+__global__ void __launch_bounds__(MSC_THREADS, (Z == 4 || RULE >= RULE_GEN) ? 2 : 3)
     msc_halfsweep_kernel(const __grid_constant__ MscParams P) {
   __shared__ MscFix fix[MSC_WARPS][MSC_FIXCAP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

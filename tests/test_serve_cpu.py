@@ -45,3 +45,37 @@ def test_request_schedules_and_sizes():
 def test_server_needs_a_gpu():
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         Server()
+
+
+def test_team_choice_follows_the_cost_model():
+    """_team_for: one block when that is predicted within team_after_s; else the
+    smallest team predicted within it; else the smallest within TEAM_SLACK of
+    the fastest.  Exercised on an object with the server's policy fields only
+    (no device)."""
+    from critmc_b200.serve import COSTS, TEAM_SLACK, TEAMS
+
+    class Policy:
+        _team_for = Server._team_for
+
+        def __init__(self, after, max_team=8):
+            self.team_after_s, self.teams = after, tuple(t for t in TEAMS if t <= max_team)
+            self.costs = dict(COSTS)
+
+    big = Request("ising", 1024, 0.44, 100_000)
+    small = Request("ising", 16, 0.44, 100_000)
+    assert Policy(None)._team_for(big, "msc") == 1
+    assert Policy(1.0)._team_for(small, "msc") == 1  # one block already fast enough
+    p = Policy(1.0)
+    per = big.sweeps
+    pred = {t: per * (p.costs[(f"team{t}", "msc")][0] + p.costs[(f"team{t}", "msc")][1] * big.n_sites)
+            for t in p.teams}
+    t = p._team_for(big, "msc")
+    within = [u for u in p.teams if pred[u] <= 1.0]
+    if within:
+        assert t == within[0]
+    else:
+        best = min(pred.values())
+        assert pred[t] <= TEAM_SLACK * best and all(pred[u] > TEAM_SLACK * best for u in p.teams if u < t)
+    assert Policy(1.0, max_team=4)._team_for(big, "msc") <= 4
+    # a generous threshold keeps long requests on one block
+    assert Policy(1e9)._team_for(big, "msc") == 1

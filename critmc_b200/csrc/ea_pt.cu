@@ -259,62 +259,58 @@ __device__ void ea_sample_run(const EaCommon& C, const EaSet& S, int sample, con
       for (int c = 0; c < 2; ++c) {
         int nf = 0;
         const uint32_t work = 2 * g.slots;  // both sets, one colour
-        const uint32_t rounds = (work + T - 1) / T;
-        for (uint32_t it = 0; it < rounds; ++it) {
-          const uint32_t j = it * T + tid;
-          uint32_t U = 0, D = 0, idx = 0;
-          if (j < work) {
-            const int set = j >= g.slots;
-            const uint32_t s = j - set * g.slots;
+        auto flush = [&]() {
+          __syncwarp();
+          for (int e = lane; e < nf; e += 32) {
+            const EaFix f = fix[warp][e];
+            const int set = f.idx >= n_sites;
+            const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
             uint32_t w_s;
             Count3 cnt;
             ea_site<Z>(g, lat, jn, set, c, s, w_s, cnt);
-            // flips with dE <= 0 (>= z/2 unsatisfied bonds) are always accepted
-            const uint32_t alw = (Z == 6) ? (cnt.b2 | (cnt.b1 & cnt.b0)) : (cnt.b1 | cnt.b2);
-            D = alw;
-            U = ~alw;
-            const uint32_t k0 = key[set][0], k1 = key[set][1];
-            ea_planes<Z>(C, cnt, k0, k1, s, sweep, (uint32_t)c, 0, 2, D, U);
-            idx = (uint32_t)set * n_sites + (uint32_t)c * g.slots + s;
-            if (U == 0) lat[idx] = w_s ^ D;
+            uint32_t D2 = f.D, U2 = f.U;
+            ea_planes<Z>(C, cnt, key[set][0], key[set][1], s, sweep, (uint32_t)c, 2, 8, D2, U2);
+            lat[f.idx] = w_s ^ D2;
           }
+          __syncwarp();
+          nf = 0;
+        };
+        auto defer = [&](uint32_t U, uint32_t D, uint32_t idx) {
           const uint32_t need = __ballot_sync(0xffffffffu, U != 0);
           if (need) {
             const int cntn = __popc(need);
-            if (nf + cntn > EA_FIXCAP) {
-              __syncwarp();
-              for (int e = lane; e < nf; e += 32) {
-                const EaFix f = fix[warp][e];
-                const int set = f.idx >= n_sites;
-                const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
-                uint32_t w_s;
-                Count3 cnt;
-                ea_site<Z>(g, lat, jn, set, c, s, w_s, cnt);
-                uint32_t D2 = f.D, U2 = f.U;
-                ea_planes<Z>(C, cnt, key[set][0], key[set][1], s, sweep,
-                             (uint32_t)c, 2, 8, D2, U2);
-                lat[f.idx] = w_s ^ D2;
-              }
-              __syncwarp();
-              nf = 0;
-            }
+            if (nf + cntn > EA_FIXCAP) flush();
             if (U != 0) fix[warp][nf + __popc(need & lt_mask)] = EaFix{idx, U, D};
             nf += cntn;
           }
+        };
+        // two work items per loop step: their site loads, Philox planes and
+        // comparisons are independent and interleave (+1 to +3 % per size);
+        // an item past the end is computed on slot 0 and discarded
+        const uint32_t rounds = (work + 2 * T - 1) / (2 * T);
+        for (uint32_t it = 0; it < rounds; ++it) {
+          const uint32_t jA = it * 2 * T + tid, jB = jA + T;
+          const bool vA = jA < work, vB = jB < work;
+          const uint32_t jAc = vA ? jA : 0u, jBc = vB ? jB : 0u;
+          const int setA = jAc >= g.slots, setB = jBc >= g.slots;
+          const uint32_t sA = jAc - setA * g.slots, sB = jBc - setB * g.slots;
+          uint32_t wA, wB;
+          Count3 cA, cB;
+          ea_site<Z>(g, lat, jn, setA, c, sA, wA, cA);
+          ea_site<Z>(g, lat, jn, setB, c, sB, wB, cB);
+          const uint32_t alwA = (Z == 6) ? (cA.b2 | (cA.b1 & cA.b0)) : (cA.b1 | cA.b2);
+          const uint32_t alwB = (Z == 6) ? (cB.b2 | (cB.b1 & cB.b0)) : (cB.b1 | cB.b2);
+          uint32_t DA = alwA, UA = vA ? ~alwA : 0u, DB = alwB, UB = vB ? ~alwB : 0u;
+          ea_planes<Z>(C, cA, key[setA][0], key[setA][1], sA, sweep, (uint32_t)c, 0, 2, DA, UA);
+          ea_planes<Z>(C, cB, key[setB][0], key[setB][1], sB, sweep, (uint32_t)c, 0, 2, DB, UB);
+          const uint32_t idxA = (uint32_t)setA * n_sites + (uint32_t)c * g.slots + sA;
+          const uint32_t idxB = (uint32_t)setB * n_sites + (uint32_t)c * g.slots + sB;
+          if (vA && UA == 0) lat[idxA] = wA ^ DA;
+          if (vB && UB == 0) lat[idxB] = wB ^ DB;
+          defer(UA, DA, idxA);
+          defer(UB, DB, idxB);
         }
-        __syncwarp();
-        for (int e = lane; e < nf; e += 32) {
-          const EaFix f = fix[warp][e];
-          const int set = f.idx >= n_sites;
-          const uint32_t s = f.idx - set * n_sites - (uint32_t)c * g.slots;
-          uint32_t w_s;
-          Count3 cnt;
-          ea_site<Z>(g, lat, jn, set, c, s, w_s, cnt);
-          uint32_t D2 = f.D, U2 = f.U;
-          ea_planes<Z>(C, cnt, key[set][0], key[set][1], s, sweep,
-                       (uint32_t)c, 2, 8, D2, U2);
-          lat[f.idx] = w_s ^ D2;
-        }
+        flush();
         __syncthreads();
       }
     }

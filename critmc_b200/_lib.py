@@ -41,6 +41,7 @@ SIGNATURES: dict[str, tuple] = {
     "critmc_ising_msc_measure": (_I32, [_P, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "critmc_item_prepare": (_I32, [_P, _D, _D, _D]),
     "critmc_items_buffer_bytes": (_I64, [_I32]),
+    "critmc_items_team_clusters": (_I32, [_I32, _I32, _I32, _I32]),
     "critmc_run_items": (_I32, [_P, _I32, _P, _I64, _P, _I32, _P]),
     "critmc_ising_msc_noalloc_max_scratch_bytes": (_I64, []),
     "critmc_ising_msc_run_noalloc": (

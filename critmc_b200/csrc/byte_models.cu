@@ -558,6 +558,16 @@ __global__ void __launch_bounds__(ITEM_THREADS) byte_items_kernel(const critmc_i
   }
 }
 
+int byte_items_team_clusters(int team) {
+  switch (team) {
+    case 2: return team_clusters(byte_items_kernel<2>, 2, ITEM_THREADS);
+    case 4: return team_clusters(byte_items_kernel<4>, 4, ITEM_THREADS);
+    case 8: return team_clusters(byte_items_kernel<8>, 8, ITEM_THREADS);
+    case 16: return team_clusters(byte_items_kernel<16>, 16, ITEM_THREADS);
+    default: return fail(CRITMC_ERR_INVALID, "team size must be 2, 4, 8 or 16");
+  }
+}
+
 int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t smem, int team, const RunCtl& ctl,
                       cudaStream_t s) {
   switch (team) {

@@ -24,12 +24,11 @@ int cuda_fail(const char* what);
 // CRITMC_OK if no CUDA error is pending, else record and clear it (CRITMC_ERR_CUDA)
 int cuda_check(const char* what);
 
-// Persistent launch of a team kernel: clusters of `cl` blocks (2..16) of
-// `threads` threads, as many clusters as fit on the GPU at once and no more
-// than `n_items`.  Clusters of more than 8 blocks need the non-portable size
-// attribute; a size the GPU cannot schedule is refused rather than launched.
-template <typename... KArgs, typename... Args>
-int launch_team(void (*kern)(KArgs...), int cl, int threads, int n_items, cudaStream_t s, Args&&... args) {
+// Clusters of `cl` blocks (2..16) of `threads` threads of a team kernel that
+// the current GPU can run at once (0: it cannot schedule that cluster size);
+// clusters of more than 8 blocks need the non-portable size attribute.
+template <typename... KArgs>
+int team_clusters(void (*kern)(KArgs...), int cl, int threads) {
   if (cl < 2 || cl > 16) return fail(CRITMC_ERR_INVALID, "team size must be 2..16");
   if (cl > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
     return cuda_fail("cluster size attribute");
@@ -41,14 +40,33 @@ int launch_team(void (*kern)(KArgs...), int cl, int threads, int n_items, cudaSt
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)cl);
   cfg.blockDim = dim3((unsigned)threads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int clusters = 0;
   if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess) return cuda_fail("cluster occupancy");
+  return clusters;
+}
+
+// Persistent launch of a team kernel: as many clusters of `cl` blocks as fit
+// on the GPU at once and no more than `n_items`.  A size the GPU cannot
+// schedule is refused rather than launched.
+template <typename... KArgs, typename... Args>
+int launch_team(void (*kern)(KArgs...), int cl, int threads, int n_items, cudaStream_t s, Args&&... args) {
+  const int clusters = team_clusters(kern, cl, threads);
+  if (clusters < 0) return clusters;
   if (clusters < 1) return fail(CRITMC_ERR_UNSUPPORTED, "this GPU cannot schedule a cluster of that many blocks");
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(std::min(n_items, clusters) * cl));
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   if (cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...) != cudaSuccess) return cuda_fail("team launch");
   return CRITMC_OK;
 }

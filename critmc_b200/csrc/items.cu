@@ -132,6 +132,16 @@ extern "C" int32_t critmc_item_prepare(critmc_item* it, double beta, double h, d
   return CRITMC_OK;
 }
 
+extern "C" int32_t critmc_items_team_clusters(int32_t kind, int32_t q_or_n, int32_t dim, int32_t team) {
+  clear_error();
+  const int fam = family_of(kind);
+  if (fam < 0) return fail(CRITMC_ERR_INVALID, "unknown item kind");
+  if (team != 2 && team != 4 && team != 8 && team != 16) return fail(CRITMC_ERR_INVALID, "team size must be 2, 4, 8 or 16");
+  if (fam == 0) return msc_items_team_clusters(team);
+  if (fam == 1) return byte_items_team_clusters(team);
+  return on_items_team_clusters(q_or_n, dim, team);
+}
+
 extern "C" int64_t critmc_items_buffer_bytes(int32_t n_items) {
   return (int64_t)ITEMS_HEADER + (int64_t)n_items * (int64_t)sizeof(critmc_item);
 }

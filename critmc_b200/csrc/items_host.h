@@ -24,4 +24,10 @@ int byte_items_launch(const critmc_item* items, int n, unsigned* queue, size_t s
 int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem, int team,
                     const RunCtl& ctl, cudaStream_t s);
 
+// Clusters of `team` blocks (2, 4, 8, 16) of each family's item kernel that the
+// current GPU runs at once (0: it cannot schedule that size), or an error.
+int msc_items_team_clusters(int team);
+int byte_items_team_clusters(int team);
+int on_items_team_clusters(int n_comp, int dim, int team);
+
 }  // namespace critmc

@@ -929,6 +929,29 @@ static int on_items_launch_nz(const critmc_item* items, int n, unsigned* queue, 
   return CRITMC_OK;
 }
 
+template <int N, int Z>
+static int on_items_team_clusters_nz(int team) {
+  switch (team) {
+    case 2: return team_clusters(on_items_kernel<N, Z, 2>, 2, ON_THREADS);
+    case 4: return team_clusters(on_items_kernel<N, Z, 4>, 4, ON_THREADS);
+    case 8: return team_clusters(on_items_kernel<N, Z, 8>, 8, ON_THREADS);
+    case 16: return team_clusters(on_items_kernel<N, Z, 16>, 16, ON_THREADS);
+    default: return fail(CRITMC_ERR_INVALID, "team size must be 2, 4, 8 or 16");
+  }
+}
+
+int on_items_team_clusters(int n_comp, int dim, int team) {
+  switch (n_comp * 10 + dim) {
+    case 21: return on_items_team_clusters_nz<2, 2>(team);
+    case 22: return on_items_team_clusters_nz<2, 4>(team);
+    case 23: return on_items_team_clusters_nz<2, 6>(team);
+    case 31: return on_items_team_clusters_nz<3, 2>(team);
+    case 32: return on_items_team_clusters_nz<3, 4>(team);
+    case 33: return on_items_team_clusters_nz<3, 6>(team);
+    default: return fail(CRITMC_ERR_INVALID, "O(n) items need n = 2 or 3 and dim 1..3");
+  }
+}
+
 int on_items_launch(const critmc_item* items, int n, int n_comp, int dim, unsigned* queue, size_t smem, int team,
                     const RunCtl& ctl, cudaStream_t s) {
   switch (n_comp * 10 + dim) {

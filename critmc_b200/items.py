@@ -153,6 +153,17 @@ class ItemRun:
                 "stiff_s": to_host(t["ss"]), "aux": aux}
 
 
+def team_clusters(kind: int, q_or_n: int, dim: int, team: int, device) -> int:
+    """Teams of ``team`` blocks of the item kernel for ``kind`` items that the
+    GPU runs at once; 0 if it cannot schedule clusters of that size."""
+    st = _lib.lib().critmc_items_team_clusters
+    with torch.cuda.device(device):
+        n = st(int(kind), int(q_or_n), int(dim), int(team))
+    if n < 0:
+        _lib.check(n)
+    return int(n)
+
+
 def launch_items(items, device, buffer: torch.Tensor | None, *, staging: torch.Tensor | None = None,
                  smem_limit: int = 0, stream=None, control=None) -> torch.Tensor:
     """Run a ctypes array (or list) of ``CritmcItem``; returns the (grown) descriptor buffer.

@@ -320,6 +320,7 @@ class Server:
         # waiting for 16 free SMs of one GPC), with up to 8 blocks 1.1 s
         self.team_after_s = team_after_s
         self.teams = tuple(t for t in TEAMS if t <= max_team)
+        self._team_ok: dict = {}
         self.team_sizes_used: set[int] = set()
         self.keep_series, self.keep_state = keep_series, keep_state
         self.stats_lag = int(stats_lag)
@@ -404,12 +405,26 @@ class Server:
         if pred[1] <= self.team_after_s:
             return 1
         for t in self.teams:
+            if not self._team_fits(req, family, t):
+                continue
             a, b = self.costs[(f"team{t}", family)]
             pred[t] = per * (a + b * req.n_sites)
             if pred[t] <= self.team_after_s:
                 return t
         fastest = min(pred.values())
         return min(t for t, p in pred.items() if p <= TEAM_SLACK * fastest)
+
+    def _team_fits(self, req: Request, family: str, team: int) -> bool:
+        """Whether this GPU schedules teams of that size for the request's kernel
+        (asked once per kernel and size)."""
+        kind = {"msc": ITEM_MSC_ISING, "byte": ITEM_BYTE_ISING, "potts": ITEM_POTTS}.get(family, ITEM_ON)
+        n = int(family[2:]) if family.startswith("on") else 0
+        key = (kind, n, len(req.shape), team)
+        if key not in self._team_ok:
+            from .items import team_clusters
+
+            self._team_ok[key] = team_clusters(kind, n, len(req.shape), team, self.device) > 0
+        return self._team_ok[key]
 
     def _grid_free(self) -> bool:
         return sum(1 for lane in self.grid_lanes if lane.jobs) < self.max_grid_lanes

@@ -378,6 +378,12 @@ typedef struct {
  * field h for Ising) and check its geometry and schedule.                   */
 int32_t critmc_item_prepare(critmc_item* item, double beta, double h, double step);
 
+/* Teams of `team` blocks (2, 4, 8 or 16) of the item kernel for items of
+ * `kind` (and q_or_n, dim for O(n)) that the current GPU runs at once: 0 if it
+ * cannot schedule clusters of that size (critmc_run_items would then refuse
+ * such items with CRITMC_ERR_UNSUPPORTED), a negative status on error.      */
+int32_t critmc_items_team_clusters(int32_t kind, int32_t q_or_n, int32_t dim, int32_t team);
+
 /* Device bytes needed to run n_items items (descriptors + queue counters).  */
 int64_t critmc_items_buffer_bytes(int32_t n_items);
 

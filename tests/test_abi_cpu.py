@@ -142,3 +142,5 @@ def test_item_team_sizes_are_checked_before_any_device_work():
     assert "team" in _lib.last_error()
     with pytest.raises(ValueError, match="team"):
         ItemRun(None, None, {}, 0.4, np.array([[0, 1]]), 1, team=5)
+    assert lib.critmc_items_team_clusters(0, 0, 2, 3) == -1  # refused before any device call
+    assert lib.critmc_items_team_clusters(9, 0, 2, 8) == -1

@@ -14,7 +14,7 @@ import torch
 
 from critmc_b200 import ON, Ising, Potts, hypercubic, square
 from critmc_b200.control import CANCELLED, TIMEOUT, RunControl
-from critmc_b200.items import ItemRun, run_items
+from critmc_b200.items import ITEM_BYTE_ISING, ITEM_MSC_ISING, ITEM_ON, ITEM_POTTS, ItemRun, run_items, team_clusters
 
 from test_gpu_items import MIX, _assert_same, _pair
 
@@ -128,3 +128,13 @@ def test_team_items_stop_on_budget_and_on_cancel(cuda):
     run_items(its, cuda)
     for a, it in zip(alone, its):
         _assert_same(a, it.finish())
+
+
+def test_team_capacity_query(cuda):
+    """The server asks which team sizes the GPU schedules: on a B200 every
+    family runs clusters of up to 16 blocks, several at once."""
+    for kind, n, dim in ((ITEM_MSC_ISING, 0, 2), (ITEM_BYTE_ISING, 0, 2), (ITEM_POTTS, 10, 2), (ITEM_ON, 2, 2),
+                         (ITEM_ON, 3, 3)):
+        counts = [team_clusters(kind, n, dim, t, cuda) for t in (2, 4, 8, 16)]
+        assert all(c >= 1 for c in counts), (kind, n, dim, counts)
+        assert counts == sorted(counts, reverse=True)

@@ -61,6 +61,9 @@ def test_team_choice_follows_the_cost_model():
             self.team_after_s, self.teams = after, tuple(t for t in TEAMS if t <= max_team)
             self.costs = dict(COSTS)
 
+        def _team_fits(self, req, family, team):  # every size schedulable (no device here)
+            return True
+
     big = Request("ising", 1024, 0.44, 100_000)
     small = Request("ising", 16, 0.44, 100_000)
     assert Policy(None)._team_for(big, "msc") == 1

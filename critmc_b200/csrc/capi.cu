@@ -41,6 +41,40 @@ int cuda_check(const char* what) {
 }
 
 namespace {
+struct TeamCapacity {
+  int dev, cl, clusters;
+  const void* kern;
+};
+std::mutex g_team_mutex;
+std::vector<TeamCapacity> g_team_capacity;  // a few entries: kernels x sizes x devices
+}  // namespace
+
+int team_clusters_cached(const void* kern, int cl, int* out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  std::lock_guard<std::mutex> lock(g_team_mutex);
+  for (const TeamCapacity& t : g_team_capacity)
+    if (t.dev == dev && t.cl == cl && t.kern == kern) {
+      *out = t.clusters;
+      return 1;
+    }
+  return 0;
+}
+
+void team_clusters_store(const void* kern, int cl, int clusters) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lock(g_team_mutex);
+  g_team_capacity.push_back(TeamCapacity{dev, cl, clusters, kern});
+}
+
+namespace {
 
 struct GraphEntry {
   std::vector<unsigned char> key;

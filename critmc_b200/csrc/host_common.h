@@ -27,9 +27,15 @@ int cuda_check(const char* what);
 // Clusters of `cl` blocks (2..16) of `threads` threads of a team kernel that
 // the current GPU can run at once (0: it cannot schedule that cluster size);
 // clusters of more than 8 blocks need the non-portable size attribute.
+// The answer is kept per device, kernel and size (a server asks before every
+// tick's launch).
+int team_clusters_cached(const void* kern, int cl, int* out);
+void team_clusters_store(const void* kern, int cl, int clusters);
 template <typename... KArgs>
 int team_clusters(void (*kern)(KArgs...), int cl, int threads) {
   if (cl < 2 || cl > 16) return fail(CRITMC_ERR_INVALID, "team size must be 2..16");
+  int known = 0;
+  if (team_clusters_cached(reinterpret_cast<const void*>(kern), cl, &known)) return known;
   if (cl > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
     return cuda_fail("cluster size attribute");
   cudaLaunchAttribute attr[1];
@@ -44,6 +50,7 @@ int team_clusters(void (*kern)(KArgs...), int cl, int threads) {
   cfg.numAttrs = 1;
   int clusters = 0;
   if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess) return cuda_fail("cluster occupancy");
+  team_clusters_store(reinterpret_cast<const void*>(kern), cl, clusters);
   return clusters;
 }
 

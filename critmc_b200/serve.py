@@ -291,7 +291,7 @@ class Server:
     """Continuous-batching sampler for a stream of mixed requests on one GPU."""
 
     def __init__(self, device=None, *, hbm_budget: int | None = None, reserve: int = 1 << 30,
-                 tick_ms: float = 20.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
+                 tick_ms: float = 10.0, max_active: int = 4096, grid_min_sites: int = 1 << 18,
                  grid_after_s: float | None = None, team_after_s: float | None = 1.0, max_team: int = 8,
                  max_grid_lanes: int = 8, arena_bytes: int = 256 << 20, keep_series: bool = True,
                  keep_state: bool = False, grid_streams: int = 32, on_result=None, costs=None,

@@ -70,6 +70,8 @@ class ItemRun:
 
     ``team``: thread blocks advancing the chain together (1; or 2, 4, 8, 16 as a
     thread-block cluster, for large lattices); the results do not depend on it.
+    The run owns the device buffers that ``item`` points to (outputs, running
+    sums): keep it alive until the launch has completed.
     """
 
     def __init__(self, model, chain, running: dict, beta: float, schedule: np.ndarray, n_meas: int,

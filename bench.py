@@ -471,10 +471,11 @@ def run_reference(args) -> None:
     float64 tables and PCG64DXSM stream), restated in C and bit-identical to
     critmc's numba ``run`` (tests/test_critmc_port_cpu.py), on every host thread.
 
-    One step advances, on each host thread, its own 4096 x 64 torus (a strip of
-    the L = 4096 workload, 262,144 sites) by one sweep, so that `--steps K`
-    stays within minutes; the rate is updates per ns of wall time over the K
-    steps."""
+    One step advances, on each host thread, its own torus of L = 4096 columns by
+    one sweep: the whole 4096 x 4096 lattice when `--steps K` allows, else the
+    tallest power-of-two strip of it (at least 64 rows) that keeps the K timed
+    steps near 40 s (a full sweep takes about 0.2 s on one core); the rate is
+    updates per ns of wall time over the K steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -482,14 +483,18 @@ def run_reference(args) -> None:
 
     oracle.lib()
     threads = os.cpu_count() or 1
-    shape = (L_HEAD, 64)
+    rows = L_HEAD
+    while rows > 64 and args.steps * rows * L_HEAD / 0.08e9 > 40.0:
+        rows //= 2
+    shape = (L_HEAD, rows)
     n = shape[0] * shape[1]
-    chains = [_critmc_port_state(shape[0], shape[1], t) for t in range(threads)]
+    _, nbr, _ = _critmc_port_state(shape[0], shape[1], 0)  # one neighbour table, shared
+    spins = [(2 * np.random.default_rng(100 + t).integers(0, 2, n) - 1).astype(np.int8) for t in range(threads)]
+    words = [oracle.pcg_words(np.random.PCG64DXSM(200 + t).state) for t in range(threads)]
     runs = [np.zeros(2, np.int64) for _ in range(threads)]
 
     def step(t: int) -> None:
-        s, nbr, words = chains[t]
-        oracle.critmc_ising_run(s, nbr, words, BETAS[t % 3], 0.0, [[0, 1]], 1, running=runs[t])
+        oracle.critmc_ising_run(spins[t], nbr, words[t], BETAS[t % 3], 0.0, [[0, 1]], 1, running=runs[t])
 
     with cf.ThreadPoolExecutor(threads) as ex:
         for _ in range(args.warmup):
@@ -499,14 +504,15 @@ def run_reference(args) -> None:
             list(ex.map(step, range(threads)))
         wall = time.perf_counter() - t0
     value = threads * n * args.steps / wall / 1e9
-    sample = (f"{threads} host threads, each advancing its own {shape[0]}x{shape[1]} torus by one typewriter "
-              f"Metropolis sweep per step with critmc's kernel restated in C (bit-identical to critmc)")
+    what = "4096x4096 lattice" if rows == L_HEAD else f"{shape[0]}x{shape[1]} strip of the 4096x4096 lattice"
+    sample = (f"{threads} host threads, each advancing its own {what} by one typewriter Metropolis sweep per "
+              f"step with critmc's kernel restated in C (bit-identical to critmc)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-        "config": {"workload": f"2D Ising L={L_HEAD} Metropolis (4096x64 strips per thread)",
+        "config": {"workload": f"2D Ising L={L_HEAD} Metropolis ({what} per thread)",
                    "parallelism": f"{threads} host threads"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
